@@ -1,0 +1,285 @@
+/*
+ * supra_b200 — C ABI of the B200 receive-processing path (DAS, MV, envelope/IQ, log compression,
+ * scan conversion) that stands in for SUPRA's receive nodes.
+ *
+ * Conventions
+ *  - Every entry point returns an int status: SB_OK (0) or a negative SB_ERR_* code. The message of
+ *    the last failure on the calling thread is returned by sb_last_error(). No C++ exception crosses
+ *    this boundary.
+ *  - All data pointers passed to *_run functions are DEVICE pointers owned by the caller; nothing is
+ *    synchronised with the host. Work is enqueued on the caller's stream (a cudaStream_t passed as
+ *    sb_stream; NULL is the legacy default stream). This mirrors SUPRA, whose nodes launch on the
+ *    stream of the input container and never synchronise (SupraLib/Container.h:104-108).
+ *  - Plans own device copies of geometry, filters and look-up tables. A plan is not thread safe:
+ *    one plan per node, as SUPRA serialises each node body under the node mutex
+ *    (SupraLib/AbstractNode.h:119-132).
+ *  - Layouts follow the reference: raw channel data [tx][channel][sample] (Beamformer/USRawData.h:24),
+ *    beamformed / envelope images [depth][scanline] (scanline fastest, RxBeamformerCuda.cu:321),
+ *    delayed channel data [scanline][channel][depth] (RawDelay.cu:307).
+ */
+#ifndef SUPRA_B200_H
+#define SUPRA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status, dtypes, streams */
+
+#define SB_OK 0
+#define SB_ERR_INVALID_ARG (-1)   /* bad pointer, size, enum or parameter range */
+#define SB_ERR_CUDA (-2)          /* a CUDA runtime call failed (message has the CUDA error) */
+#define SB_ERR_UNSUPPORTED (-3)   /* dtype / configuration combination not implemented */
+#define SB_ERR_NO_MEMORY (-4)     /* device or host allocation failed */
+#define SB_ERR_TIMEOUT (-5)       /* a bounded device-side wait gave up (persistent kernels) */
+#define SB_ERR_NOT_READY (-6)     /* plan used before it was fully initialised */
+
+typedef enum sb_dtype {
+    SB_INT16 = 1,      /* SUPRA TypeInt16 */
+    SB_FLOAT32 = 2,    /* SUPRA TypeFloat */
+    SB_UINT8 = 3,      /* SUPRA TypeUint8 */
+    SB_COMPLEX64 = 4,  /* interleaved (re, im) float pairs; extension, no SUPRA counterpart */
+    SB_UINT16 = 5      /* SUPRA TypeUint16 (MV output type list) */
+} sb_dtype;
+
+typedef void* sb_stream; /* a cudaStream_t */
+
+const char* sb_last_error(void);
+int sb_version(int* major, int* minor);
+
+/* ---------------------------------------------------------------- geometry */
+
+/* Window types, same numbering as SUPRA's WindowType (Beamformer/WindowFunction.h:37-44). */
+typedef enum sb_window {
+    SB_WINDOW_RECTANGULAR = 0,
+    SB_WINDOW_HANN = 1,
+    SB_WINDOW_HAMMING = 2,
+    SB_WINDOW_GAUSS = 3
+} sb_window;
+
+/* Transmit reference of one receive scanline. Byte-compatible with
+ * ScanlineRxParameters3D::TransmitParameters (SupraLib/USImageProperties.h:52-57). */
+typedef struct sb_tx_params {
+    uint16_t first_active_element[2]; /* x, y element index of the first active element */
+    uint16_t last_active_element[2];  /* x, y; the reference loops use `<`, so this one is skipped */
+    uint16_t tx_scanline_idx;         /* transmit event whose channel data this scanline uses */
+    uint16_t _pad[3];
+    double initial_delay_s;           /* [s] */
+} sb_tx_params;
+
+/* Receive scanline, byte-compatible with ScanlineRxParameters3D (SupraLib/USImageProperties.h:43-95),
+ * so a std::vector<ScanlineRxParameters3D> can be passed as-is. Positions in mm; direction in the
+ * reference's swapped axis order {lateral x, depth, elevation} (Beamformer/Beamformer.cpp:1062-1063). */
+typedef struct sb_scanline_rx {
+    double position[3];
+    double direction[3];
+    double tx_weights[4];
+    sb_tx_params tx[4];
+    double max_element_distance[2]; /* mm, used to normalise the receive window */
+} sb_scanline_rx;
+
+/* Receive geometry: what RxBeamformerParameters + USRawData hand to RxBeamformerCuda
+ * (Beamformer/RxBeamformerParameters.h:38-112, Beamformer/USRawData.h:24-80). */
+typedef struct sb_geometry {
+    uint32_t num_elements;        /* transducer elements */
+    uint32_t element_layout[2];   /* x, y; 2D probes have y = 1 */
+    uint32_t num_channels;        /* received channels per transmit */
+    uint32_t num_samples;         /* samples per channel */
+    uint32_t num_tx;              /* transmit events (rows of the raw data) */
+    uint32_t num_rx;              /* receive scanlines = rx_layout[0] * rx_layout[1] */
+    uint32_t rx_layout[2];        /* x, y; 3D when both > 1 */
+    uint32_t num_depths;          /* receive depths per scanline */
+    double sampling_frequency_hz; /* dt = 1 / fs */
+    const float* element_x_mm;    /* [num_elements] element centre x (RxBeamformerParameters m_rxElementXs) */
+    const float* element_y_mm;    /* [num_elements] element centre elevation (m_rxElementYs) */
+    const float* depths_mm;       /* [num_depths]   receive depths (m_rxDepths) */
+    const sb_scanline_rx* scanlines;      /* [num_rx] */
+    const int32_t* element_to_channel;    /* optional [num_elements]; -1 = not connected; NULL = e % num_channels */
+} sb_geometry;
+
+/* ---------------------------------------------------------------- window + FIR design (host) */
+
+/* 64-entry (or n-entry) receive window LUT normalised to its maximum (Beamformer/WindowFunction.cpp:18-49). */
+int sb_window_lut(int window_type, float window_parameter, uint32_t num_entries, float* out_host);
+
+/* FIR design by the window method; type: 0 low-pass, 1 high-pass, 2 band-pass, 3 Hilbert;
+ * window: 0 rectangular, 1 Hann, 2 Hamming, 3 Kaiser (SupraLib/utilities/FirFilterFactory.h:58-230). */
+int sb_fir_design(uint32_t length, int type, int window, double sampling_frequency, double frequency,
+                  double bandwidth, float* out_host);
+
+/* ---------------------------------------------------------------- delay-and-sum */
+
+typedef struct sb_das_plan sb_das_plan;
+
+/* Replaces RxBeamformerCuda(const RxBeamformerParameters&) (Beamformer/RxBeamformerCuda.cu:24-52):
+ * copies the geometry to the device. Host pointers in `geometry` are read during the call only. */
+int sb_das_plan_create(const sb_geometry* geometry, sb_das_plan** plan);
+int sb_das_plan_destroy(sb_das_plan* plan);
+
+/* Replaces RxBeamformerCuda::performRxBeamforming<ChannelDataType, ImageDataType>
+ * (Beamformer/RxBeamformerCuda.cu:540-663) with sampleBeamformer = DelayAndSum.
+ * rf: [num_tx][num_channels][num_samples] (SB_INT16 or SB_FLOAT32).
+ * out: [num_depths][num_rx] (SB_FLOAT32 or SB_INT16, clamped as clampCast).
+ * The speed of sound is an argument: no host round trip of the geometry when it changes
+ * (RxBeamformerCuda.cu:58-107 copies every buffer D->H->D). 2D or 3D is chosen from rx_layout. */
+int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out, int out_dtype,
+               double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
+               int interpolate_transmits, int32_t additional_offset, sb_stream stream);
+
+/* Replaces RawDelay::performDelay (Beamformer/RawDelay.cu:556-650): delayed, apodised and weight-
+ * normalised channel samples, out [num_rx][num_channels][num_depths]; slots beyond the active
+ * aperture are written as 0. */
+int sb_rawdelay_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out, int out_dtype,
+                    double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
+                    sb_stream stream);
+
+/* ---------------------------------------------------------------- envelope, log, IQ */
+
+typedef struct sb_hilbert_plan sb_hilbert_plan;
+
+/* Replaces HilbertFirEnvelope(filterLength) (Beamformer/HilbertFirEnvelope.cu:63-82). */
+int sb_hilbert_plan_create(uint32_t filter_length, sb_hilbert_plan** plan);
+int sb_hilbert_plan_destroy(sb_hilbert_plan* plan);
+/* Replaces HilbertFirEnvelope::demodulate (HilbertFirEnvelope.cu:84-104): env = sqrt(x^2 + (h*x)^2).
+ * in/out [num_samples][num_scanlines]. Even filter lengths read one tap past the end in the
+ * reference; here that tap is 0. */
+int sb_hilbert_env_run(const sb_hilbert_plan* plan, const void* in, int in_dtype, void* out, int out_dtype,
+                       uint32_t num_scanlines, uint32_t num_samples, sb_stream stream);
+
+/* Replaces LogCompressor::compress (Beamformer/LogCompressor.cu:44-66). */
+int sb_logcompress_run(const void* in, int in_dtype, void* out, int out_dtype, size_t num_values,
+                       double dynamic_range_db, double gain, double in_max, sb_stream stream);
+
+typedef struct sb_iq_plan sb_iq_plan;
+/* Replaces IQDemodulator(fs, fref, cutoff, lowpassLength, bandpassLength) (Beamformer/IQDemodulator.cu:177-202)
+ * plus the frequency-compounding list of IQDemodulatorNode (Beamformer/IQDemodulatorNode.cpp:126-165).
+ * reference_frequencies / bandwidths / weights have num_filters entries (<= 8); entry 0 is the
+ * unfiltered signal, entries >= 1 use Kaiser band-passes. */
+int sb_iq_plan_create(double sampling_frequency, double cutoff_frequency, uint32_t lowpass_filter_length,
+                      uint32_t bandpass_filter_length, uint32_t num_filters,
+                      const double* reference_frequencies, const double* bandwidths, const double* weights,
+                      sb_iq_plan** plan);
+int sb_iq_plan_destroy(sb_iq_plan* plan);
+/* Replaces IQDemodulator::demodulateMagnitudeFrequencyCompounding (IQDemodulator.cu:215-345):
+ * real magnitude output [num_samples / decimation][num_scanlines]. */
+int sb_iq_magnitude_run(const sb_iq_plan* plan, const void* in, int in_dtype, void* out, int out_dtype,
+                        uint32_t num_scanlines, uint32_t num_samples, uint32_t decimation, sb_stream stream);
+
+/* Extension without a reference counterpart: complex baseband IQ. Mixes with exp(-j 2 pi f n / fs),
+ * low-passes with a Hamming-window FIR of lowpass_length taps (cutoff `cutoff_frequency`) and keeps
+ * every `decimation`-th sample. out: SB_COMPLEX64 [num_samples / decimation][num_scanlines]. */
+int sb_iq_complex_run(const void* in, int in_dtype, void* out, uint32_t num_scanlines, uint32_t num_samples,
+                      double sampling_frequency, double mixing_frequency, double cutoff_frequency,
+                      uint32_t lowpass_length, uint32_t decimation, sb_stream stream);
+
+/* ---------------------------------------------------------------- scan conversion */
+
+typedef struct sb_scan_plan sb_scan_plan;
+
+/* Replaces ScanConverter::updateInternals (Beamformer/ScanConverter.cu:513-815). scanlines is the
+ * layout_x x layout_y grid of the reference's (*scanlines)[x][y], flattened with x fastest
+ * (index x + y * layout_x, the order of sb_geometry.scanlines). depth_mm is the image depth,
+ * num_samples the samples per scanline. Tables are built on the host (2D, double precision,
+ * serial order: on a shared scanline edge the higher quad index wins) or on the device (3D). */
+int sb_scan_plan_create(const sb_scanline_rx* scanlines, uint32_t layout_x, uint32_t layout_y,
+                        uint32_t num_samples, double depth_mm, double resolution_mm, sb_scan_plan** plan);
+int sb_scan_plan_destroy(sb_scan_plan* plan);
+int sb_scan_image_size(const sb_scan_plan* plan, uint32_t size_xyz[3]);
+/* Host-only 2D table build (no device memory touched): size_xyz receives the image size; when all
+ * table pointers are non-NULL they are filled (each size_x * size_y entries). Same tables as
+ * sb_scan_plan_create builds for 2D layouts. */
+int sb_scan_tables_2d_host(const sb_scanline_rx* scanlines, uint32_t layout_x, uint32_t num_samples, double depth_mm,
+                           double resolution_mm, uint32_t size_xyz[3], uint8_t* mask, uint32_t* sample_idx,
+                           float* weight_x, float* weight_y);
+/* Host copies of the mask / sampleIdx / weightX / weightY / weightZ tables (any pointer may be NULL). */
+int sb_scan_copy_tables(const sb_scan_plan* plan, uint8_t* mask, uint32_t* sample_idx, float* weight_x,
+                        float* weight_y, float* weight_z);
+/* Replaces ScanConverter::convert (ScanConverter.cu:436-495): in [num_samples][scanlines] -> image. */
+int sb_scan_run(const sb_scan_plan* plan, const void* in, int in_dtype, void* out, int out_dtype,
+                sb_stream stream);
+
+/* Fused HilbertFirEnvelope -> LogCompressor -> ScanConverter (2D or 3D): FP32 RF [num_samples][scanlines]
+ * in, image out (SB_UINT8 or SB_FLOAT32). No envelope or log image is written to HBM. */
+int sb_env_log_scan_run(const sb_hilbert_plan* hilbert, const sb_scan_plan* scan, const float* rf,
+                        void* out, int out_dtype, double dynamic_range_db, double gain, double in_max,
+                        sb_stream stream);
+
+/* ---------------------------------------------------------------- minimum variance */
+
+typedef struct sb_mv_stats {
+    uint64_t systems;        /* linear systems solved */
+    uint64_t fp64_systems;   /* systems re-solved in FP64 (condition estimate above threshold) */
+    float max_condition_estimate;
+} sb_mv_stats;
+
+/* Replaces RxBeamformerMV::performRxBeamforming (Beamformer/RxBeamformerMV.cu:382-622).
+ * raw_delayed: [num_scanlines][num_channels][num_samples] as written by sb_rawdelay_run
+ *   (SB_FLOAT32 real, or SB_COMPLEX64 for the complex extension).
+ * out: [num_samples][num_scanlines] (SB_FLOAT32 / SB_INT16 real, SB_COMPLEX64 for complex input).
+ * subarray_size 0 means num_channels / 2 (as the reference). loading_scale multiplies the reference's
+ * diagonal loading trace(R)/L (1.0 = reference). Systems whose Cholesky condition estimate exceeds
+ * fp64_threshold are solved again in FP64 (<= 0 disables). stats_device may be NULL. */
+int sb_mv_run(const void* raw_delayed, int in_dtype, void* out, int out_dtype, uint32_t num_scanlines,
+              uint32_t num_channels, uint32_t num_samples, uint32_t subarray_size, uint32_t temporal_smoothing,
+              double subarray_scaling_power, int compute_means, float loading_scale, float fp64_threshold,
+              sb_mv_stats* stats_host, sb_stream stream);
+
+/* ---------------------------------------------------------------- batched, graph-captured DAS + IQ */
+
+typedef struct sb_batch_plan sb_batch_plan;
+
+typedef struct sb_batch_frame {
+    const sb_das_plan* probe;  /* geometry of this frame's probe (plans may be shared) */
+    const void* rf;            /* device [num_tx][num_channels][num_samples] int16 */
+    void* iq_out;              /* device complex64 [num_depths / decimation][num_rx] */
+} sb_batch_frame;
+
+typedef struct sb_batch_params {
+    double f_number;
+    double speed_of_sound_mm_s;
+    int window_type;
+    float window_parameter;
+    double mixing_frequency_hz;
+    double cutoff_frequency_hz;
+    uint32_t lowpass_length;   /* taps of the decimation low-pass */
+    uint32_t decimation;
+    int32_t lines_per_item;    /* tile shape: scanlines per work item (0 = autotuned / default) */
+    int32_t depth_tile;        /* tile shape: depths per chunk (0 = autotuned / default) */
+} sb_batch_params;
+
+/* Persistent batched DAS + complex IQ over frames of uneven probes in one launch. */
+int sb_batch_plan_create(const sb_batch_frame* frames, uint32_t num_frames, const sb_batch_params* params,
+                         sb_batch_plan** plan);
+int sb_batch_plan_destroy(sb_batch_plan* plan);
+/* Enqueue one batch. use_graph != 0 replays a captured CUDA graph of the launch sequence. */
+int sb_batch_run(sb_batch_plan* plan, int use_graph, sb_stream stream);
+/* Optional: write the fused per-frame RF (FP32 [num_depths][num_rx]) too; pass NULL to disable. */
+int sb_batch_set_rf_outputs(sb_batch_plan* plan, float* const* rf_out);
+/* Time candidate tile shapes on the device and keep the fastest; cache_path (may be NULL) stores
+ * the choice per problem signature. Returns the chosen shape. */
+int sb_batch_autotune(sb_batch_plan* plan, const char* cache_path, int32_t* lines_per_item, int32_t* depth_tile,
+                      sb_stream stream);
+
+/* ---------------------------------------------------------------- adjoint DAS */
+
+/* Extension without a reference counterpart. Forward with per-element apodisation:
+ *   s = sum_e apod[e] w_e lerp(rf_e, tau_e(c)) / sum_e apod[e] w_e * n_active
+ * (apod == NULL means 1, which equals sb_das_run). FP32 rf [num_tx][num_channels][num_samples]. */
+int sb_das_forward_apod(const sb_das_plan* plan, const float* rf, const float* apod, float* out,
+                        double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
+                        sb_stream stream);
+/* Adjoint of sb_das_forward_apod: given grad_out [num_depths][num_rx] accumulates into grad_rf
+ * (same shape as rf; may be NULL), grad_apod [num_elements] (may be NULL) and grad_c (one float,
+ * derivative w.r.t. the speed of sound in mm/s; may be NULL). Outputs are overwritten, not accumulated. */
+int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, const float* grad_out,
+                   float* grad_rf, float* grad_apod, float* grad_c, double f_number, double speed_of_sound_mm_s,
+                   int window_type, float window_parameter, sb_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SUPRA_B200_H */

@@ -1,0 +1,233 @@
+"""ORACLE — test infrastructure only.
+
+ctypes wrapper of oracle/liboracle.so (the CPU restatement of SUPRA's receive kernels) and of
+oracle/_ref/libsupra_ref.so (the reference's own sources compiled for the CPU, used to pin the
+restatement). Imported only by tests/, __graft_entry__.smoke() and bench.py's CPU baseline /
+reference arm; the product path never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional, Sequence
+
+import numpy as np
+
+from supra_b200.abi import sb_geometry, SB_FLOAT32, SB_INT16, SB_UINT8
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libsupra_ref.so")
+
+_vp = C.c_void_p
+_lib = None
+_ref = None
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle (and the reference checker when the reference sources are present)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "all"])
+    if ref and os.path.isdir("/root/reference/src/SupraLib"):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build(ref=False)
+        _lib = C.CDLL(LIB)
+        _lib.orc_window_get.restype = C.c_float
+        _lib.orc_window_get.argtypes = [C.c_int, C.c_float, C.c_uint32, C.c_float]
+    return _lib
+
+
+def ref_lib() -> Optional[C.CDLL]:
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            return None
+        _ref = C.CDLL(REF_LIB)
+        _ref.ref_window_get.restype = C.c_float
+        _ref.ref_window_get.argtypes = [C.c_int, C.c_float, C.c_uint32, C.c_float]
+    return _ref
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def nthreads() -> int:
+    return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------------------ design helpers
+def window_lut(window_type: int, param: float = 0.0, n: int = 64, ref: bool = False) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    L = ref_lib() if ref else lib()
+    fn = L.ref_window_lut if ref else L.orc_window_lut
+    fn(C.c_int(window_type), C.c_float(param), C.c_uint32(n), _vp(_p(out)))
+    return out
+
+
+def window_get(window_type: int, param: float, n: int, rel: float, ref: bool = False) -> float:
+    if ref:
+        return ref_lib().ref_window_get(window_type, param, n, rel)
+    return lib().orc_window_get(window_type, param, n, rel)
+
+
+def fir(length: int, ftype: int, window: int, fs: float = 2.0, f: float = 0.0, bw: float = 0.0,
+        ref: bool = False) -> np.ndarray:
+    out = np.zeros(length, np.float32)
+    L = ref_lib() if ref else lib()
+    fn = L.ref_fir if ref else L.orc_fir
+    fn(C.c_uint32(length), C.c_int(ftype), C.c_int(window), C.c_double(fs), C.c_double(f), C.c_double(bw),
+       _vp(_p(out)))
+    return out
+
+
+# ------------------------------------------------------------------------------ kernels
+def das(geom, rf: np.ndarray, f_number=1.0, c_mm_s=None, window=1, window_param=0.0, interp_tx=False,
+        additional_offset=0, precision=32, apod: Optional[np.ndarray] = None, threads=None,
+        ref: bool = False) -> np.ndarray:
+    """DAS of one frame; rf [num_tx][num_channels][num_samples] (any dtype, converted to float32)."""
+    g = geom.ctypes()
+    rf32 = np.ascontiguousarray(rf, dtype=np.float32)
+    c = geom.speed_of_sound_mm_s if c_mm_s is None else c_mm_s
+    n = geom.num_depths * geom.num_rx
+    if ref:
+        out = np.full(n, np.nan, np.float32)
+        ref_lib().ref_das(C.byref(g), _vp(_p(rf32)), _vp(_p(out)), C.c_double(f_number), C.c_double(c),
+                          C.c_int(window), C.c_float(window_param), C.c_int(int(interp_tx)),
+                          C.c_int32(additional_offset))
+        return out.reshape(geom.num_depths, geom.num_rx)
+    if precision == 64:
+        out64 = np.full(n, np.nan, np.float64)
+        outp32, outp64 = None, _vp(_p(out64))
+    else:
+        out32 = np.full(n, np.nan, np.float32)
+        outp32, outp64 = _vp(_p(out32)), None
+    ap = None if apod is None else np.ascontiguousarray(apod, dtype=np.float32)
+    st = lib().orc_das(C.byref(g), _vp(_p(rf32)), outp32, outp64, C.c_double(f_number), C.c_double(c),
+                       C.c_int(window), C.c_float(window_param), C.c_int(int(interp_tx)), C.c_int32(additional_offset),
+                       None if ap is None else _vp(_p(ap)), C.c_int(precision), C.c_int(threads or nthreads()))
+    assert st == 0
+    out = out64 if precision == 64 else out32
+    return out.reshape(geom.num_depths, geom.num_rx)
+
+
+def rawdelay(geom, rf: np.ndarray, f_number=1.0, c_mm_s=None, window=1, window_param=0.0, threads=None):
+    g = geom.ctypes()
+    rf32 = np.ascontiguousarray(rf, dtype=np.float32)
+    c = geom.speed_of_sound_mm_s if c_mm_s is None else c_mm_s
+    out = np.zeros(geom.num_rx * geom.num_channels * geom.num_depths, np.float32)
+    st = lib().orc_rawdelay(C.byref(g), _vp(_p(rf32)), _vp(_p(out)), C.c_double(f_number), C.c_double(c),
+                            C.c_int(window), C.c_float(window_param), C.c_int(threads or nthreads()))
+    assert st == 0
+    return out.reshape(geom.num_rx, geom.num_channels, geom.num_depths)
+
+
+def hilbert_env(x: np.ndarray, filter_length: int, threads=None) -> np.ndarray:
+    """x [num_samples][num_scanlines] float32."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.zeros_like(x)
+    lib().orc_hilbert_env(_vp(_p(x)), _vp(_p(out)), C.c_uint32(x.shape[1]), C.c_uint32(x.shape[0]),
+                          C.c_uint32(filter_length), C.c_int(threads or nthreads()))
+    return out
+
+
+def logcompress(x: np.ndarray, dynamic_range: float, gain: float, in_max: float, out_dtype=np.uint8) -> np.ndarray:
+    x = np.ascontiguousarray(x)
+    in_code = SB_INT16 if x.dtype == np.int16 else SB_UINT8 if x.dtype == np.uint8 else SB_FLOAT32
+    if in_code == SB_FLOAT32:
+        x = x.astype(np.float32, copy=False)
+    out = np.zeros(x.shape, out_dtype)
+    oc = SB_UINT8 if out_dtype == np.uint8 else SB_FLOAT32
+    lib().orc_logcompress(_vp(_p(x)), C.c_int(in_code), _vp(_p(out)), C.c_int(oc), C.c_size_t(x.size),
+                          C.c_double(dynamic_range), C.c_double(gain), C.c_double(in_max))
+    return out
+
+
+def iq_magnitude(x: np.ndarray, decimation: int, fs: float, cutoff: float, lp_len: int, bp_len: int,
+                 ref_freqs: Sequence[float], bandwidths: Sequence[float], weights: Sequence[float], threads=None):
+    x = np.ascontiguousarray(x, np.float32)
+    nS, nL = x.shape
+    n_out = nS // decimation if decimation > 1 else nS
+    out = np.zeros((n_out, nL), np.float32)
+    rf_ = np.ascontiguousarray(ref_freqs, np.float64)
+    bw_ = np.ascontiguousarray(bandwidths, np.float64)
+    w_ = np.ascontiguousarray(weights, np.float64)
+    st = lib().orc_iq_magnitude(_vp(_p(x)), _vp(_p(out)), C.c_uint32(nL), C.c_uint32(nS), C.c_uint32(decimation),
+                                C.c_double(fs), C.c_double(cutoff), C.c_uint32(lp_len), C.c_uint32(bp_len),
+                                C.c_uint32(len(rf_)), _vp(_p(rf_)), _vp(_p(bw_)), _vp(_p(w_)),
+                                C.c_int(threads or nthreads()))
+    assert st == 0
+    return out
+
+
+def iq_complex(x: np.ndarray, fs: float, fmix: float, cutoff: float, lp_len: int, decimation: int, threads=None):
+    x = np.ascontiguousarray(x, np.float32)
+    nS, nL = x.shape
+    out = np.zeros((nS // decimation, nL, 2), np.float64)
+    lib().orc_iq_complex(_vp(_p(x)), _vp(_p(out)), C.c_uint32(nL), C.c_uint32(nS), C.c_double(fs), C.c_double(fmix),
+                         C.c_double(cutoff), C.c_uint32(lp_len), C.c_uint32(decimation), C.c_int(threads or nthreads()))
+    return out[..., 0] + 1j * out[..., 1]
+
+
+def scan_tables(scanlines: np.ndarray, lx: int, ly: int, num_samples: int, depth: float, resolution: float):
+    size = np.zeros(3, np.uint32)
+    bb = np.zeros(3, np.float64)
+    sl = np.ascontiguousarray(scanlines)
+    L = lib()
+    L.orc_scan_tables(_vp(_p(sl)), C.c_uint32(lx), C.c_uint32(ly), C.c_uint32(num_samples), C.c_double(depth),
+                      C.c_double(resolution), _vp(_p(size)), _vp(_p(bb)), None, None, None, None, None)
+    n = int(size[0]) * int(size[1]) * int(size[2])
+    mask = np.zeros(n, np.uint8)
+    sidx = np.zeros(n, np.uint32)
+    wx = np.zeros(n, np.float32)
+    wy = np.zeros(n, np.float32)
+    wz = np.zeros(n, np.float32)
+    L.orc_scan_tables(_vp(_p(sl)), C.c_uint32(lx), C.c_uint32(ly), C.c_uint32(num_samples), C.c_double(depth),
+                      C.c_double(resolution), _vp(_p(size)), _vp(_p(bb)), _vp(_p(mask)), _vp(_p(sidx)),
+                      _vp(_p(wx)), _vp(_p(wy)), _vp(_p(wz)))
+    return dict(size=tuple(int(v) for v in size), bb_min=bb, mask=mask, sample_idx=sidx, weight_x=wx,
+                weight_y=wy, weight_z=wz)
+
+
+def scan_apply(x: np.ndarray, lx: int, ly: int, tables: dict, out_dtype=np.uint8) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float32)
+    size = np.array(tables["size"], np.uint32)
+    n = int(np.prod(size))
+    out = np.zeros(n, out_dtype)
+    oc = SB_UINT8 if out_dtype == np.uint8 else SB_INT16 if out_dtype == np.int16 else SB_FLOAT32
+    lib().orc_scan_apply(_vp(_p(x)), C.c_uint32(lx), C.c_uint32(ly), C.c_uint32(x.shape[0]), _vp(_p(size)),
+                         _vp(_p(tables["mask"])), _vp(_p(tables["sample_idx"])), _vp(_p(tables["weight_x"])),
+                         _vp(_p(tables["weight_y"])), _vp(_p(tables["weight_z"])), _vp(_p(out)), C.c_int(oc))
+    return out.reshape(size[2], size[1], size[0])
+
+
+def mv(raw: np.ndarray, L: int, T: int, scaling_power=1.5, loading_scale=1.0, precision=32, block=2000,
+       threads=None) -> np.ndarray:
+    """raw [nRx][nCh][nS] float32 (real) or complex64; returns [nS][nRx]."""
+    iscomplex = np.iscomplexobj(raw)
+    nRx, nCh, nS = raw.shape
+    if iscomplex:
+        r = np.ascontiguousarray(raw.astype(np.complex64)).view(np.float32)
+    else:
+        r = np.ascontiguousarray(raw, np.float32)
+    if precision == 64:
+        out = np.zeros(nS * nRx * (2 if iscomplex else 1), np.float64)
+        st = lib().orc_mv(_vp(_p(r)), C.c_int(int(iscomplex)), None, _vp(_p(out)), C.c_uint32(nRx), C.c_uint32(nCh),
+                          C.c_uint32(nS), C.c_uint32(L), C.c_uint32(T), C.c_double(scaling_power),
+                          C.c_float(loading_scale), C.c_int(64), C.c_uint32(block), C.c_int(threads or nthreads()))
+    else:
+        out = np.zeros(nS * nRx * (2 if iscomplex else 1), np.float32)
+        st = lib().orc_mv(_vp(_p(r)), C.c_int(int(iscomplex)), _vp(_p(out)), None, C.c_uint32(nRx), C.c_uint32(nCh),
+                          C.c_uint32(nS), C.c_uint32(L), C.c_uint32(T), C.c_double(scaling_power),
+                          C.c_float(loading_scale), C.c_int(32), C.c_uint32(block), C.c_int(threads or nthreads()))
+    assert st == 0
+    if iscomplex:
+        out = out.reshape(nS, nRx, 2)
+        return out[..., 0] + 1j * out[..., 1]
+    return out.reshape(nS, nRx)

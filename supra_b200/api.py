@@ -1,0 +1,284 @@
+"""Python binding of the C ABI over torch device tensors.
+
+Mirrors the reference's algorithm classes (RxBeamformerCuda, RawDelay, HilbertFirEnvelope,
+LogCompressor, IQDemodulator, ScanConverter, RxBeamformerMV): the same constructor arguments and
+per-call parameters, device buffers in and out, launched on the current torch stream. Every call
+goes through libsupra_b200.so; there is no other implementation behind these classes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import abi
+from .abi import (SB_COMPLEX64, SB_FLOAT32, SB_INT16, SB_UINT8, SB_UINT16, check, load_library, sb_geometry,
+                  sb_mv_stats)
+
+_DT = {torch.int16: SB_INT16, torch.float32: SB_FLOAT32, torch.uint8: SB_UINT8, torch.complex64: SB_COMPLEX64}
+_TORCH = {SB_INT16: torch.int16, SB_FLOAT32: torch.float32, SB_UINT8: torch.uint8, SB_COMPLEX64: torch.complex64}
+
+
+def _stream() -> C.c_void_p:
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[C.c_void_p]:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("supra_b200 kernels take CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("tensor must be contiguous")
+    return C.c_void_p(t.data_ptr())
+
+
+def dtype_code(t: torch.Tensor) -> int:
+    try:
+        return _DT[t.dtype]
+    except KeyError:
+        raise ValueError(f"unsupported dtype {t.dtype}") from None
+
+
+class RxBeamformer:
+    """RxBeamformerCuda (Beamformer/RxBeamformerCuda.cu:24-663), DelayAndSum, 2D or 3D."""
+
+    def __init__(self, geometry):
+        self.lib = load_library()
+        self.geometry = geometry
+        g = geometry.ctypes()
+        self._plan = C.c_void_p()
+        check("sb_das_plan_create", self.lib.sb_das_plan_create(C.byref(g), C.byref(self._plan)))
+
+    def __del__(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            self.lib.sb_das_plan_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._plan
+
+    def beamform(self, rf: torch.Tensor, f_number=1.0, speed_of_sound_mm_s=None, window_type=1, window_parameter=0.0,
+                 interpolate_transmits=False, additional_offset=0, out_dtype=torch.float32,
+                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        g = self.geometry
+        c = g.speed_of_sound_mm_s if speed_of_sound_mm_s is None else speed_of_sound_mm_s
+        if out is None:
+            out = torch.empty((g.num_depths, g.num_rx), dtype=out_dtype, device=rf.device)
+        check("sb_das_run", self.lib.sb_das_run(self._plan, _ptr(rf), dtype_code(rf), _ptr(out), dtype_code(out),
+                                                float(f_number), float(c), int(window_type), float(window_parameter),
+                                                int(bool(interpolate_transmits)), int(additional_offset), _stream()))
+        return out
+
+    def raw_delay(self, rf: torch.Tensor, f_number=1.0, speed_of_sound_mm_s=None, window_type=1, window_parameter=0.0,
+                  out_dtype=torch.float32) -> torch.Tensor:
+        """RawDelay::performDelay (Beamformer/RawDelay.cu:556-650): [num_rx][num_channels][num_depths]."""
+        g = self.geometry
+        c = g.speed_of_sound_mm_s if speed_of_sound_mm_s is None else speed_of_sound_mm_s
+        out = torch.empty((g.num_rx, g.num_channels, g.num_depths), dtype=out_dtype, device=rf.device)
+        check("sb_rawdelay_run", self.lib.sb_rawdelay_run(self._plan, _ptr(rf), dtype_code(rf), _ptr(out),
+                                                          dtype_code(out), float(f_number), float(c), int(window_type),
+                                                          float(window_parameter), _stream()))
+        return out
+
+
+class HilbertFirEnvelope:
+    """HilbertFirEnvelope(filterLength) (Beamformer/HilbertFirEnvelope.cu:63-104)."""
+
+    def __init__(self, filter_length: int = 65):
+        self.lib = load_library()
+        self._plan = C.c_void_p()
+        check("sb_hilbert_plan_create", self.lib.sb_hilbert_plan_create(int(filter_length), C.byref(self._plan)))
+
+    def __del__(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            self.lib.sb_hilbert_plan_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    @property
+    def handle(self):
+        return self._plan
+
+    def demodulate(self, img: torch.Tensor) -> torch.Tensor:
+        nS, nL = img.shape
+        out = torch.empty((nS, nL), dtype=torch.float32, device=img.device)
+        check("sb_hilbert_env_run", self.lib.sb_hilbert_env_run(self._plan, _ptr(img), dtype_code(img), _ptr(out),
+                                                                SB_FLOAT32, nL, nS, _stream()))
+        return out
+
+
+class LogCompressor:
+    """LogCompressor::compress (Beamformer/LogCompressor.cu:44-66)."""
+
+    def __init__(self):
+        self.lib = load_library()
+
+    def compress(self, img: torch.Tensor, dynamic_range=80.0, gain=1.0, in_max=1024.0,
+                 out_dtype=torch.float32) -> torch.Tensor:
+        out = torch.empty(img.shape, dtype=out_dtype, device=img.device)
+        check("sb_logcompress_run", self.lib.sb_logcompress_run(_ptr(img), dtype_code(img), _ptr(out), dtype_code(out),
+                                                                img.numel(), float(dynamic_range), float(gain),
+                                                                float(in_max), _stream()))
+        return out
+
+
+class IQDemodulator:
+    """IQDemodulator + IQDemodulatorNode's frequency-compounding list (Beamformer/IQDemodulator.cu,
+    Beamformer/IQDemodulatorNode.cpp:126-165)."""
+
+    def __init__(self, sampling_frequency=40e6, cutoff_frequency=2.5e6, lowpass_filter_length=51,
+                 bandpass_filter_length=51, reference_frequencies: Sequence[float] = (7e6,),
+                 bandwidths: Sequence[float] = (1e6,), weights: Sequence[float] = (1.0,)):
+        self.lib = load_library()
+        self.fs = sampling_frequency
+        self.cutoff = cutoff_frequency
+        rf = np.ascontiguousarray(reference_frequencies, np.float64)
+        bw = np.ascontiguousarray(bandwidths, np.float64)
+        w = np.ascontiguousarray(weights, np.float64)
+        self._plan = C.c_void_p()
+        check("sb_iq_plan_create", self.lib.sb_iq_plan_create(float(sampling_frequency), float(cutoff_frequency),
+                                                              int(lowpass_filter_length), int(bandpass_filter_length),
+                                                              len(rf), rf.ctypes.data, bw.ctypes.data, w.ctypes.data,
+                                                              C.byref(self._plan)))
+
+    def __del__(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            self.lib.sb_iq_plan_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    @staticmethod
+    def decimated_length(num_samples: int, decimation: int) -> int:
+        return num_samples // decimation if decimation > 1 else num_samples
+
+    def demodulate_magnitude(self, img: torch.Tensor, decimation: int = 8, out_dtype=torch.float32) -> torch.Tensor:
+        nS, nL = img.shape
+        out = torch.empty((self.decimated_length(nS, decimation), nL), dtype=out_dtype, device=img.device)
+        check("sb_iq_magnitude_run", self.lib.sb_iq_magnitude_run(self._plan, _ptr(img), dtype_code(img), _ptr(out),
+                                                                  dtype_code(out), nL, nS, int(decimation), _stream()))
+        return out
+
+
+def iq_complex(img: torch.Tensor, sampling_frequency: float, mixing_frequency: float, cutoff_frequency: float,
+               lowpass_length: int, decimation: int) -> torch.Tensor:
+    """Complex baseband IQ (extension): [num_samples / decimation][num_scanlines] complex64."""
+    lib = load_library()
+    nS, nL = img.shape
+    out = torch.empty((nS // max(decimation, 1), nL), dtype=torch.complex64, device=img.device)
+    check("sb_iq_complex_run", lib.sb_iq_complex_run(_ptr(img), dtype_code(img), _ptr(out), nL, nS,
+                                                     float(sampling_frequency), float(mixing_frequency),
+                                                     float(cutoff_frequency), int(lowpass_length), int(decimation),
+                                                     _stream()))
+    return out
+
+
+class ScanConverter:
+    """ScanConverter (Beamformer/ScanConverter.cu:436-815). `scanlines` is the SCANLINE_DTYPE array of
+    the receive geometry (x fastest)."""
+
+    def __init__(self, scanlines: np.ndarray, layout, num_samples: int, depth_mm: float, resolution_mm: float):
+        self.lib = load_library()
+        self.layout = tuple(int(v) for v in layout)
+        sl = np.ascontiguousarray(scanlines)
+        self._plan = C.c_void_p()
+        check("sb_scan_plan_create", self.lib.sb_scan_plan_create(sl.ctypes.data, self.layout[0], self.layout[1],
+                                                                  int(num_samples), float(depth_mm),
+                                                                  float(resolution_mm), C.byref(self._plan)))
+        size = (C.c_uint32 * 3)()
+        check("sb_scan_image_size", self.lib.sb_scan_image_size(self._plan, size))
+        self.image_size = (int(size[0]), int(size[1]), int(size[2]))
+
+    def __del__(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            self.lib.sb_scan_plan_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    @property
+    def handle(self):
+        return self._plan
+
+    @property
+    def numel(self) -> int:
+        return self.image_size[0] * self.image_size[1] * self.image_size[2]
+
+    def tables(self) -> dict:
+        n = self.numel
+        mask = np.zeros(n, np.uint8)
+        sidx = np.zeros(n, np.uint32)
+        wx = np.zeros(n, np.float32)
+        wy = np.zeros(n, np.float32)
+        wz = np.zeros(n, np.float32)
+        check("sb_scan_copy_tables", self.lib.sb_scan_copy_tables(self._plan, mask.ctypes.data, sidx.ctypes.data,
+                                                                  wx.ctypes.data, wy.ctypes.data, wz.ctypes.data))
+        return dict(size=self.image_size, mask=mask, sample_idx=sidx, weight_x=wx, weight_y=wy, weight_z=wz)
+
+    def _shape(self):
+        W, H, D = self.image_size
+        return (D, H, W) if D > 1 else (H, W)
+
+    def convert(self, img: torch.Tensor, out_dtype=torch.uint8) -> torch.Tensor:
+        out = torch.empty(self._shape(), dtype=out_dtype, device=img.device)
+        check("sb_scan_run", self.lib.sb_scan_run(self._plan, _ptr(img), dtype_code(img), _ptr(out), dtype_code(out),
+                                                  _stream()))
+        return out
+
+    def env_log_convert(self, hilbert: HilbertFirEnvelope, rf: torch.Tensor, dynamic_range=80.0, gain=1.0,
+                        in_max=1024.0, out_dtype=torch.uint8) -> torch.Tensor:
+        """Fused HilbertFirEnvelope -> LogCompressor -> ScanConverter."""
+        out = torch.empty(self._shape(), dtype=out_dtype, device=rf.device)
+        check("sb_env_log_scan_run", self.lib.sb_env_log_scan_run(hilbert.handle, self._plan, _ptr(rf), _ptr(out),
+                                                                  dtype_code(out), float(dynamic_range), float(gain),
+                                                                  float(in_max), _stream()))
+        return out
+
+
+def scan_tables_2d_host(scanlines: np.ndarray, layout_x: int, num_samples: int, depth_mm: float, resolution_mm: float):
+    """Host-only 2D table build of the product (no GPU needed)."""
+    lib = load_library()
+    sl = np.ascontiguousarray(scanlines)
+    size = np.zeros(3, np.uint32)
+    check("sb_scan_tables_2d_host", lib.sb_scan_tables_2d_host(sl.ctypes.data, layout_x, num_samples, depth_mm,
+                                                               resolution_mm, size.ctypes.data, None, None, None, None))
+    n = int(size[0]) * int(size[1]) * int(size[2])
+    mask = np.zeros(n, np.uint8)
+    sidx = np.zeros(n, np.uint32)
+    wx = np.zeros(n, np.float32)
+    wy = np.zeros(n, np.float32)
+    check("sb_scan_tables_2d_host", lib.sb_scan_tables_2d_host(sl.ctypes.data, layout_x, num_samples, depth_mm,
+                                                               resolution_mm, size.ctypes.data, mask.ctypes.data,
+                                                               sidx.ctypes.data, wx.ctypes.data, wy.ctypes.data))
+    return dict(size=tuple(int(v) for v in size), mask=mask, sample_idx=sidx, weight_x=wx, weight_y=wy)
+
+
+def window_lut(window_type: int, window_parameter: float = 0.0, n: int = 64) -> np.ndarray:
+    lib = load_library()
+    out = np.zeros(n, np.float32)
+    check("sb_window_lut", lib.sb_window_lut(int(window_type), float(window_parameter), n, out.ctypes.data))
+    return out
+
+
+def fir_design(length: int, ftype: int, window: int, fs=2.0, f=0.0, bw=0.0) -> np.ndarray:
+    lib = load_library()
+    out = np.zeros(length, np.float32)
+    check("sb_fir_design", lib.sb_fir_design(int(length), int(ftype), int(window), float(fs), float(f), float(bw),
+                                             out.ctypes.data))
+    return out
+
+
+def mv_beamform(raw_delayed: torch.Tensor, subarray_size=0, temporal_smoothing=3, subarray_scaling_power=1.5,
+                compute_means=False, loading_scale=1.0, fp64_threshold=1e6, out_dtype=None):
+    """RxBeamformerMV::performRxBeamforming (Beamformer/RxBeamformerMV.cu:382-622).
+    raw_delayed [num_rx][num_channels][num_depths] float32 or complex64 -> ([num_depths][num_rx], stats)."""
+    lib = load_library()
+    nRx, nCh, nS = raw_delayed.shape
+    if out_dtype is None:
+        out_dtype = torch.complex64 if raw_delayed.dtype == torch.complex64 else torch.float32
+    out = torch.empty((nS, nRx), dtype=out_dtype, device=raw_delayed.device)
+    stats = sb_mv_stats()
+    check("sb_mv_run", lib.sb_mv_run(_ptr(raw_delayed), dtype_code(raw_delayed), _ptr(out), dtype_code(out), nRx, nCh,
+                                     nS, int(subarray_size), int(temporal_smoothing), float(subarray_scaling_power),
+                                     int(bool(compute_means)), float(loading_scale), float(fp64_threshold),
+                                     C.byref(stats), _stream()))
+    return out, stats

@@ -1,0 +1,462 @@
+// Delay-and-sum receive beamforming (2D and 3D) and the raw-delay stage, per frame.
+//
+// Semantics follow RxBeamformerCuda / RxSampleBeamformerDelayAndSum (Beamformer/RxBeamformerCuda.cu:119-323,
+// Beamformer/RxSampleBeamformerDelayAndSum.h:26-208) and RawDelay (Beamformer/RawDelay.cu:221-468).
+// The discrete decisions of the reference — aperture membership, the nearest window-LUT entry, the
+// sample index — are evaluated with the same IEEE float operations in the same order (explicit
+// _rn intrinsics, so nothing is contracted into FMAs), which keeps them bit-identical to the CPU
+// restatement of the reference.
+#include <cmath>
+#include <vector>
+
+#include "das.cuh"
+#include "design.h"
+
+namespace sb {
+
+WindowLut makeLut(int windowType, float windowParameter) {
+    WindowLut w;
+    std::vector<float> v = windowLut(windowType, windowParameter, 64);
+    for (int i = 0; i < 64; i++) w.v[i] = v[i];
+    return w;
+}
+
+namespace {
+
+// convertToDtSpace (RxBeamformerCuda.cu:58-107), first-call form: mm -> units of c*dt in double,
+// then rounded to float as the kernels read them.
+__global__ void dtConvertKernel(const float* xeMM, const float* yeMM, uint32_t nE, const float* dMM, uint32_t nD,
+                                const sb_scanline_rx* lines, uint32_t nRx, double factor, double factorTime,
+                                float* xe, float* ye, float* d, LineDT* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nE) {
+        xe[i] = static_cast<float>(static_cast<double>(xeMM[i]) * factor);
+        ye[i] = static_cast<float>(static_cast<double>(yeMM[i]) * factor);
+    }
+    if (i < nD) d[i] = static_cast<float>(static_cast<double>(dMM[i]) * factor);
+    if (i < nRx) {
+        const sb_scanline_rx& s = lines[i];
+        LineDT o;
+        o.x = static_cast<float>(s.position[0] * factor);
+        o.z = static_cast<float>(s.position[2] * factor);
+        o.dirX = static_cast<float>(s.direction[0]);
+        o.dirY = static_cast<float>(s.direction[1]);
+        o.dirZ = static_cast<float>(s.direction[2]);
+        o.maxDistX = static_cast<float>(s.max_element_distance[0] * factor);
+        o.maxDistY = static_cast<float>(s.max_element_distance[1] * factor);
+        int hi = 0;
+        float hw = static_cast<float>(s.tx_weights[0]);
+        int mask = 0;
+        for (int k = 0; k < 4; k++) {
+            o.txWeight[k] = static_cast<float>(s.tx_weights[k]);
+            o.initialDelay[k] = static_cast<float>(s.tx[k].initial_delay_s * factorTime);
+            o.firstX[k] = s.tx[k].first_active_element[0];
+            o.firstY[k] = s.tx[k].first_active_element[1];
+            o.lastX[k] = s.tx[k].last_active_element[0];
+            o.lastY[k] = s.tx[k].last_active_element[1];
+            o.txIdx[k] = s.tx[k].tx_scanline_idx;
+            if (s.tx_weights[k] > 0.0) mask |= 1 << k;
+            if (k > 0 && s.tx_weights[k] > static_cast<double>(hw)) {  // double vs promoted float, as the reference
+                hw = static_cast<float>(s.tx_weights[k]);
+                hi = k;
+            }
+        }
+        o.highest = hi;
+        o.activeMask = mask;
+        out[i] = o;
+    }
+}
+
+struct DasArgs {
+    const void* rf;
+    void* out;
+    const float* xe;
+    const float* ye;
+    const float* depth;
+    const LineDT* lines;
+    const int32_t* e2c;
+    const float* apod;
+    uint32_t nE, layoutX, nCh, nS, nTx, nRx, nD;
+    float c, dt, F, offset;
+    int interpTx;
+    WindowLut lut;
+};
+
+// WindowFunctionGpu::get (Beamformer/WindowFunction.h:58-64): nearest of 64 entries.
+__device__ __forceinline__ float lutGet(const float* lut, float rel) {
+    float cl = fminf(fmaxf(rel, -1.0f), 1.0f);
+    uint32_t idx = static_cast<uint32_t>(roundf(__fmul_rn(31.5f, __fadd_rn(cl, 1.0f))));
+    return lut[idx];
+}
+
+// computeAperture_D(F, d*dt*c)/c/dt (Beamformer/RxBeamformerCommon.h:21-25, RxBeamformerCuda.cu:263)
+__device__ __forceinline__ float apertureDT(float d, float dt, float c, float F) {
+    return __fdiv_rn(__fdiv_rn(__fdiv_rn(__fmul_rn(__fmul_rn(d, dt), c), __fmul_rn(2.0f, F)), c), dt);
+}
+
+template <typename RF>
+__device__ __forceinline__ float sample2D(const DasArgs& a, const LineDT& s, int k, const float* lut, float aDT,
+                                          float depth, float invMax) {
+    float sample = 0.0f, weightAcum = 0.0f;
+    int numAdds = 0;
+    const float iD = s.initialDelay[k];
+    const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
+    const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, depth));
+    const float dy = __fmul_rn(s.dirY, depth);
+    const float dy2 = __fmul_rn(dy, dy);
+    for (int e = s.firstX[k]; e < s.lastX[k]; e++) {
+        int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(static_cast<uint32_t>(e) % a.nCh);
+        if (ch < 0) continue;
+        const float xel = __ldg(a.xe + e);
+        const float dx = __fsub_rn(xel, s.x);
+        if (fabsf(dx) <= aDT) {
+            float w = lutGet(lut, __fmul_rn(dx, invMax));
+            if (a.apod) w = __fmul_rn(w, __ldg(a.apod + e));
+            weightAcum = __fadd_rn(weightAcum, w);
+            numAdds++;
+            const float ex = __fsub_rn(xel, xz);
+            const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2));
+            const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(dist, depth)), a.offset);
+            const int32_t delay = static_cast<int32_t>(floorf(delayf));
+            const float frac = __fsub_rn(delayf, static_cast<float>(delay));
+            const RF* p = tx + static_cast<size_t>(ch) * a.nS;
+            if (static_cast<uint32_t>(delay) < a.nS - 1) {
+                const float v0 = toFloat(p[delay]), v1 = toFloat(p[delay + 1]);
+                const float v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
+                sample = __fadd_rn(sample, __fmul_rn(w, v));
+            } else if (static_cast<uint32_t>(delay) < a.nS && frac == 0.0f) {
+                sample = __fadd_rn(sample, __fmul_rn(w, toFloat(p[delay])));
+            }
+        }
+    }
+    return numAdds > 0 ? __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds)) : 0.0f;
+}
+
+template <typename RF>
+__device__ __forceinline__ float sample3D(const DasArgs& a, const LineDT& s, int k, const float* lut, float aDT2,
+                                          float depth, float invX, float invY) {
+    float sample = 0.0f, weightAcum = 0.0f;
+    int numAdds = 0;
+    const float iD = s.initialDelay[k];
+    const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
+    const float px = __fadd_rn(s.x, __fmul_rn(s.dirX, depth));
+    const float pz = __fadd_rn(s.z, __fmul_rn(s.dirZ, depth));
+    const float ay = __fmul_rn(s.dirY, depth);
+    const float ay2 = __fmul_rn(ay, ay);
+    for (uint32_t ex = s.firstX[k]; ex < s.lastX[k]; ex++) {
+        for (uint32_t ey = s.firstY[k]; ey < s.lastY[k]; ey++) {
+            const uint32_t e = ex + ey * a.layoutX;
+            int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(e % a.nCh);
+            if (ch < 0) continue;
+            const float xel = __ldg(a.xe + e), zel = __ldg(a.ye + e);
+            const float dx = __fsub_rn(xel, s.x), dz = __fsub_rn(zel, s.z);
+            if (__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)) <= aDT2) {
+                const float w = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(dx, invX)), lutGet(lut, __fmul_rn(dz, invY))));
+                weightAcum = __fadd_rn(weightAcum, w);
+                numAdds++;
+                const float qx = __fsub_rn(xel, px), qz = __fsub_rn(zel, pz);
+                const float q = __fadd_rn(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qz, qz)), ay2);
+                const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(__fsqrt_rn(q), depth)), a.offset);
+                const uint32_t delay = static_cast<uint32_t>(floorf(delayf));  // saturates at 0 like the reference
+                const float frac = __fsub_rn(delayf, static_cast<float>(delay));
+                const RF* p = tx + static_cast<size_t>(ch) * a.nS;
+                if (delay < a.nS - 1) {
+                    const float v0 = toFloat(p[delay]), v1 = toFloat(p[delay + 1]);
+                    const float v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
+                    sample = __fadd_rn(sample, __fmul_rn(w, v));
+                } else if (delay < a.nS && frac == 0.0f) {
+                    sample = __fadd_rn(sample, __fmul_rn(w, toFloat(p[delay])));
+                }
+            }
+        }
+    }
+    return numAdds > 0 ? __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds)) : 0.0f;
+}
+
+// One thread per (scanline, depth); block = 256 consecutive depths of one scanline.
+template <typename RF, typename OUT, bool IS3D>
+__global__ void __launch_bounds__(256) dasKernel(DasArgs a) {
+    __shared__ float lut[64];
+    if (threadIdx.x < 64) lut[threadIdx.x] = a.lut.v[threadIdx.x];
+    __syncthreads();
+    const uint32_t line = blockIdx.y;
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nD) return;
+    const LineDT s = a.lines[line];
+    const float d = __ldg(a.depth + r);
+    float aDT = apertureDT(d, a.dt, a.c, a.F);
+    float invX = 0.0f, invY = 0.0f;
+    if (IS3D) {
+        aDT = __fmul_rn(aDT, aDT);
+        const float sq = __fsqrt_rn(aDT);
+        invX = __fdiv_rn(1.0f, fminf(sq, s.maxDistX));
+        invY = __fdiv_rn(1.0f, fminf(sq, s.maxDistY));
+    } else {
+        invX = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+    }
+    float acc = 0.0f;
+    for (int k = 0; k < 4; k++) {
+        if (!a.interpTx && k != s.highest) continue;
+        if (!((s.activeMask >> k) & 1)) continue;
+        const float v = IS3D ? sample3D<RF>(a, s, k, lut, aDT, d, invX, invY) : sample2D<RF>(a, s, k, lut, aDT, d, invX);
+        acc = a.interpTx ? __fadd_rn(acc, __fmul_rn(s.txWeight[k], v)) : __fadd_rn(acc, v);
+    }
+    static_cast<OUT*>(a.out)[line + static_cast<size_t>(r) * a.nRx] = clampCast<OUT>(acc);
+}
+
+// RawDelay (Beamformer/RawDelay.cu:221-312 with the kernel :406-468): highest-weight transmit only,
+// out [line][local element][depth], normalised by numAdds / sum(w); unused slots written as 0.
+template <typename RF, typename OUT>
+__global__ void __launch_bounds__(256) rawDelayKernel(DasArgs a) {
+    __shared__ float lut[64];
+    if (threadIdx.x < 64) lut[threadIdx.x] = a.lut.v[threadIdx.x];
+    __syncthreads();
+    const uint32_t line = blockIdx.y;
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nD) return;
+    const LineDT s = a.lines[line];
+    OUT* out = static_cast<OUT*>(a.out) + static_cast<size_t>(line) * a.nCh * a.nD + r;
+    const int k = s.highest;
+    int written = 0;
+    if ((s.activeMask >> k) & 1) {
+        const float d = __ldg(a.depth + r);
+        const float aDT = apertureDT(d, a.dt, a.c, a.F);
+        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+        float weightAcum = 0.0f;
+        int numAdds = 0;
+        for (int e = s.firstX[k]; e < s.lastX[k]; e++) {
+            const float dx = __fsub_rn(__ldg(a.xe + e), s.x);
+            if (fabsf(dx) <= aDT) {
+                weightAcum = __fadd_rn(weightAcum, lutGet(lut, __fmul_rn(dx, invMax)));
+                numAdds++;
+            }
+        }
+        const float scale = numAdds > 0 ? __fmul_rn(__fdiv_rn(1.0f, weightAcum), static_cast<float>(numAdds)) : 1.0f;
+        const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
+        const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
+        const float dy = __fmul_rn(s.dirY, d);
+        const float dy2 = __fmul_rn(dy, dy);
+        for (int e = s.firstX[k]; e < s.lastX[k] && written < static_cast<int>(a.nCh); e++, written++) {
+            float sample = 0.0f;
+            const float xel = __ldg(a.xe + e);
+            const float dx = __fsub_rn(xel, s.x);
+            if (fabsf(dx) <= aDT) {
+                const float w = lutGet(lut, __fmul_rn(dx, invMax));
+                const float ex = __fsub_rn(xel, xz);
+                const float delayf = __fadd_rn(s.initialDelay[k], __fadd_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2)), d));
+                const int32_t delay = static_cast<int32_t>(floorf(delayf));
+                const float frac = __fsub_rn(delayf, static_cast<float>(delay));
+                const RF* p = tx + static_cast<size_t>(static_cast<uint32_t>(e) % a.nCh) * a.nS;
+                if (static_cast<uint32_t>(delay) < a.nS - 1) {
+                    sample = __fmul_rn(w, __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), toFloat(p[delay])),
+                                                    __fmul_rn(frac, toFloat(p[delay + 1]))));
+                } else if (static_cast<uint32_t>(delay) < a.nS && frac == 0.0f) {
+                    sample = __fmul_rn(w, toFloat(p[delay]));
+                }
+            }
+            out[static_cast<size_t>(written) * a.nD] = clampCast<OUT>(__fmul_rn(sample, scale));
+        }
+    }
+    for (int j = written; j < static_cast<int>(a.nCh); j++) out[static_cast<size_t>(j) * a.nD] = clampCast<OUT>(0.0f);
+}
+
+int checkWindow(int windowType, float windowParameter) {
+    SB_REQUIRE(windowType >= 0 && windowType <= 3, "window type %d not in [0,3]", windowType);
+    SB_REQUIRE(!(windowType == SB_WINDOW_GAUSS && windowParameter == 0.0f), "Gauss window needs a non-zero parameter");
+    return SB_OK;
+}
+
+int fillArgs(sb_das_plan* p, DasArgs& a, const void* rf, void* out, double fNumber, double c, int windowType,
+             float windowParameter, int interpTx, int32_t offset, cudaStream_t st) {
+    SB_REQUIRE(fNumber > 0.0, "f-number must be > 0");
+    SB_REQUIRE(c > 0.0, "speed of sound must be > 0");
+    int e = checkWindow(windowType, windowParameter);
+    if (e != SB_OK) return e;
+    e = ensureDtSpace(p, c, st);
+    if (e != SB_OK) return e;
+    a.rf = rf;
+    a.out = out;
+    a.xe = p->dXe;
+    a.ye = p->dYe;
+    a.depth = p->dDepth;
+    a.lines = p->dLines;
+    a.e2c = p->dE2C;
+    a.apod = nullptr;
+    a.nE = p->numElements;
+    a.layoutX = p->layoutX;
+    a.nCh = p->numChannels;
+    a.nS = p->numSamples;
+    a.nTx = p->numTx;
+    a.nRx = p->numRx;
+    a.nD = p->numDepths;
+    a.c = static_cast<float>(c);
+    a.dt = static_cast<float>(1.0 / p->fs);
+    a.F = static_cast<float>(fNumber);
+    a.offset = static_cast<float>(offset);
+    a.interpTx = interpTx ? 1 : 0;
+    a.lut = makeLut(windowType, windowParameter);
+    return SB_OK;
+}
+
+}  // namespace
+
+int ensureDtSpace(sb_das_plan* p, double c, cudaStream_t st) {
+    if (p->cachedC == c) return SB_OK;
+    const double dt = 1.0 / p->fs;
+    const double factor = 1 / 1.0 / (c * dt);
+    const double factorTime = 1 / 1.0 / dt;
+    uint32_t n = std::max(std::max(p->numElements, p->numDepths), p->numRx);
+    dtConvertKernel<<<(n + 255) / 256, 256, 0, st>>>(p->dXeMM, p->dYeMM, p->numElements, p->dDepthMM, p->numDepths,
+                                                     p->dLinesMM, p->numRx, factor, factorTime, p->dXe, p->dYe,
+                                                     p->dDepth, p->dLines);
+    SB_CHECK_LAUNCH("dtConvertKernel");
+    p->cachedC = c;
+    return SB_OK;
+}
+
+}  // namespace sb
+
+using namespace sb;
+
+extern "C" {
+
+int sb_das_plan_create(const sb_geometry* g, sb_das_plan** out) {
+    SB_REQUIRE(g && out, "sb_das_plan_create: null argument");
+    *out = nullptr;
+    SB_REQUIRE(g->num_elements > 0 && g->num_channels > 0 && g->num_samples > 1 && g->num_tx > 0 && g->num_depths > 0,
+               "sb_das_plan_create: empty geometry");
+    SB_REQUIRE(g->num_rx == g->rx_layout[0] * g->rx_layout[1] && g->num_rx > 0, "num_rx != rx_layout product");
+    SB_REQUIRE(g->element_layout[0] * g->element_layout[1] == g->num_elements, "element_layout != num_elements");
+    SB_REQUIRE(g->sampling_frequency_hz > 0, "sampling frequency must be > 0");
+    SB_REQUIRE(g->element_x_mm && g->element_y_mm && g->depths_mm && g->scanlines, "null geometry array");
+    bool is3D = g->rx_layout[0] > 1 && g->rx_layout[1] > 1;
+    int32_t maxAx = 0, maxAy = 0;
+    for (uint32_t i = 0; i < g->num_rx; i++) {
+        const sb_scanline_rx& s = g->scanlines[i];
+        for (int k = 0; k < 4; k++) {
+            if (!(s.tx_weights[k] > 0.0)) continue;
+            SB_REQUIRE(s.tx[k].tx_scanline_idx < g->num_tx, "scanline %u: transmit index %u >= num_tx %u", i,
+                       s.tx[k].tx_scanline_idx, g->num_tx);
+            SB_REQUIRE(s.tx[k].last_active_element[0] <= g->element_layout[0] &&
+                           s.tx[k].last_active_element[1] <= g->element_layout[1],
+                       "scanline %u: aperture beyond the element layout", i);
+            maxAx = std::max(maxAx, static_cast<int32_t>(s.tx[k].last_active_element[0]) - s.tx[k].first_active_element[0]);
+            maxAy = std::max(maxAy, static_cast<int32_t>(s.tx[k].last_active_element[1]) - s.tx[k].first_active_element[1]);
+        }
+    }
+    if (g->element_to_channel)
+        for (uint32_t e = 0; e < g->num_elements; e++)
+            SB_REQUIRE(g->element_to_channel[e] < static_cast<int32_t>(g->num_channels), "element %u maps to channel %d",
+                       e, g->element_to_channel[e]);
+    sb_das_plan* p = new sb_das_plan();
+    p->numElements = g->num_elements;
+    p->layoutX = g->element_layout[0];
+    p->layoutY = g->element_layout[1];
+    p->numChannels = g->num_channels;
+    p->numSamples = g->num_samples;
+    p->numTx = g->num_tx;
+    p->numRx = g->num_rx;
+    p->rxLayoutX = g->rx_layout[0];
+    p->rxLayoutY = g->rx_layout[1];
+    p->numDepths = g->num_depths;
+    p->fs = g->sampling_frequency_hz;
+    p->is3D = is3D;
+    p->hasChannelMap = g->element_to_channel != nullptr;
+    p->maxApertureX = maxAx;
+    p->maxApertureY = maxAy;
+    p->hLines = new std::vector<sb_scanline_rx>(g->scanlines, g->scanlines + g->num_rx);
+    p->hXeMM = new std::vector<float>(g->element_x_mm, g->element_x_mm + g->num_elements);
+    p->hDepthMM = new std::vector<float>(g->depths_mm, g->depths_mm + g->num_depths);
+    auto cleanup = [&](int code) {
+        sb_das_plan_destroy(p);
+        return code;
+    };
+    size_t nE = g->num_elements, nD = g->num_depths, nRx = g->num_rx;
+    cudaError_t e = cudaSuccess;
+    e = cudaMalloc(&p->dXeMM, nE * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&p->dYeMM, nE * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&p->dDepthMM, nD * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&p->dLinesMM, nRx * sizeof(sb_scanline_rx));
+    if (e == cudaSuccess) e = cudaMalloc(&p->dXe, nE * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&p->dYe, nE * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&p->dDepth, nD * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&p->dLines, nRx * sizeof(LineDT));
+    if (e == cudaSuccess && g->element_to_channel) e = cudaMalloc(&p->dE2C, nE * sizeof(int32_t));
+    if (e != cudaSuccess) return cleanup(cudaFail(e, "sb_das_plan_create: cudaMalloc"));
+    e = cudaMemcpy(p->dXeMM, g->element_x_mm, nE * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->dYeMM, g->element_y_mm, nE * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->dDepthMM, g->depths_mm, nD * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->dLinesMM, g->scanlines, nRx * sizeof(sb_scanline_rx), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && g->element_to_channel)
+        e = cudaMemcpy(p->dE2C, g->element_to_channel, nE * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cleanup(cudaFail(e, "sb_das_plan_create: cudaMemcpy"));
+    *out = p;
+    return SB_OK;
+}
+
+int sb_das_plan_destroy(sb_das_plan* p) {
+    if (!p) return SB_OK;
+    cudaFree(p->dXeMM);
+    cudaFree(p->dYeMM);
+    cudaFree(p->dDepthMM);
+    cudaFree(p->dLinesMM);
+    cudaFree(p->dE2C);
+    cudaFree(p->dXe);
+    cudaFree(p->dYe);
+    cudaFree(p->dDepth);
+    cudaFree(p->dLines);
+    delete p->hLines;
+    delete p->hXeMM;
+    delete p->hDepthMM;
+    delete p;
+    return SB_OK;
+}
+
+int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out, int out_dtype, double f_number,
+               double speed_of_sound_mm_s, int window_type, float window_parameter, int interpolate_transmits,
+               int32_t additional_offset, sb_stream stream) {
+    SB_REQUIRE(plan && rf && out, "sb_das_run: null argument");
+    SB_REQUIRE(rf_dtype == SB_INT16 || rf_dtype == SB_FLOAT32, "sb_das_run: rf dtype %d unsupported", rf_dtype);
+    SB_REQUIRE(out_dtype == SB_FLOAT32 || out_dtype == SB_INT16, "sb_das_run: out dtype %d unsupported", out_dtype);
+    sb_das_plan* p = const_cast<sb_das_plan*>(plan);
+    cudaStream_t st = S(stream);
+    DasArgs a;
+    int err = fillArgs(p, a, rf, out, f_number, speed_of_sound_mm_s, window_type, window_parameter,
+                       interpolate_transmits, additional_offset, st);
+    if (err != SB_OK) return err;
+    dim3 grid((p->numDepths + 255) / 256, p->numRx);
+#define SB_DAS_LAUNCH(RFT, OUTT)                                                        \
+    do {                                                                                \
+        if (p->is3D) dasKernel<RFT, OUTT, true><<<grid, 256, 0, st>>>(a);              \
+        else dasKernel<RFT, OUTT, false><<<grid, 256, 0, st>>>(a);                     \
+    } while (0)
+    if (rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_DAS_LAUNCH(int16_t, float);
+    else if (rf_dtype == SB_INT16) SB_DAS_LAUNCH(int16_t, int16_t);
+    else if (out_dtype == SB_FLOAT32) SB_DAS_LAUNCH(float, float);
+    else SB_DAS_LAUNCH(float, int16_t);
+#undef SB_DAS_LAUNCH
+    SB_CHECK_LAUNCH("dasKernel");
+    return SB_OK;
+}
+
+int sb_rawdelay_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out, int out_dtype, double f_number,
+                    double speed_of_sound_mm_s, int window_type, float window_parameter, sb_stream stream) {
+    SB_REQUIRE(plan && rf && out, "sb_rawdelay_run: null argument");
+    SB_REQUIRE(rf_dtype == SB_INT16 || rf_dtype == SB_FLOAT32, "sb_rawdelay_run: rf dtype %d unsupported", rf_dtype);
+    SB_REQUIRE(out_dtype == SB_FLOAT32 || out_dtype == SB_INT16, "sb_rawdelay_run: out dtype %d unsupported", out_dtype);
+    sb_das_plan* p = const_cast<sb_das_plan*>(plan);
+    if (p->is3D) return fail(SB_ERR_UNSUPPORTED, "sb_rawdelay_run: 3D raw delay is not implemented");
+    cudaStream_t st = S(stream);
+    DasArgs a;
+    int err = fillArgs(p, a, rf, out, f_number, speed_of_sound_mm_s, window_type, window_parameter, 0, 0, st);
+    if (err != SB_OK) return err;
+    dim3 grid((p->numDepths + 255) / 256, p->numRx);
+    if (rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32) rawDelayKernel<int16_t, float><<<grid, 256, 0, st>>>(a);
+    else if (rf_dtype == SB_INT16) rawDelayKernel<int16_t, int16_t><<<grid, 256, 0, st>>>(a);
+    else if (out_dtype == SB_FLOAT32) rawDelayKernel<float, float><<<grid, 256, 0, st>>>(a);
+    else rawDelayKernel<float, int16_t><<<grid, 256, 0, st>>>(a);
+    SB_CHECK_LAUNCH("rawDelayKernel");
+    return SB_OK;
+}
+
+}  // extern "C"

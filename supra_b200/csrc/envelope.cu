@@ -1,0 +1,342 @@
+// Envelope detection (Hilbert FIR), log compression and IQ demodulation.
+//   HilbertFirEnvelope   Beamformer/HilbertFirEnvelope.cu:28-104
+//   LogCompressor        Beamformer/LogCompressor.cu:22-66
+//   IQDemodulator        Beamformer/IQDemodulator.cu:68-345 (frequency-compounded magnitude)
+// plus a complex baseband IQ demodulator (extension). Images are [sample][scanline], scanline fastest.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "design.h"
+#include "envelope.cuh"
+
+namespace sb {
+
+namespace {
+
+// ----------------------------------------------------------------------------- Hilbert envelope
+// One thread per (scanline, sample); the filter (plus one zero tap, see Q3 below) sits in shared
+// memory. env = sqrt(x^2 + (sum_j x[s - N/2 + j] h[j])^2), j = 0..2*(N/2) with out-of-range samples
+// skipped. For even N the reference reads h[N] one past its buffer; here that tap is 0.
+template <typename IN, typename OUT>
+__global__ void __launch_bounds__(256) hilbertKernel(const IN* __restrict__ in, OUT* __restrict__ out,
+                                                     const float* __restrict__ taps, int nS, int nL, int N) {
+    extern __shared__ float h[];
+    for (int i = threadIdx.y * blockDim.x + threadIdx.x; i <= N; i += blockDim.x * blockDim.y) h[i] = i < N ? taps[i] : 0.0f;
+    __syncthreads();
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y * blockDim.y + threadIdx.y;
+    if (l >= nL || s >= nS) return;
+    float acc = 0.0f;
+    const int start = s - N / 2, end = s + N / 2;
+    for (int cs = start, fe = 0; cs <= end; cs++, fe++) {
+        if (cs >= 0 && cs < nS) acc = __fadd_rn(acc, __fmul_rn(toFloat(in[l + static_cast<size_t>(cs) * nL]), h[fe]));
+    }
+    const float v = toFloat(in[l + static_cast<size_t>(s) * nL]);
+    out[l + static_cast<size_t>(s) * nL] = static_cast<OUT>(__fsqrt_rn(__fadd_rn(__fmul_rn(v, v), __fmul_rn(acc, acc))));
+}
+
+// ----------------------------------------------------------------------------- log compression
+template <typename IN, typename OUT>
+__global__ void logKernel(const IN* __restrict__ in, OUT* __restrict__ out, size_t n, float inScale, float k) {
+    size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (; i < n; i += stride) out[i] = clampCast<OUT>(logCompress(toFloat(in[i]), inScale, k));
+}
+
+// ----------------------------------------------------------------------------- IQ magnitude
+// One CTA = 32 scanlines x OT decimated outputs. Phase 1 evaluates the filter-bank magnitude
+// (kernelFilterBankDemodulation, IQDemodulator.cu:68-137) for every input sample the low-pass needs
+// and keeps it in shared memory; phase 2 applies the decimating low-pass (kernelFilterStrided
+// :142-175). No full-resolution intermediate goes to HBM.
+constexpr int IQ_LINES = 32;
+constexpr int IQ_OT = 16;
+
+template <typename IN, typename OUT>
+__global__ void __launch_bounds__(256) iqMagnitudeKernel(const IN* __restrict__ in, OUT* __restrict__ out, IqArgs a) {
+    extern __shared__ float sm[];
+    float* band = sm;                                   // [rows][IQ_LINES]
+    const int rows = (IQ_OT - 1) * a.stride + a.lpN + 1;
+    const int l0 = blockIdx.x * IQ_LINES;
+    const int so0 = blockIdx.y * IQ_OT;
+    const int sIn0 = so0 * a.stride - a.lpN / 2;       // first input sample a low-pass tap touches
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < rows * IQ_LINES; idx += blockDim.x) {
+        const int row = idx / IQ_LINES, li = idx % IQ_LINES;
+        const int s = sIn0 + row, l = l0 + li;
+        float v = 0.0f;
+        if (l < a.nL && s >= 0 && s < a.nS) {
+            float acc[8];
+            const float sv = toFloat(in[l + static_cast<size_t>(s) * a.nL]);
+            for (int f = 0; f < a.numFilters; f++) acc[f] = f < 1 ? sv : 0.0f;
+            if (a.numFilters > 1) {
+                const int start = s - a.bpN / 2, end = s + a.bpN / 2;
+                for (int cs = start, fe = 0; cs <= end; cs++, fe++) {
+                    if (cs >= 0 && cs < a.nS) {
+                        const float x = toFloat(in[l + static_cast<size_t>(cs) * a.nL]);
+                        for (int f = 1; f < a.numFilters; f++)
+                            acc[f] = __fadd_rn(acc[f], __fmul_rn(x, a.bank[f * (a.bpN + 1) + fe]));
+                    }
+                }
+            }
+            float m = 0.0f;
+            for (int f = 0; f < a.numFilters; f++) {
+                const float ph = __fmul_rn(static_cast<float>(s), a.fOverFs[f]);
+                float phI = __fadd_rn(ph, 0.0f);
+                float phQ = __fadd_rn(ph, 0.75f);
+                phI = __fsub_rn(phI, truncf(phI));
+                phQ = __fsub_rn(phQ, truncf(phQ));
+                const float dI = __fmul_rn(acc[f], cosf(__fmul_rn(__fmul_rn(phI, 2.0f), static_cast<float>(M_PI))));
+                const float dQ = __fmul_rn(acc[f], cosf(__fmul_rn(__fmul_rn(phQ, 2.0f), static_cast<float>(M_PI))));
+                m = __fadd_rn(m, __fmul_rn(a.weights[f], __fsqrt_rn(__fadd_rn(__fmul_rn(dI, dI), __fmul_rn(dQ, dQ)))));
+            }
+            v = __fmul_rn(a.scale, m);
+        }
+        band[row * IQ_LINES + li] = v;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < IQ_OT * IQ_LINES; idx += blockDim.x) {
+        const int o = idx / IQ_LINES, li = idx % IQ_LINES;
+        const int so = so0 + o, l = l0 + li;
+        const int si = so * a.stride;
+        if (so >= a.nOut || l >= a.nL || si >= a.nS) continue;
+        float acc = 0.0f;
+        const int start = si - a.lpN / 2, end = si + a.lpN / 2;
+        for (int cs = start, fe = 0; cs <= end; cs++, fe++) {
+            if (cs >= 0 && cs < a.nS) acc = __fadd_rn(acc, __fmul_rn(band[(cs - sIn0) * IQ_LINES + li], a.lp[fe]));
+        }
+        out[l + static_cast<size_t>(so) * a.nL] = clampCast<OUT>(acc);
+    }
+}
+
+// ----------------------------------------------------------------------------- complex IQ
+template <typename IN>
+__global__ void __launch_bounds__(256) iqComplexKernel(const IN* __restrict__ in, float2* __restrict__ out,
+                                                       IqComplexArgs a) {
+    extern __shared__ float sm[];
+    const int rows = (IQ_OT - 1) * a.dec + a.taps;
+    float* xs = sm;                         // [rows][IQ_LINES]
+    float2* rot = reinterpret_cast<float2*>(xs + rows * IQ_LINES);  // [rows]
+    const int l0 = blockIdx.x * IQ_LINES;
+    const int so0 = blockIdx.y * IQ_OT;
+    const int s0 = so0 * a.dec - a.half;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+        const int n = s0 + r;
+        double ph = static_cast<double>(a.fOverFs) * n;
+        ph -= floor(ph);
+        float sn, cs;
+        sincospif(static_cast<float>(2.0 * ph), &sn, &cs);
+        rot[r] = make_float2(cs, -sn);
+    }
+    for (int idx = threadIdx.x; idx < rows * IQ_LINES; idx += blockDim.x) {
+        const int r = idx / IQ_LINES, li = idx % IQ_LINES;
+        const int s = s0 + r, l = l0 + li;
+        xs[idx] = (l < a.nL && s >= 0 && s < a.nS) ? toFloat(in[l + static_cast<size_t>(s) * a.nL]) : 0.0f;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < IQ_OT * IQ_LINES; idx += blockDim.x) {
+        const int o = idx / IQ_LINES, li = idx % IQ_LINES;
+        const int so = so0 + o, l = l0 + li;
+        if (so >= a.nOut || l >= a.nL) continue;
+        float re = 0.0f, im = 0.0f;
+        const int rb = o * a.dec;
+        for (int j = 0; j < a.taps; j++) {
+            const float x = xs[(rb + j) * IQ_LINES + li] * a.lp[j];
+            const float2 w = rot[rb + j];
+            re = fmaf(x, w.x, re);
+            im = fmaf(x, w.y, im);
+        }
+        out[l + static_cast<size_t>(so) * a.nL] = make_float2(re, im);
+    }
+}
+
+}  // namespace
+
+int launchLog(const void* in, int inDt, void* out, int outDt, size_t n, float inScale, float k, cudaStream_t st) {
+    int blocks = static_cast<int>(std::min<size_t>((n + 255) / 256, static_cast<size_t>(smCount()) * 16));
+    if (blocks < 1) blocks = 1;
+#define SB_LOG(INT, OUTT) logKernel<INT, OUTT><<<blocks, 256, 0, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), n, inScale, k)
+    if (inDt == SB_FLOAT32 && outDt == SB_UINT8) SB_LOG(float, uint8_t);
+    else if (inDt == SB_FLOAT32 && outDt == SB_FLOAT32) SB_LOG(float, float);
+    else if (inDt == SB_INT16 && outDt == SB_UINT8) SB_LOG(int16_t, uint8_t);
+    else if (inDt == SB_INT16 && outDt == SB_FLOAT32) SB_LOG(int16_t, float);
+    else if (inDt == SB_UINT8 && outDt == SB_UINT8) SB_LOG(uint8_t, uint8_t);
+    else if (inDt == SB_UINT8 && outDt == SB_FLOAT32) SB_LOG(uint8_t, float);
+    else return fail(SB_ERR_UNSUPPORTED, "log compression %d -> %d unsupported", inDt, outDt);
+#undef SB_LOG
+    SB_CHECK_LAUNCH("logKernel");
+    return SB_OK;
+}
+
+// LogCompressor constants (LogCompressor.cu:22-34, :44-64): inScale = 10^(DR/20) / inMax and
+// k = gain * outMax / log10(10^(DR/20) + 1), both rounded to float from double.
+void logConstants(double dynamicRange, double gain, double inMax, int inDt, float& inScale, float& k) {
+    double dr = std::pow(10, (dynamicRange / 20));
+    double inMaxT = inDt == SB_INT16   ? static_cast<double>(static_cast<int16_t>(inMax))
+                    : inDt == SB_UINT8 ? static_cast<double>(static_cast<uint8_t>(inMax))
+                                       : static_cast<double>(static_cast<float>(inMax));
+    inScale = static_cast<float>(dr / inMaxT);
+    k = static_cast<float>(gain * 255.0 / std::log10(dr + 1));
+}
+
+}  // namespace sb
+
+using namespace sb;
+
+struct sb_iq_plan {
+    sb::IqArgs args;  // filters embedded by value
+};
+
+extern "C" {
+
+int sb_hilbert_plan_create(uint32_t filter_length, sb_hilbert_plan** plan) {
+    SB_REQUIRE(plan && filter_length >= 1 && filter_length <= 1024, "sb_hilbert_plan_create: filter length %u", filter_length);
+    *plan = nullptr;
+    std::vector<float> taps = firDesign(filter_length, 3, 2, 2.0, 0.0, 0.0);
+    sb_hilbert_plan* p = new sb_hilbert_plan{filter_length, nullptr};
+    cudaError_t e = cudaMalloc(&p->dTaps, filter_length * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(p->dTaps, taps.data(), filter_length * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(p->dTaps);
+        delete p;
+        return cudaFail(e, "sb_hilbert_plan_create");
+    }
+    *plan = p;
+    return SB_OK;
+}
+
+int sb_hilbert_plan_destroy(sb_hilbert_plan* p) {
+    if (!p) return SB_OK;
+    cudaFree(p->dTaps);
+    delete p;
+    return SB_OK;
+}
+
+int sb_hilbert_env_run(const sb_hilbert_plan* p, const void* in, int in_dtype, void* out, int out_dtype,
+                       uint32_t num_scanlines, uint32_t num_samples, sb_stream stream) {
+    SB_REQUIRE(p && in && out, "sb_hilbert_env_run: null argument");
+    SB_REQUIRE(num_scanlines > 0 && num_samples > 0, "sb_hilbert_env_run: empty image");
+    cudaStream_t st = S(stream);
+    dim3 block(32, 8);
+    dim3 grid((num_scanlines + 31) / 32, (num_samples + 7) / 8);
+    size_t shm = (p->N + 1) * sizeof(float);
+    int nS = static_cast<int>(num_samples), nL = static_cast<int>(num_scanlines), N = static_cast<int>(p->N);
+    if (in_dtype == SB_FLOAT32 && out_dtype == SB_FLOAT32)
+        hilbertKernel<float, float><<<grid, block, shm, st>>>(static_cast<const float*>(in), static_cast<float*>(out), p->dTaps, nS, nL, N);
+    else if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32)
+        hilbertKernel<int16_t, float><<<grid, block, shm, st>>>(static_cast<const int16_t*>(in), static_cast<float*>(out), p->dTaps, nS, nL, N);
+    else
+        return fail(SB_ERR_UNSUPPORTED, "sb_hilbert_env_run: %d -> %d unsupported", in_dtype, out_dtype);
+    SB_CHECK_LAUNCH("hilbertKernel");
+    return SB_OK;
+}
+
+int sb_logcompress_run(const void* in, int in_dtype, void* out, int out_dtype, size_t num_values,
+                       double dynamic_range_db, double gain, double in_max, sb_stream stream) {
+    SB_REQUIRE(in && out, "sb_logcompress_run: null argument");
+    SB_REQUIRE(in_max > 0 && dynamic_range_db > 0, "sb_logcompress_run: inMax and dynamic range must be > 0");
+    if (num_values == 0) return SB_OK;
+    float inScale, k;
+    logConstants(dynamic_range_db, gain, in_max, in_dtype, inScale, k);
+    return launchLog(in, in_dtype, out, out_dtype, num_values, inScale, k, S(stream));
+}
+
+int sb_iq_plan_create(double fs, double cutoff, uint32_t lpLen, uint32_t bpLen, uint32_t numFilters,
+                      const double* refFreqs, const double* bandwidths, const double* weights, sb_iq_plan** plan) {
+    SB_REQUIRE(plan && refFreqs && bandwidths && weights, "sb_iq_plan_create: null argument");
+    SB_REQUIRE(numFilters >= 1 && numFilters <= 8, "sb_iq_plan_create: 1..8 filters, got %u", numFilters);
+    SB_REQUIRE(lpLen >= 1 && lpLen <= kIqMaxTaps - 1 && bpLen >= 1 && bpLen <= kIqMaxTaps - 1,
+               "sb_iq_plan_create: filter lengths must be in [1, %d]", kIqMaxTaps - 1);
+    SB_REQUIRE(fs > 0 && cutoff > 0, "sb_iq_plan_create: frequencies must be > 0");
+    sb_iq_plan* p = new sb_iq_plan();
+    IqArgs& a = p->args;
+    a.numFilters = static_cast<int>(numFilters);
+    a.bpN = static_cast<int>(bpLen);
+    a.lpN = static_cast<int>(lpLen);
+    float weightAcum = 0;
+    for (uint32_t k = 0; k < numFilters; k++) {
+        std::vector<float> bp = (refFreqs[k] > 0 && bandwidths[k] > 0) ? firDesign(bpLen, 2, 3, fs, refFreqs[k], bandwidths[k])
+                                                                       : std::vector<float>(bpLen, 0.0f);
+        for (uint32_t j = 0; j <= bpLen; j++) a.bank[k * (bpLen + 1) + j] = j < bpLen ? bp[j] : 0.0f;
+        a.weights[k] = static_cast<float>(weights[k]);
+        weightAcum += static_cast<float>(weights[k]);
+        a.fOverFs[k] = static_cast<float>(refFreqs[k] / fs);
+    }
+    a.scale = 1 / weightAcum;
+    std::vector<float> lp = firDesign(lpLen, 0, 2, fs, cutoff, 0.0);
+    for (uint32_t j = 0; j <= lpLen; j++) a.lp[j] = j < lpLen ? lp[j] : 0.0f;
+    *plan = p;
+    return SB_OK;
+}
+
+int sb_iq_plan_destroy(sb_iq_plan* p) {
+    delete p;
+    return SB_OK;
+}
+
+int sb_iq_magnitude_run(const sb_iq_plan* p, const void* in, int in_dtype, void* out, int out_dtype,
+                        uint32_t num_scanlines, uint32_t num_samples, uint32_t decimation, sb_stream stream) {
+    SB_REQUIRE(p && in && out, "sb_iq_magnitude_run: null argument");
+    SB_REQUIRE(num_scanlines > 0 && num_samples > 0, "sb_iq_magnitude_run: empty image");
+    IqArgs a = p->args;
+    a.nS = static_cast<int>(num_samples);
+    a.nL = static_cast<int>(num_scanlines);
+    a.stride = static_cast<int>(std::max(decimation, 1u));
+    a.nOut = decimation > 1 ? a.nS / static_cast<int>(decimation) : a.nS;
+    if (a.nOut == 0) return SB_OK;
+    const int rows = (IQ_OT - 1) * a.stride + a.lpN + 1;
+    size_t shm = static_cast<size_t>(rows) * IQ_LINES * sizeof(float);
+    SB_REQUIRE(shm <= 200 * 1024, "sb_iq_magnitude_run: decimation %u too large", decimation);
+    cudaStream_t st = S(stream);
+    dim3 grid((a.nL + IQ_LINES - 1) / IQ_LINES, (a.nOut + IQ_OT - 1) / IQ_OT);
+#define SB_IQM(INT, OUTT)                                                                                      \
+    do {                                                                                                       \
+        SB_CUDA(cudaFuncSetAttribute(iqMagnitudeKernel<INT, OUTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     static_cast<int>(shm)));                                                  \
+        iqMagnitudeKernel<INT, OUTT><<<grid, 256, shm, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), a); \
+        SB_CHECK_LAUNCH("iqMagnitudeKernel");                                                                  \
+        return SB_OK;                                                                                          \
+    } while (0)
+    if (in_dtype == SB_FLOAT32 && out_dtype == SB_FLOAT32) SB_IQM(float, float);
+    if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_IQM(int16_t, float);
+    if (in_dtype == SB_FLOAT32 && out_dtype == SB_INT16) SB_IQM(float, int16_t);
+    if (in_dtype == SB_INT16 && out_dtype == SB_INT16) SB_IQM(int16_t, int16_t);
+#undef SB_IQM
+    return fail(SB_ERR_UNSUPPORTED, "sb_iq_magnitude_run: %d -> %d unsupported", in_dtype, out_dtype);
+}
+
+int sb_iq_complex_run(const void* in, int in_dtype, void* out, uint32_t num_scanlines, uint32_t num_samples, double fs,
+                      double fmix, double cutoff, uint32_t lpLen, uint32_t decimation, sb_stream stream) {
+    SB_REQUIRE(in && out, "sb_iq_complex_run: null argument");
+    SB_REQUIRE(fs > 0 && cutoff > 0 && lpLen >= 1 && lpLen < kIqMaxTaps, "sb_iq_complex_run: bad filter parameters");
+    SB_REQUIRE(in_dtype == SB_FLOAT32 || in_dtype == SB_INT16, "sb_iq_complex_run: dtype %d", in_dtype);
+    IqComplexArgs a;
+    a.nS = static_cast<int>(num_samples);
+    a.nL = static_cast<int>(num_scanlines);
+    a.dec = static_cast<int>(std::max(decimation, 1u));
+    a.nOut = a.nS / a.dec;
+    a.fOverFs = fmix / fs;
+    std::vector<float> lp = firDesign(lpLen, 0, 2, fs, cutoff, 0.0);
+    // taps j = 0 .. 2*(N/2) centred on the output sample (the reference's FIR loop form); for even N
+    // the last one is 0
+    a.half = static_cast<int>(lpLen) / 2;
+    a.taps = 2 * a.half + 1;
+    for (int j = 0; j < a.taps; j++) a.lp[j] = j < static_cast<int>(lpLen) ? lp[j] : 0.0f;
+    if (a.nOut == 0 || a.nL == 0) return SB_OK;
+    const int rows = (IQ_OT - 1) * a.dec + a.taps;
+    size_t shm = static_cast<size_t>(rows) * IQ_LINES * sizeof(float) + static_cast<size_t>(rows) * sizeof(float2);
+    SB_REQUIRE(shm <= 200 * 1024, "sb_iq_complex_run: decimation %u too large", decimation);
+    cudaStream_t st = S(stream);
+    dim3 grid((a.nL + IQ_LINES - 1) / IQ_LINES, (a.nOut + IQ_OT - 1) / IQ_OT);
+    if (in_dtype == SB_FLOAT32) {
+        SB_CUDA(cudaFuncSetAttribute(iqComplexKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)));
+        iqComplexKernel<float><<<grid, 256, shm, st>>>(static_cast<const float*>(in), static_cast<float2*>(out), a);
+    } else {
+        SB_CUDA(cudaFuncSetAttribute(iqComplexKernel<int16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)));
+        iqComplexKernel<int16_t><<<grid, 256, shm, st>>>(static_cast<const int16_t*>(in), static_cast<float2*>(out), a);
+    }
+    SB_CHECK_LAUNCH("iqComplexKernel");
+    return SB_OK;
+}
+
+}  // extern "C"
