@@ -1,0 +1,273 @@
+"""Benchmark of the batched receive path: beamformed px/s on config 1 (64 frames of three linear
+probes per launch, DAS + complex IQ, persistent CUDA-graph-captured kernel).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). N > 1 runs N independent replicas (one batch per GPU, no collective
+on the data path; torch.distributed is used only for the barrier and the max-over-ranks time).
+--impl reference times the CPU restatement of the reference's semantics (the oracle) on the host
+cores over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "beamformed px/s"
+UNIT = "px/s"
+WORKLOAD = ("c1 batched DAS+IQ: 64 frames/launch (22x P64/1024 smp, 21x P128/2048, 21x P192/3072), 0.3 mm, "
+            "fs 40 MHz, 64-ch aperture, F#1 Hann, int16 in; IQ 5 MHz mix, 32-tap LPF, /4, complex64 out")
+# DRAM bytes per beamformed pixel of batchDasIqKernel measured by ncu on a 6-frame case of this workload
+# (dram__bytes_read.sum + dram__bytes_write.sum / pixels); the summary is in profiles/.
+TRAFFIC_BYTES_PER_PX = None
+
+
+def peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_step(geoms, rfs, threads):
+    """One bounded step of the CPU restatement: DAS (reference FP32 semantics) + complex IQ of one frame
+    of each probe. Returns beamformed pixels."""
+    from oracle import oracle as O
+    px = 0
+    for g, rf in zip(geoms, rfs):
+        img = O.das(g, rf, 1.0, window=1, threads=threads)
+        img = np.nan_to_num(img, nan=0.0, posinf=0.0, neginf=0.0)
+        O.iq_complex(img.astype(np.float32), 40e6, 5e6, 2.5e6, 32, 4, threads=threads)
+        px += g.num_rx * g.num_depths
+    return px
+
+
+def cpu_sample(threads):
+    from supra_b200.workloads import c1_frame, c1_geometries
+    geoms = c1_geometries()
+    rfs = [c1_frame(g, 2000 + i, device="cpu").numpy() for i, g in enumerate(geoms)]
+    return geoms, rfs
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    geoms, rfs = cpu_sample(threads)
+    for _ in range(args.warmup):
+        cpu_reference_step(geoms, rfs, threads)
+    t0 = time.perf_counter()
+    px = 0
+    for _ in range(args.steps):
+        px += cpu_reference_step(geoms, rfs, threads)
+    dt = time.perf_counter() - t0
+    value = px / dt
+    sample = "per step: DAS + complex IQ of one frame of each probe (P64, P128, P192) = 917504 px"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from supra_b200.api import BatchedDasIq, RxBeamformer, check_device_errors
+    from supra_b200.workloads import c1_workload
+
+    wl = c1_workload(device="cuda", seed0=1000 + 100 * rank)
+    plans = [RxBeamformer(g) for g in wl.geometries]
+    frames = [(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)]
+    batch = BatchedDasIq(frames, 1.0, 1540e3, 1, 0.0, 5e6, 2.5e6, 32, 4)
+    shape = batch.autotune(os.path.join(HERE, "supra_b200", "lib", "autotune_cache.txt"))
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        batch.run(use_graph=True)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clk:
+        evs[0].record(stream)
+        for i in range(args.steps):
+            batch.run(use_graph=True)
+            evs[i + 1].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    check_device_errors()
+    per = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    total_ms = evs[0].elapsed_time(evs[-1])
+    t = torch.tensor([total_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    px = wl.beamformed_px
+    value = px * args.steps * world / (total_ms / 1e3)
+    kern_ms = statistics.mean(per)
+    alg_bytes = wl.rf_bytes + wl.iq_bytes(4)
+    hbm, peak_kind = peaks()
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    traffic = None if TRAFFIC_BYTES_PER_PX is None else TRAFFIC_BYTES_PER_PX * px
+
+    # end to end through the public API: pinned host RF -> device, batch, IQ -> pinned host
+    host_rf = [r.cpu().pin_memory() for r in wl.rf]
+    host_iq = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in batch.outputs]
+    h2d = sum(h.numel() * h.element_size() for h in host_rf)
+    d2h = sum(h.numel() * h.element_size() for h in host_iq)
+
+    def e2e_step():
+        for h, d in zip(host_rf, wl.rf):
+            d.copy_(h, non_blocking=True)
+        batch.run(use_graph=True)
+        for h, d in zip(host_iq, batch.outputs):
+            h.copy_(d, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    e_ms = torch.tensor([a.elapsed_time(b)], device="cuda")
+    if world > 1:
+        dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
+    e2e_value = px * args.e2e_steps * world / (float(e_ms.item()) / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        geoms, rfs = cpu_sample(threads)
+        cpu_reference_step(geoms, rfs, threads)
+        t0 = time.perf_counter()
+        n = 0
+        while time.perf_counter() - t0 < 10.0:
+            n += cpu_reference_step(geoms, rfs, threads)
+        cpu = {"value": n / (time.perf_counter() - t0), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": "oracle DAS (reference FP32 semantics) + complex IQ, one frame per probe per step, ~10 s"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frames_per_launch": len(wl.rf), "beamformed_px_per_launch": px,
+                       "parallelism": f"replicas x{world}", "l2": "inputs 2.47 GB per launch > L2, no flush",
+                       "tile_shape": {"ctas_per_sm": shape[0], "depth_tile": shape[1]}, "graph_captured": True},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "peak_kind": peak_kind, "kernel": "batchDasIqKernel",
+                         "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    del batch
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

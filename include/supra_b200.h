@@ -246,8 +246,8 @@ typedef struct sb_batch_params {
     double cutoff_frequency_hz;
     uint32_t lowpass_length;   /* taps of the decimation low-pass */
     uint32_t decimation;
-    int32_t lines_per_item;    /* tile shape: scanlines per work item (0 = autotuned / default) */
-    int32_t depth_tile;        /* tile shape: depths per chunk (0 = autotuned / default) */
+    int32_t ctas_per_sm;       /* tile shape: resident CTAs per SM, 1..3 (0 = default / autotuned) */
+    int32_t depth_tile;        /* tile shape: depths per chunk, 128 or 256 (0 = default / autotuned) */
 } sb_batch_params;
 
 /* Persistent batched DAS + complex IQ over frames of uneven probes in one launch. */
@@ -259,9 +259,13 @@ int sb_batch_run(sb_batch_plan* plan, int use_graph, sb_stream stream);
 /* Optional: write the fused per-frame RF (FP32 [num_depths][num_rx]) too; pass NULL to disable. */
 int sb_batch_set_rf_outputs(sb_batch_plan* plan, float* const* rf_out);
 /* Time candidate tile shapes on the device and keep the fastest; cache_path (may be NULL) stores
- * the choice per problem signature. Returns the chosen shape. */
-int sb_batch_autotune(sb_batch_plan* plan, const char* cache_path, int32_t* lines_per_item, int32_t* depth_tile,
+ * the choice per problem signature and is consulted first. Returns the chosen shape. Synchronises. */
+int sb_batch_autotune(sb_batch_plan* plan, const char* cache_path, int32_t* ctas_per_sm, int32_t* depth_tile,
                       sb_stream stream);
+
+/* Device-side failure flag shared by the kernels with bounded waits: returns SB_ERR_TIMEOUT if any
+ * wait gave up since the last call (and clears the flag when reset != 0). Synchronises the device. */
+int sb_check_device_errors(int reset);
 
 /* ---------------------------------------------------------------- adjoint DAS */
 

@@ -282,3 +282,68 @@ def mv_beamform(raw_delayed: torch.Tensor, subarray_size=0, temporal_smoothing=3
                                      int(bool(compute_means)), float(loading_scale), float(fp64_threshold),
                                      C.byref(stats), _stream()))
     return out, stats
+
+
+class BatchedDasIq:
+    """Persistent, graph-captured batched DAS + complex IQ over frames of uneven probes.
+
+    frames: list of (RxBeamformer, rf tensor [num_tx][num_channels][num_samples] int16 on the device).
+    Output tensors (complex64 [num_depths / decimation][num_rx]) are allocated here, one per frame.
+    """
+
+    def __init__(self, frames, f_number=1.0, speed_of_sound_mm_s=1540e3, window_type=1, window_parameter=0.0,
+                 mixing_frequency=5e6, cutoff_frequency=2.5e6, lowpass_length=32, decimation=4, ctas_per_sm=0,
+                 depth_tile=0):
+        self.lib = load_library()
+        self.frames = frames
+        self.outputs = []
+        arr = (abi.sb_batch_frame * len(frames))()
+        for i, (bf, rf) in enumerate(frames):
+            g = bf.geometry
+            out = torch.empty((g.num_depths // max(decimation, 1), g.num_rx), dtype=torch.complex64, device=rf.device)
+            self.outputs.append(out)
+            arr[i].probe = bf.handle.value
+            arr[i].rf = rf.data_ptr()
+            arr[i].iq_out = out.data_ptr()
+        prm = abi.sb_batch_params()
+        prm.f_number = f_number
+        prm.speed_of_sound_mm_s = speed_of_sound_mm_s
+        prm.window_type = window_type
+        prm.window_parameter = window_parameter
+        prm.mixing_frequency_hz = mixing_frequency
+        prm.cutoff_frequency_hz = cutoff_frequency
+        prm.lowpass_length = lowpass_length
+        prm.decimation = decimation
+        prm.ctas_per_sm = ctas_per_sm
+        prm.depth_tile = depth_tile
+        self._plan = C.c_void_p()
+        check("sb_batch_plan_create", self.lib.sb_batch_plan_create(arr, len(frames), C.byref(prm), C.byref(self._plan)))
+        self.rf_outputs = None
+
+    def __del__(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            self.lib.sb_batch_plan_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    def enable_rf_outputs(self):
+        """Also write each frame's beamformed RF (FP32 [num_depths][num_rx])."""
+        self.rf_outputs = [torch.empty((bf.geometry.num_depths, bf.geometry.num_rx), dtype=torch.float32,
+                                       device=rf.device) for bf, rf in self.frames]
+        ptrs = (C.c_void_p * len(self.rf_outputs))(*[t.data_ptr() for t in self.rf_outputs])
+        check("sb_batch_set_rf_outputs", self.lib.sb_batch_set_rf_outputs(self._plan, ptrs))
+
+    def run(self, use_graph=True):
+        check("sb_batch_run", self.lib.sb_batch_run(self._plan, int(bool(use_graph)), _stream()))
+        return self.outputs
+
+    def autotune(self, cache_path=None):
+        c = C.c_int32()
+        t = C.c_int32()
+        check("sb_batch_autotune", self.lib.sb_batch_autotune(self._plan, cache_path.encode() if cache_path else None,
+                                                              C.byref(c), C.byref(t), _stream()))
+        return int(c.value), int(t.value)
+
+
+def check_device_errors(reset=True):
+    lib = load_library()
+    check("sb_check_device_errors", lib.sb_check_device_errors(int(bool(reset))))

@@ -65,4 +65,8 @@ template <typename T> __device__ __forceinline__ float toFloat(T v) { return sta
 // Number of SMs of the current device (cached per device).
 int smCount();
 
+// Per-device int in global memory that kernels set when a bounded wait gives up (nullptr if it
+// could not be allocated).
+int* deviceErrorFlag();
+
 }  // namespace sb

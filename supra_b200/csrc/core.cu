@@ -48,9 +48,38 @@ int smCount() {
     return cache[dev];
 }
 
+int* deviceErrorFlag() {
+    static std::mutex m;
+    static int* flags[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> l(m);
+    if (!flags[dev]) {
+        int* f = nullptr;
+        if (cudaMalloc(&f, sizeof(int)) != cudaSuccess) return nullptr;
+        if (cudaMemset(f, 0, sizeof(int)) != cudaSuccess) {
+            cudaFree(f);
+            return nullptr;
+        }
+        flags[dev] = f;
+    }
+    return flags[dev];
+}
+
 }  // namespace sb
 
 extern "C" {
+
+int sb_check_device_errors(int reset) {
+    int* f = sb::deviceErrorFlag();
+    if (!f) return sb::fail(SB_ERR_NO_MEMORY, "sb_check_device_errors: no device flag");
+    SB_CUDA(cudaDeviceSynchronize());
+    int h = 0;
+    SB_CUDA(cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost));
+    if (reset && h) SB_CUDA(cudaMemset(f, 0, sizeof(int)));
+    if (h) return sb::fail(SB_ERR_TIMEOUT, "a device-side bounded wait gave up (staged channel data never arrived)");
+    return SB_OK;
+}
 
 const char* sb_last_error(void) { return sb::g_lastError.c_str(); }
 

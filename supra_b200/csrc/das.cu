@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "das.cuh"
+#include "das_core.cuh"
 #include "design.h"
 
 namespace sb {
@@ -260,6 +261,45 @@ __global__ void __launch_bounds__(256) rawDelayKernel(DasArgs a) {
     for (int j = written; j < static_cast<int>(a.nCh); j++) out[static_cast<size_t>(j) * a.nD] = clampCast<OUT>(0.0f);
 }
 
+// Staged per-frame 2D DAS: one CTA per (scanline, chunksPerCta chunks of NT depths).
+template <typename RF, typename OUT, int NT>
+__global__ void __launch_bounds__(NT) dasStagedKernel(FrameDesc f, WindowLut lut, void* out, uint32_t maxW,
+                                                      uint32_t chunksPerCta, int* errFlag) {
+    extern __shared__ __align__(128) unsigned char smraw[];
+    CtaState& st = *reinterpret_cast<CtaState*>(smraw);
+    RF* smemRF = reinterpret_cast<RF*>(smraw + ((sizeof(CtaState) + 127) & ~size_t(127)));
+    const int tid = threadIdx.x;
+    const uint32_t line = blockIdx.y;
+    if (tid < 64) st.lut[tid] = lut.v[tid];
+    if (tid == 0) {
+        mbarInit(&st.bar[0], 1);
+        mbarInit(&st.bar[1], 1);
+        mbarInitFence();
+        st.phase[0] = st.phase[1] = 0;
+    }
+    __syncthreads();
+    const LineK s = reduceLine(f.lines[line]);
+    OUT* o = static_cast<OUT*>(out);
+    const bool ok = setupLine<NT>(st, f, s);
+    const bool useOffset = f.offset != 0.0f;
+    for (uint32_t c = 0; c < chunksPerCta; c++) {
+        const uint32_t r0 = (blockIdx.x * chunksPerCta + c) * NT;
+        if (r0 >= f.nD) break;
+        const uint32_t r = r0 + tid;
+        if (!ok) {  // no active transmit: the reference writes clampCast(0)
+            if (r < f.nD) o[line + static_cast<size_t>(r) * f.nRx] = clampCast<OUT>(0.0f);
+            continue;
+        }
+        planChunk<RF, NT>(st, smemRF, 0, f, s, r0, maxW, maxW, useOffset);
+        if (!waitChunk(st, 0)) {
+            if (tid == 0) atomicExch(errFlag, 1);
+            return;
+        }
+        if (r < f.nD) o[line + static_cast<size_t>(r) * f.nRx] = clampCast<OUT>(dasDepth<RF>(st, smemRF, 0, maxW, f, s, r, useOffset));
+        __syncthreads();
+    }
+}
+
 int checkWindow(int windowType, float windowParameter) {
     SB_REQUIRE(windowType >= 0 && windowType <= 3, "window type %d not in [0,3]", windowType);
     SB_REQUIRE(!(windowType == SB_WINDOW_GAUSS && windowParameter == 0.0f), "Gauss window needs a non-zero parameter");
@@ -295,6 +335,64 @@ int fillArgs(sb_das_plan* p, DasArgs& a, const void* rf, void* out, double fNumb
     a.offset = static_cast<float>(offset);
     a.interpTx = interpTx ? 1 : 0;
     a.lut = makeLut(windowType, windowParameter);
+    return SB_OK;
+}
+
+constexpr int kStagedThreads = 256;
+constexpr size_t kStagedSmemBudget = 72 * 1024;
+
+uint32_t stagedMaxW(uint32_t nCh, size_t rfSize) {
+    const size_t state = (sizeof(CtaState) + 127) & ~size_t(127);
+    if (kStagedSmemBudget <= state) return 0;
+    size_t w = (kStagedSmemBudget - state) / (nCh * rfSize);
+    w &= ~size_t(7);
+    return static_cast<uint32_t>(std::min<size_t>(w, 4096));
+}
+
+FrameDesc frameOf(const sb_das_plan* p, const DasArgs& a) {
+    FrameDesc f;
+    f.rf = a.rf;
+    f.lines = a.lines;
+    f.xe = a.xe;
+    f.depth = a.depth;
+    f.e2c = a.e2c;
+    f.nCh = a.nCh;
+    f.nS = a.nS;
+    f.nTx = a.nTx;
+    f.nRx = a.nRx;
+    f.nD = a.nD;
+    f.c = a.c;
+    f.dt = a.dt;
+    f.F = a.F;
+    f.offset = a.offset;
+    return f;
+}
+
+int launchStaged(const sb_das_plan* p, const DasArgs& a, int rfDt, int outDt, cudaStream_t st) {
+    const size_t rfSize = rfDt == SB_INT16 ? 2 : 4;
+    const uint32_t maxW = stagedMaxW(p->numChannels, rfSize);
+    const size_t shm = ((sizeof(CtaState) + 127) & ~size_t(127)) + static_cast<size_t>(maxW) * p->numChannels * rfSize;
+    const uint32_t nChunks = (p->numDepths + kStagedThreads - 1) / kStagedThreads;
+    // enough CTAs to fill the GPU (about 3 resident per SM), fewer setups per scanline otherwise
+    uint32_t per = 1;
+    while (per < nChunks && static_cast<size_t>(p->numRx) * ((nChunks + per * 2 - 1) / (per * 2)) >= static_cast<size_t>(smCount()) * 6)
+        per *= 2;
+    dim3 grid((nChunks + per - 1) / per, p->numRx);
+    FrameDesc f = frameOf(p, a);
+    int* err = deviceErrorFlag();
+    if (!err) return fail(SB_ERR_NO_MEMORY, "error flag allocation failed");
+#define SB_STAGED(RFT, OUTT)                                                                                           \
+    do {                                                                                                               \
+        auto kern = dasStagedKernel<RFT, OUTT, kStagedThreads>;                                                        \
+        SB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)));       \
+        kern<<<grid, kStagedThreads, shm, st>>>(f, a.lut, a.out, maxW, per, err);                                      \
+    } while (0)
+    if (rfDt == SB_INT16 && outDt == SB_FLOAT32) SB_STAGED(int16_t, float);
+    else if (rfDt == SB_INT16) SB_STAGED(int16_t, int16_t);
+    else if (outDt == SB_FLOAT32) SB_STAGED(float, float);
+    else SB_STAGED(float, int16_t);
+#undef SB_STAGED
+    SB_CHECK_LAUNCH("dasStagedKernel");
     return SB_OK;
 }
 
@@ -424,6 +522,11 @@ int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out,
     int err = fillArgs(p, a, rf, out, f_number, speed_of_sound_mm_s, window_type, window_parameter,
                        interpolate_transmits, additional_offset, st);
     if (err != SB_OK) return err;
+    const size_t rfSize = rf_dtype == SB_INT16 ? 2 : 4;
+    const bool staged = !p->is3D && !interpolate_transmits && p->maxApertureX <= kMaxApertureElems &&
+                        (p->numSamples * rfSize) % 16 == 0 && (reinterpret_cast<uintptr_t>(rf) % 16) == 0 &&
+                        stagedMaxW(p->numChannels, rfSize) >= 64;
+    if (staged) return launchStaged(p, a, rf_dtype, out_dtype, st);
     dim3 grid((p->numDepths + 255) / 256, p->numRx);
 #define SB_DAS_LAUNCH(RFT, OUTT)                                                        \
     do {                                                                                \
