@@ -129,6 +129,26 @@ int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out,
                double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
                int interpolate_transmits, int32_t additional_offset, sb_stream stream);
 
+/* Allocation-free delay-and-sum, for callers that cannot allocate device memory: hosts that reserve
+ * their whole device budget up front and hand out buffers from their own pool (as SUPRA's container
+ * pool does), or real-time frame loops that cannot afford cudaMalloc/cudaFree (cudaFree synchronises
+ * the device). No counterpart in the reference. Same arguments and result as sb_das_plan_create +
+ * sb_das_run + sb_das_plan_destroy, but nothing is allocated: the geometry (host memory, read by
+ * copies enqueued on `stream`; if it is page-locked keep it unchanged until the stream has passed this
+ * call) is converted into a fixed scratch area in device memory that the library reserves statically
+ * (about 0.4 MB per GPU that loads the library, held until the process exits).
+ * Limits: num_elements <= SB_DAS_STATIC_MAX_ELEMENTS, num_depths <= SB_DAS_STATIC_MAX_DEPTHS,
+ * num_rx <= SB_DAS_STATIC_MAX_SCANLINES; larger geometries are rejected with SB_ERR_INVALID_ARG.
+ * The first call on a device looks up the scratch area's device address (once per device); make that
+ * first call before any stream capture. All calls share the one scratch area: calls whose work
+ * overlaps on the GPU (different streams, or threads) race and must be serialised by the caller. */
+#define SB_DAS_STATIC_MAX_ELEMENTS 1024
+#define SB_DAS_STATIC_MAX_DEPTHS 8192
+#define SB_DAS_STATIC_MAX_SCANLINES 1024
+int sb_das_run_static(const sb_geometry* geometry, const void* rf, int rf_dtype, void* out, int out_dtype,
+                      double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
+                      int interpolate_transmits, int32_t additional_offset, sb_stream stream);
+
 /* Replaces RawDelay::performDelay (Beamformer/RawDelay.cu:556-650): delayed, apodised and weight-
  * normalised channel samples, out [num_rx][num_channels][num_depths]; slots beyond the active
  * aperture are written as 0. */

@@ -7,6 +7,7 @@
 // _rn intrinsics, so nothing is contracted into FMAs), which keeps them bit-identical to the CPU
 // restatement of the reference.
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "das.cuh"
@@ -563,3 +564,182 @@ int sb_rawdelay_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void*
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free variant
+// sb_das_run_static: the per-frame DAS without any device allocation. Its scratch (the geometry as
+// given, the geometry in DT space, the wait-failure flag) lives in one statically reserved device
+// array; the launch is the same dtConvertKernel + DAS kernels as sb_das_run.
+namespace sb {
+namespace {
+
+constexpr size_t r256(size_t n) { return (n + 255) & ~size_t(255); }
+constexpr uint32_t kSE = SB_DAS_STATIC_MAX_ELEMENTS, kSD = SB_DAS_STATIC_MAX_DEPTHS, kSL = SB_DAS_STATIC_MAX_SCANLINES;
+constexpr size_t kOffXeMM = 0;
+constexpr size_t kOffYeMM = kOffXeMM + r256(kSE * sizeof(float));
+constexpr size_t kOffDepthMM = kOffYeMM + r256(kSE * sizeof(float));
+constexpr size_t kOffLinesMM = kOffDepthMM + r256(kSD * sizeof(float));
+constexpr size_t kOffE2C = kOffLinesMM + r256(kSL * sizeof(sb_scanline_rx));
+constexpr size_t kOffXe = kOffE2C + r256(kSE * sizeof(int32_t));
+constexpr size_t kOffYe = kOffXe + r256(kSE * sizeof(float));
+constexpr size_t kOffDepth = kOffYe + r256(kSE * sizeof(float));
+constexpr size_t kOffLines = kOffDepth + r256(kSD * sizeof(float));
+constexpr size_t kOffErr = kOffLines + r256(kSL * sizeof(LineDT));
+constexpr size_t kStaticScratchBytes = kOffErr + 256;
+
+}  // namespace
+}  // namespace sb
+
+// Device scratch of sb_das_run_static. In host code this name is only a stand-in for the device
+// array: its device address comes from cudaGetSymbolAddress (staticScratchBase).
+static __device__ __align__(256) unsigned char g_dasStaticScratch[sb::kStaticScratchBytes];
+
+namespace sb {
+namespace {
+
+std::mutex g_staticMutex;
+unsigned char* g_staticBase[64] = {nullptr};
+
+// Device address of the scratch array on the current device, looked up once per device.
+int staticScratchBase(unsigned char** base) {
+    int dev = 0;
+    SB_CUDA(cudaGetDevice(&dev));
+    SB_REQUIRE(dev >= 0 && dev < 64, "sb_das_run_static: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_staticMutex);
+    if (!g_staticBase[dev]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_dasStaticScratch);
+        if (e != cudaSuccess || !ptr) return cudaFail(e, "sb_das_run_static: cudaGetSymbolAddress");
+        g_staticBase[dev] = static_cast<unsigned char*>(ptr);
+    }
+    *base = g_staticBase[dev];
+    return SB_OK;
+}
+
+}  // namespace
+}  // namespace sb
+
+extern "C" int sb_das_run_static(const sb_geometry* g, const void* rf, int rf_dtype, void* out, int out_dtype,
+                                 double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
+                                 int interpolate_transmits, int32_t additional_offset, sb_stream stream) {
+    using namespace sb;
+    SB_REQUIRE(g && rf && out, "sb_das_run_static: null argument");
+    SB_REQUIRE(rf_dtype == SB_INT16 || rf_dtype == SB_FLOAT32, "sb_das_run_static: rf dtype %d unsupported", rf_dtype);
+    SB_REQUIRE(out_dtype == SB_FLOAT32 || out_dtype == SB_INT16, "sb_das_run_static: out dtype %d unsupported", out_dtype);
+    SB_REQUIRE(g->num_elements > 0 && g->num_channels > 0 && g->num_samples > 1 && g->num_tx > 0 && g->num_depths > 0,
+               "sb_das_run_static: empty geometry");
+    SB_REQUIRE(g->num_elements <= kSE && g->num_depths <= kSD && g->num_rx <= kSL,
+               "sb_das_run_static: geometry (%u elements, %u depths, %u scanlines) exceeds the static limits "
+               "(%u, %u, %u)", g->num_elements, g->num_depths, g->num_rx, kSE, kSD, kSL);
+    SB_REQUIRE(g->num_rx == g->rx_layout[0] * g->rx_layout[1] && g->num_rx > 0, "num_rx != rx_layout product");
+    SB_REQUIRE(g->element_layout[0] * g->element_layout[1] == g->num_elements, "element_layout != num_elements");
+    SB_REQUIRE(g->sampling_frequency_hz > 0, "sampling frequency must be > 0");
+    SB_REQUIRE(g->element_x_mm && g->element_y_mm && g->depths_mm && g->scanlines, "null geometry array");
+    SB_REQUIRE(f_number > 0.0 && speed_of_sound_mm_s > 0.0, "f-number and speed of sound must be > 0");
+    int err = checkWindow(window_type, window_parameter);
+    if (err != SB_OK) return err;
+    int32_t maxAx = 0;
+    for (uint32_t i = 0; i < g->num_rx; i++) {
+        const sb_scanline_rx& s = g->scanlines[i];
+        for (int k = 0; k < 4; k++) {
+            if (!(s.tx_weights[k] > 0.0)) continue;
+            SB_REQUIRE(s.tx[k].tx_scanline_idx < g->num_tx, "scanline %u: transmit index %u >= num_tx %u", i,
+                       s.tx[k].tx_scanline_idx, g->num_tx);
+            SB_REQUIRE(s.tx[k].last_active_element[0] <= g->element_layout[0] &&
+                           s.tx[k].last_active_element[1] <= g->element_layout[1],
+                       "scanline %u: aperture beyond the element layout", i);
+            maxAx = std::max(maxAx, static_cast<int32_t>(s.tx[k].last_active_element[0]) - s.tx[k].first_active_element[0]);
+        }
+    }
+    if (g->element_to_channel)
+        for (uint32_t e = 0; e < g->num_elements; e++)
+            SB_REQUIRE(g->element_to_channel[e] < static_cast<int32_t>(g->num_channels), "element %u maps to channel %d",
+                       e, g->element_to_channel[e]);
+    unsigned char* base = nullptr;
+    err = staticScratchBase(&base);
+    if (err != SB_OK) return err;
+    cudaStream_t st = S(stream);
+    float* xeMM = reinterpret_cast<float*>(base + kOffXeMM);
+    float* yeMM = reinterpret_cast<float*>(base + kOffYeMM);
+    float* dMM = reinterpret_cast<float*>(base + kOffDepthMM);
+    sb_scanline_rx* linesMM = reinterpret_cast<sb_scanline_rx*>(base + kOffLinesMM);
+    int32_t* e2c = reinterpret_cast<int32_t*>(base + kOffE2C);
+    float* xe = reinterpret_cast<float*>(base + kOffXe);
+    float* ye = reinterpret_cast<float*>(base + kOffYe);
+    float* dDT = reinterpret_cast<float*>(base + kOffDepth);
+    LineDT* lines = reinterpret_cast<LineDT*>(base + kOffLines);
+    int* flag = reinterpret_cast<int*>(base + kOffErr);
+    const size_t nE = g->num_elements, nD = g->num_depths, nRx = g->num_rx;
+    SB_CUDA(cudaMemcpyAsync(xeMM, g->element_x_mm, nE * sizeof(float), cudaMemcpyHostToDevice, st));
+    SB_CUDA(cudaMemcpyAsync(yeMM, g->element_y_mm, nE * sizeof(float), cudaMemcpyHostToDevice, st));
+    SB_CUDA(cudaMemcpyAsync(dMM, g->depths_mm, nD * sizeof(float), cudaMemcpyHostToDevice, st));
+    SB_CUDA(cudaMemcpyAsync(linesMM, g->scanlines, nRx * sizeof(sb_scanline_rx), cudaMemcpyHostToDevice, st));
+    if (g->element_to_channel)
+        SB_CUDA(cudaMemcpyAsync(e2c, g->element_to_channel, nE * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    SB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));  // the wait-failure flag starts clear on every call
+    const double dt = 1.0 / g->sampling_frequency_hz;
+    const double factor = 1 / 1.0 / (speed_of_sound_mm_s * dt);
+    const double factorTime = 1 / 1.0 / dt;
+    const uint32_t n = std::max(std::max(g->num_elements, g->num_depths), g->num_rx);
+    dtConvertKernel<<<(n + 255) / 256, 256, 0, st>>>(xeMM, yeMM, g->num_elements, dMM, g->num_depths, linesMM,
+                                                     g->num_rx, factor, factorTime, xe, ye, dDT, lines);
+    SB_CHECK_LAUNCH("sb_das_run_static: dtConvertKernel");
+    DasArgs a;
+    a.rf = rf;
+    a.out = out;
+    a.xe = xe;
+    a.ye = ye;
+    a.depth = dDT;
+    a.lines = lines;
+    a.e2c = g->element_to_channel ? e2c : nullptr;
+    a.apod = nullptr;
+    a.nE = g->num_elements;
+    a.layoutX = g->element_layout[0];
+    a.nCh = g->num_channels;
+    a.nS = g->num_samples;
+    a.nTx = g->num_tx;
+    a.nRx = g->num_rx;
+    a.nD = g->num_depths;
+    a.c = static_cast<float>(speed_of_sound_mm_s);
+    a.dt = static_cast<float>(dt);
+    a.F = static_cast<float>(f_number);
+    a.offset = static_cast<float>(additional_offset);
+    a.interpTx = interpolate_transmits ? 1 : 0;
+    a.lut = makeLut(window_type, window_parameter);
+    const bool is3D = g->rx_layout[0] > 1 && g->rx_layout[1] > 1;
+    const size_t rfSize = rf_dtype == SB_INT16 ? 2 : 4;
+    const uint32_t maxW = stagedMaxW(g->num_channels, rfSize);
+    const bool staged = !is3D && !interpolate_transmits && maxAx <= kMaxApertureElems && (g->num_samples * rfSize) % 16 == 0 &&
+                        (reinterpret_cast<uintptr_t>(rf) % 16) == 0 && maxW >= 64;
+    if (staged) {
+        const size_t shm = ((sizeof(CtaState) + 127) & ~size_t(127)) + static_cast<size_t>(maxW) * g->num_channels * rfSize;
+        const uint32_t nChunks = (g->num_depths + kStagedThreads - 1) / kStagedThreads;
+        dim3 grid(nChunks, g->num_rx);
+        FrameDesc f = frameOf(nullptr, a);
+#define SB_STATIC_STAGED(RFT, OUTT)                                                                                    \
+    do {                                                                                                               \
+        auto kern = dasStagedKernel<RFT, OUTT, kStagedThreads>;                                                        \
+        SB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)));       \
+        kern<<<grid, kStagedThreads, shm, st>>>(f, a.lut, a.out, maxW, 1u, flag);                                      \
+    } while (0)
+        if (rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_STATIC_STAGED(int16_t, float);
+        else if (rf_dtype == SB_INT16) SB_STATIC_STAGED(int16_t, int16_t);
+        else if (out_dtype == SB_FLOAT32) SB_STATIC_STAGED(float, float);
+        else SB_STATIC_STAGED(float, int16_t);
+#undef SB_STATIC_STAGED
+        SB_CHECK_LAUNCH("sb_das_run_static: dasStagedKernel");
+        return SB_OK;
+    }
+    dim3 grid((g->num_depths + 255) / 256, g->num_rx);
+#define SB_STATIC_GENERIC(RFT, OUTT)                                                   \
+    do {                                                                               \
+        if (is3D) dasKernel<RFT, OUTT, true><<<grid, 256, 0, st>>>(a);                \
+        else dasKernel<RFT, OUTT, false><<<grid, 256, 0, st>>>(a);                    \
+    } while (0)
+    if (rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_STATIC_GENERIC(int16_t, float);
+    else if (rf_dtype == SB_INT16) SB_STATIC_GENERIC(int16_t, int16_t);
+    else if (out_dtype == SB_FLOAT32) SB_STATIC_GENERIC(float, float);
+    else SB_STATIC_GENERIC(float, int16_t);
+#undef SB_STATIC_GENERIC
+    SB_CHECK_LAUNCH("sb_das_run_static: dasKernel");
+    return SB_OK;
+}
