@@ -254,9 +254,11 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "frames_per_launch": len(wl.rf), "beamformed_px_per_launch": px,
                        "parallelism": f"replicas x{world}", "l2": "inputs 2.47 GB per launch > L2, no flush",
-                       "tile_shape": {"ctas_per_sm": shape[0], "depth_tile": shape[1]}, "graph_captured": True},
+                       "tile_shape": {"ctas_per_sm": shape[0], "depth_tile": shape[1], "frames_per_pack": shape[2]},
+                       "graph_captured": True},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": traffic, "peak_kind": peak_kind, "kernel": "batchDasIqKernel",
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "batchPackKernel" if shape[2] > 1 else "batchDasIqKernel",
                          "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

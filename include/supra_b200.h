@@ -266,11 +266,14 @@ typedef struct sb_batch_params {
     double cutoff_frequency_hz;
     uint32_t lowpass_length;   /* taps of the decimation low-pass */
     uint32_t decimation;
-    int32_t ctas_per_sm;       /* tile shape: resident CTAs per SM, 1..3 (0 = default / autotuned) */
-    int32_t depth_tile;        /* tile shape: depths per chunk, 128 or 256 (0 = default / autotuned) */
+    int32_t ctas_per_sm;       /* persistent CTAs per SM (0 = default / autotuned) */
+    int32_t depth_tile;        /* depths per chunk / per CTA block: 128, 256, 384 or 512 (0 = default) */
+    int32_t frames_per_pack;   /* 1: per-frame TMA-staged pipeline; 2, 4 or 8: frames of one probe share the
+                                  per-element geometry work (0 = default / autotuned) */
 } sb_batch_params;
 
-/* Persistent batched DAS + complex IQ over frames of uneven probes in one launch. */
+/* Persistent batched DAS + complex IQ over frames of uneven probes in one launch. Frames whose
+ * `probe` plans are the same object are grouped: they share delays, apertures and weights. */
 int sb_batch_plan_create(const sb_batch_frame* frames, uint32_t num_frames, const sb_batch_params* params,
                          sb_batch_plan** plan);
 int sb_batch_plan_destroy(sb_batch_plan* plan);
@@ -281,7 +284,7 @@ int sb_batch_set_rf_outputs(sb_batch_plan* plan, float* const* rf_out);
 /* Time candidate tile shapes on the device and keep the fastest; cache_path (may be NULL) stores
  * the choice per problem signature and is consulted first. Returns the chosen shape. Synchronises. */
 int sb_batch_autotune(sb_batch_plan* plan, const char* cache_path, int32_t* ctas_per_sm, int32_t* depth_tile,
-                      sb_stream stream);
+                      int32_t* frames_per_pack, sb_stream stream);
 
 /* Device-side failure flag shared by the kernels with bounded waits: returns SB_ERR_TIMEOUT if any
  * wait gave up since the last call (and clears the flag when reset != 0). Synchronises the device. */

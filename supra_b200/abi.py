@@ -118,6 +118,7 @@ class sb_batch_params(C.Structure):
         ("decimation", C.c_uint32),
         ("ctas_per_sm", C.c_int32),
         ("depth_tile", C.c_int32),
+        ("frames_per_pack", C.c_int32),
     ]
 
 
@@ -166,7 +167,7 @@ _SIGNATURES = {
     "sb_batch_plan_destroy": (_int, [_vp]),
     "sb_batch_run": (_int, [_vp, _int, _vp]),
     "sb_batch_set_rf_outputs": (_int, [_vp, _vp]),
-    "sb_batch_autotune": (_int, [_vp, C.c_char_p, C.POINTER(_i32), C.POINTER(_i32), _vp]),
+    "sb_batch_autotune": (_int, [_vp, C.c_char_p, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), _vp]),
     "sb_check_device_errors": (_int, [_int]),
     "sb_das_forward_apod": (_int, [_vp, _vp, _vp, _vp, _f64, _f64, _int, _f32, _vp]),
     "sb_das_adjoint": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _f64, _f64, _int, _f32, _vp]),

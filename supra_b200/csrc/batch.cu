@@ -21,6 +21,8 @@
 #include <vector>
 
 #include "das_core.cuh"
+#include "das_ws.cuh"
+#include "batch_pack.cuh"
 #include "design.h"
 #include "envelope.cuh"
 
@@ -53,92 +55,130 @@ struct BatchArgs {
     float lp[kIqMaxTaps + 1];
 };
 
-constexpr size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
+__host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
 
-template <int NT>
-__global__ void __launch_bounds__(NT) batchDasIqKernel(BatchArgs a) {
+// Bounded wait helper for the pipeline: returns false (and flags the error) when it gives up.
+__device__ __forceinline__ bool waitOrFlag(uint64_t* bar, uint32_t parity, int* err) {
+    if (mbarWaitBounded(bar, parity, kWaitLimit)) return true;
+    atomicExch(err, 1);
+    return false;
+}
+
+// NC consumer warps + 1 producer warp; chunk = NC * 32 depths.
+template <int NC>
+__global__ void __launch_bounds__((NC + 1) * 32) batchDasIqKernel(BatchArgs a) {
+    constexpr int CH = NC * 32;
     extern __shared__ __align__(128) unsigned char smraw[];
-    CtaState& st = *reinterpret_cast<CtaState*>(smraw);
-    int16_t* smemRF = reinterpret_cast<int16_t*>(smraw + align128(sizeof(CtaState)));
-    float* lineBuf = reinterpret_cast<float*>(smraw + align128(sizeof(CtaState)) +
-                                              align128(static_cast<size_t>(2) * a.maxCh * a.maxW * sizeof(int16_t)));
-    __shared__ uint32_t itemIdx;
-    const int tid = threadIdx.x;
-    if (tid < 64) st.lut[tid] = a.lut.v[tid];
-    if (tid == 0) {
-        mbarInit(&st.bar[0], 1);
-        mbarInit(&st.bar[1], 1);
+    WsState& st = *reinterpret_cast<WsState*>(smraw);
+    int16_t* stages = reinterpret_cast<int16_t*>(smraw + align128(sizeof(WsState)));
+    float* lineBuf = reinterpret_cast<float*>(smraw + align128(sizeof(WsState)) +
+                                              align128(static_cast<size_t>(kStages) * a.maxCh * a.maxW * sizeof(int16_t)));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x < 64) st.lut[threadIdx.x] = a.lut.v[threadIdx.x];
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kStages; i++) {
+            mbarInit(&st.full[i], 1);
+            mbarInit(&st.empty[i], NC);
+        }
+        mbarInit(&st.slotFree[0], 1);
+        mbarInit(&st.slotFree[1], 1);
         mbarInitFence();
-        st.phase[0] = st.phase[1] = 0;
     }
     __syncthreads();
-    for (;;) {
-        if (tid == 0) itemIdx = atomicAdd(a.counter, 1u);
-        __syncthreads();
-        const uint32_t it = itemIdx;
-        if (it >= a.nItems) break;
-        const BatchItem bi = a.items[it];
-        const BatchFrameDev& fr = a.frames[bi.frame];
-        const FrameDesc f = fr.f;
-        const uint32_t line = bi.line;
-        const LineK s = reduceLine(f.lines[line]);
-        const bool ok = setupLine<NT>(st, f, s);
-        const bool useOffset = f.offset != 0.0f;
-        const uint32_t nChunks = (f.nD + NT - 1) / NT;
-        bool failed = false;
-        if (ok) {
-            planChunk<int16_t, NT>(st, smemRF, 0, f, s, 0, a.maxW, a.maxW, useOffset);
+    if (warp == 0) {
+        // ---------------------------------------------------------------- producer
+        uint32_t chunkCount = 0;
+        uint32_t slotUse[2] = {0, 0};
+        int slotIdx = 0;
+        for (;;) {
+            uint32_t it = 0;
+            if (lane == 0) it = atomicAdd(a.counter, 1u);
+            it = __shfl_sync(0xffffffffu, it, 0);
+            if (it >= a.nItems) {
+                const int stage = chunkCount % kStages;
+                if (!waitOrFlag(&st.empty[stage], ((chunkCount / kStages) & 1) ^ 1, a.err)) return;
+                if (lane == 0) {
+                    st.meta[stage].flags = 2;
+                    mbarArrive(&st.full[stage]);
+                }
+                return;
+            }
+            if (!waitOrFlag(&st.slotFree[slotIdx], (slotUse[slotIdx] & 1) ^ 1, a.err)) return;
+            slotUse[slotIdx]++;
+            LineSlot& sl = st.slot[slotIdx];
+            const BatchItem bi = a.items[it];
+            const BatchFrameDev& fr = a.frames[bi.frame];
+            if (lane == 0) {
+                sl.f = fr.f;
+                sl.frame = bi.frame;
+                sl.line = bi.line;
+                sl.s = reduceLine(fr.f.lines[bi.line]);
+            }
+            __syncwarp();
+            producerSetupLine(sl, st.lut, lane);
+            const uint32_t nD = sl.f.nD;
+            const uint32_t nChunks = (nD + CH - 1) / CH;
             for (uint32_t c = 0; c < nChunks; c++) {
-                const int b = c & 1;
-                if (c + 1 < nChunks) planChunk<int16_t, NT>(st, smemRF, b ^ 1, f, s, (c + 1) * NT, a.maxW, a.maxW, useOffset);
-                if (!waitChunk(st, b)) {
-                    failed = true;
-                    break;
-                }
-                const uint32_t r = c * NT + tid;
-                if (r < f.nD) {
-                    const float v = clampCast<float>(dasDepth<int16_t>(st, smemRF, b, a.maxW, f, s, r, useOffset));
-                    lineBuf[r] = v;
-                    if (fr.rfOut) fr.rfOut[line + static_cast<size_t>(r) * f.nRx] = v;
-                }
-                __syncthreads();
+                const int stage = chunkCount % kStages;
+                if (!waitOrFlag(&st.empty[stage], ((chunkCount / kStages) & 1) ^ 1, a.err)) return;
+                producerIssueChunk<CH>(st, stages, stage, slotIdx, c * CH, c + 1 == nChunks, a.maxW, lane);
+                chunkCount++;
             }
-        } else {
-            for (uint32_t r = tid; r < f.nD; r += NT) {
-                lineBuf[r] = 0.0f;
-                if (fr.rfOut) fr.rfOut[line + static_cast<size_t>(r) * f.nRx] = 0.0f;
+            slotIdx ^= 1;
+        }
+    }
+    // -------------------------------------------------------------------- consumers
+    const int ctid = threadIdx.x - 32;
+    uint32_t chunkCount = 0;
+    for (;;) {
+        const int stage = chunkCount % kStages;
+        if (!waitOrFlag(&st.full[stage], (chunkCount / kStages) & 1, a.err)) return;
+        const StageMeta m = st.meta[stage];
+        if (m.flags & 2) return;
+        const LineSlot& sl = st.slot[m.slot];
+        const BatchFrameDev& fr = a.frames[sl.frame];
+        const uint32_t r = m.r0 + ctid;
+        if (r < sl.f.nD) {
+            float v = 0.0f;
+            if (sl.valid) {
+                const int16_t* stg = stages + static_cast<size_t>(stage) * sl.f.nCh * a.maxW;
+                v = sl.f.offset != 0.0f ? consumerDepth<true>(sl, st.lut, m, stg, a.maxW, r)
+                                        : consumerDepth<false>(sl, st.lut, m, stg, a.maxW, r);
             }
+            v = clampCast<float>(v);
+            lineBuf[r] = v;
+            if (fr.rfOut) fr.rfOut[sl.line + static_cast<size_t>(r) * sl.f.nRx] = v;
         }
-        if (failed) {
-            if (tid == 0) atomicExch(a.err, 1);
-            mbarWaitBounded(&st.bar[0], st.phase[0], kWaitLimit);
-            mbarWaitBounded(&st.bar[1], st.phase[1], kWaitLimit);
-            return;
-        }
-        __syncthreads();
-        // complex baseband IQ of the scanline: taps j = 0 .. taps-1 centred on sample so * dec
-        const int nD = static_cast<int>(f.nD);
-        const int nOut = nD / a.dec;
-        for (int so = tid; so < nOut; so += NT) {
-            float re = 0.0f, im = 0.0f;
-            const int base = so * a.dec - a.half;
-            for (int j = 0; j < a.taps; j++) {
-                const int n = base + j;
-                if (n >= 0 && n < nD) {
-                    const float x = lineBuf[n] * a.lp[j];
-                    const float2 w = __ldg(a.rot + n);
-                    re = fmaf(x, w.x, re);
-                    im = fmaf(x, w.y, im);
+        __syncwarp();
+        if (lane == 0) mbarArrive(&st.empty[stage]);
+        chunkCount++;
+        if (m.flags & 1) {
+            consumerBarrier(CH);
+            // complex baseband IQ of the scanline: taps j = 0 .. taps-1 centred on sample so * dec
+            const int nD = static_cast<int>(sl.f.nD);
+            const int nOut = nD / a.dec;
+            for (int so = ctid; so < nOut; so += CH) {
+                float re = 0.0f, im = 0.0f;
+                const int base = so * a.dec - a.half;
+                for (int j = 0; j < a.taps; j++) {
+                    const int n = base + j;
+                    if (n >= 0 && n < nD) {
+                        const float x = lineBuf[n] * a.lp[j];
+                        const float2 w = __ldg(a.rot + n);
+                        re = fmaf(x, w.x, re);
+                        im = fmaf(x, w.y, im);
+                    }
                 }
+                fr.iq[sl.line + static_cast<size_t>(so) * sl.f.nRx] = make_float2(re, im);
             }
-            fr.iq[line + static_cast<size_t>(so) * f.nRx] = make_float2(re, im);
+            consumerBarrier(CH);
+            if (ctid == 0) mbarArrive(&st.slotFree[m.slot]);
         }
-        __syncthreads();
     }
 }
 
 size_t batchSmem(uint32_t maxCh, uint32_t maxW, uint32_t maxD) {
-    return align128(sizeof(CtaState)) + align128(static_cast<size_t>(2) * maxCh * maxW * sizeof(int16_t)) +
+    return align128(sizeof(WsState)) + align128(static_cast<size_t>(kStages) * maxCh * maxW * sizeof(int16_t)) +
            align128(static_cast<size_t>(maxD) * sizeof(float));
 }
 
@@ -147,9 +187,17 @@ size_t batchSmem(uint32_t maxCh, uint32_t maxW, uint32_t maxD) {
 
 using namespace sb;
 
+struct PackSet {
+    PackDev* dPacks = nullptr;
+    PackItem* dItems = nullptr;
+    uint32_t nItems = 0;
+};
+
 struct sb_batch_plan {
     std::vector<sb_batch_frame> frames;
     sb_batch_params params;
+    PackSet packs[4];  // frames per pack 1 (unused), 2, 4, 8
+    int fp = 8;
     BatchFrameDev* dFrames = nullptr;
     BatchItem* dItems = nullptr;
     float2* dRot = nullptr;
@@ -160,7 +208,7 @@ struct sb_batch_plan {
     int nt = 256, ctasPerSm = 2;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
-    int graphNt = 0, graphCtas = 0;
+    int graphNt = 0, graphCtas = 0, graphFp = 0;
     std::string signature;
 };
 
@@ -177,25 +225,131 @@ uint32_t batchMaxW(uint32_t maxCh, uint32_t maxD, int ctasPerSm) {
     size_t budget = std::min<size_t>(static_cast<size_t>(smemPerSm) / ctasPerSm - 2048, static_cast<size_t>(smemPerBlock));
     size_t fixed = batchSmem(maxCh, 0, maxD) + 256;
     if (budget <= fixed) return 0;
-    size_t w = (budget - fixed) / (2 * static_cast<size_t>(maxCh) * sizeof(int16_t));
+    size_t w = (budget - fixed) / (kStages * static_cast<size_t>(maxCh) * sizeof(int16_t));
     w &= ~size_t(7);
     return static_cast<uint32_t>(std::min<size_t>(w, 4096));
 }
 
-int launchBatch(sb_batch_plan* p, int nt, int ctas, cudaStream_t st) {
+int packSlot(int fp) { return fp == 2 ? 1 : fp == 4 ? 2 : fp == 8 ? 3 : -1; }
+
+// Groups frames by probe plan into packs of up to fp frames; items (pack, line, depth segment),
+// longest first.
+int buildPacks(sb_batch_plan* p, int fp) {
+    const int slot = packSlot(fp);
+    if (slot < 0) return fail(SB_ERR_INVALID_ARG, "sb_batch: frames_per_pack %d not in {1, 2, 4, 8}", fp);
+    PackSet& ps = p->packs[slot];
+    if (ps.dPacks) return SB_OK;
+    std::vector<PackDev> packs;
+    std::vector<const sb_das_plan*> probes;
+    for (const auto& fr : p->frames)
+        if (std::find(probes.begin(), probes.end(), fr.probe) == probes.end()) probes.push_back(fr.probe);
+    for (const sb_das_plan* probe : probes) {
+        std::vector<size_t> idx;
+        for (size_t i = 0; i < p->frames.size(); i++)
+            if (p->frames[i].probe == probe) idx.push_back(i);
+        for (size_t b = 0; b < idx.size(); b += fp) {
+            const BatchFrameDev& f0 = p->hFrames[idx[b]];
+            PackDev d;
+            std::memset(&d, 0, sizeof(d));
+            d.lines = f0.f.lines;
+            d.xe = f0.f.xe;
+            d.depth = f0.f.depth;
+            d.e2c = f0.f.e2c;
+            d.nCh = f0.f.nCh;
+            d.nS = f0.f.nS;
+            d.nRx = f0.f.nRx;
+            d.nD = f0.f.nD;
+            d.c = f0.f.c;
+            d.dt = f0.f.dt;
+            d.F = f0.f.F;
+            d.offset = f0.f.offset;
+            d.nf = static_cast<int>(std::min<size_t>(fp, idx.size() - b));
+            for (int k = 0; k < d.nf; k++) {
+                const BatchFrameDev& fk = p->hFrames[idx[b + k]];
+                d.rf[k] = static_cast<const int16_t*>(fk.f.rf);
+                d.iq[k] = fk.iq;
+                d.rfOut[k] = fk.rfOut;
+            }
+            packs.push_back(d);
+        }
+    }
+    const int dec = p->args.dec;
+    const uint32_t seg = static_cast<uint32_t>(1024 - (1024 % dec));
+    std::vector<PackItem> items;
+    for (uint32_t k = 0; k < packs.size(); k++)
+        for (uint32_t l = 0; l < packs[k].nRx; l++)
+            for (uint32_t s0 = 0; s0 < packs[k].nD; s0 += seg) items.push_back({k, l, s0, std::min(packs[k].nD, s0 + seg)});
+    std::stable_sort(items.begin(), items.end(), [&](const PackItem& a, const PackItem& b) {
+        return static_cast<uint64_t>(a.seg1 - a.seg0) * packs[a.pack].nf > static_cast<uint64_t>(b.seg1 - b.seg0) * packs[b.pack].nf;
+    });
+    cudaError_t e = cudaMalloc(&ps.dPacks, packs.size() * sizeof(PackDev));
+    if (e == cudaSuccess) e = cudaMalloc(&ps.dItems, items.size() * sizeof(PackItem));
+    if (e == cudaSuccess) e = cudaMemcpy(ps.dPacks, packs.data(), packs.size() * sizeof(PackDev), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ps.dItems, items.data(), items.size() * sizeof(PackItem), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(ps.dPacks);
+        cudaFree(ps.dItems);
+        ps.dPacks = nullptr;
+        ps.dItems = nullptr;
+        return cudaFail(e, "sb_batch: pack tables");
+    }
+    ps.nItems = static_cast<uint32_t>(items.size());
+    return SB_OK;
+}
+
+void freePacks(sb_batch_plan* p) {
+    for (auto& ps : p->packs) {
+        cudaFree(ps.dPacks);
+        cudaFree(ps.dItems);
+        ps = PackSet();
+    }
+}
+
+int launchBatch(sb_batch_plan* p, int nt, int ctas, int fp, cudaStream_t st) {
+    const int grid = smCount() * ctas;
+    if (fp > 1) {
+        int e = buildPacks(p, fp);
+        if (e != SB_OK) return e;
+        const PackSet& ps = p->packs[packSlot(fp)];
+        PackArgs a;
+        a.packs = ps.dPacks;
+        a.items = ps.dItems;
+        a.nItems = ps.nItems;
+        a.counter = p->dCounter;
+        a.rot = p->dRot;
+        a.taps = p->args.taps;
+        a.half = p->args.half;
+        a.dec = p->args.dec;
+        a.lut = p->args.lut;
+        for (int j = 0; j <= kIqMaxTaps; j++) a.lp[j] = p->args.lp[j];
+        SB_CUDA(cudaMemsetAsync(p->dCounter, 0, sizeof(uint32_t), st));
+#define SB_PACK_LAUNCH(FPV, NTV) batchPackKernel<FPV, NTV><<<grid, NTV, 0, st>>>(a)
+        if (nt != 128 && nt != 256) return fail(SB_ERR_INVALID_ARG, "sb_batch: pack kernel block %d not in {128, 256}", nt);
+        if (fp == 2) { if (nt == 128) SB_PACK_LAUNCH(2, 128); else SB_PACK_LAUNCH(2, 256); }
+        else if (fp == 4) { if (nt == 128) SB_PACK_LAUNCH(4, 128); else SB_PACK_LAUNCH(4, 256); }
+        else { if (nt == 128) SB_PACK_LAUNCH(8, 128); else SB_PACK_LAUNCH(8, 256); }
+#undef SB_PACK_LAUNCH
+        SB_CHECK_LAUNCH("batchPackKernel");
+        return SB_OK;
+    }
     BatchArgs a = p->args;
     a.maxW = batchMaxW(p->maxCh, p->maxD, ctas);
     if (a.maxW < 64) return fail(SB_ERR_UNSUPPORTED, "sb_batch: shape (%d CTAs/SM) leaves no room to stage samples", ctas);
     const size_t shm = batchSmem(p->maxCh, a.maxW, p->maxD);
-    const int grid = smCount() * ctas;
     SB_CUDA(cudaMemsetAsync(p->dCounter, 0, sizeof(uint32_t), st));
-    if (nt == 128) {
-        SB_CUDA(cudaFuncSetAttribute(batchDasIqKernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)));
-        batchDasIqKernel<128><<<grid, 128, shm, st>>>(a);
-    } else {
-        SB_CUDA(cudaFuncSetAttribute(batchDasIqKernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)));
-        batchDasIqKernel<256><<<grid, 256, shm, st>>>(a);
+#define SB_BATCH_LAUNCH(NCW)                                                                                          \
+    do {                                                                                                              \
+        SB_CUDA(cudaFuncSetAttribute(batchDasIqKernel<NCW>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm))); \
+        batchDasIqKernel<NCW><<<grid, (NCW + 1) * 32, shm, st>>>(a);                                                   \
+    } while (0)
+    switch (nt) {
+    case 128: SB_BATCH_LAUNCH(4); break;
+    case 256: SB_BATCH_LAUNCH(8); break;
+    case 384: SB_BATCH_LAUNCH(12); break;
+    case 512: SB_BATCH_LAUNCH(16); break;
+    default: return fail(SB_ERR_INVALID_ARG, "sb_batch: depth tile %d not in {128, 256, 384, 512}", nt);
     }
+#undef SB_BATCH_LAUNCH
     SB_CHECK_LAUNCH("batchDasIqKernel");
     return SB_OK;
 }
@@ -220,9 +374,13 @@ int sb_batch_plan_create(const sb_batch_frame* frames, uint32_t num_frames, cons
                "sb_batch_plan_create: low-pass length must be in [1, %d)", kIqMaxTaps);
     SB_REQUIRE(params->decimation >= 1, "sb_batch_plan_create: decimation must be >= 1");
     SB_REQUIRE(params->window_type >= 0 && params->window_type <= 3, "sb_batch_plan_create: window type");
-    SB_REQUIRE(params->depth_tile == 0 || params->depth_tile == 128 || params->depth_tile == 256,
-               "sb_batch_plan_create: depth_tile must be 0, 128 or 256");
-    SB_REQUIRE(params->ctas_per_sm >= 0 && params->ctas_per_sm <= 3, "sb_batch_plan_create: ctas_per_sm in [0, 3]");
+    SB_REQUIRE(params->depth_tile == 0 || params->depth_tile == 128 || params->depth_tile == 256 ||
+                   params->depth_tile == 384 || params->depth_tile == 512,
+               "sb_batch_plan_create: depth_tile must be 0, 128, 256, 384 or 512");
+    SB_REQUIRE(params->ctas_per_sm >= 0 && params->ctas_per_sm <= 8, "sb_batch_plan_create: ctas_per_sm in [0, 8]");
+    SB_REQUIRE(params->frames_per_pack == 0 || params->frames_per_pack == 1 || params->frames_per_pack == 2 ||
+                   params->frames_per_pack == 4 || params->frames_per_pack == 8,
+               "sb_batch_plan_create: frames_per_pack must be 0, 1, 2, 4 or 8");
     sb_batch_plan* p = new sb_batch_plan();
     p->frames.assign(frames, frames + num_frames);
     p->params = *params;
@@ -315,11 +473,13 @@ int sb_batch_plan_create(const sb_batch_frame* frames, uint32_t num_frames, cons
     std::vector<float> lp = firDesign(params->lowpass_length, 0, 2, fs0, params->cutoff_frequency_hz, 0.0);
     for (int j = 0; j <= kIqMaxTaps; j++) a.lp[j] = j < static_cast<int>(params->lowpass_length) ? lp[j] : 0.0f;
     a.lut = makeLut(params->window_type, params->window_parameter);
-    p->nt = params->depth_tile ? params->depth_tile : 256;
-    p->ctasPerSm = params->ctas_per_sm ? params->ctas_per_sm : 2;
+    p->fp = params->frames_per_pack ? params->frames_per_pack : 8;
+    p->nt = params->depth_tile ? params->depth_tile : (p->fp > 1 ? 256 : 384);
+    p->ctasPerSm = params->ctas_per_sm ? params->ctas_per_sm : (p->fp > 1 ? 4 : 1);
     sig << "F" << params->f_number << "L" << params->lowpass_length << "D" << params->decimation;
     p->signature = sig.str();
-    if (batchMaxW(p->maxCh, p->maxD, p->ctasPerSm) < 64) return bad(fail(SB_ERR_UNSUPPORTED, "sb_batch_plan_create: frames too large to stage"));
+    if (p->fp == 1 && batchMaxW(p->maxCh, p->maxD, p->ctasPerSm) < 64)
+        return bad(fail(SB_ERR_UNSUPPORTED, "sb_batch_plan_create: frames too large to stage"));
     *plan = p;
     return SB_OK;
 }
@@ -327,6 +487,7 @@ int sb_batch_plan_create(const sb_batch_frame* frames, uint32_t num_frames, cons
 int sb_batch_plan_destroy(sb_batch_plan* p) {
     if (!p) return SB_OK;
     dropGraph(p);
+    freePacks(p);
     cudaFree(p->dFrames);
     cudaFree(p->dItems);
     cudaFree(p->dRot);
@@ -339,21 +500,27 @@ int sb_batch_set_rf_outputs(sb_batch_plan* p, float* const* rf_out) {
     SB_REQUIRE(p, "sb_batch_set_rf_outputs: null plan");
     for (size_t i = 0; i < p->hFrames.size(); i++) p->hFrames[i].rfOut = rf_out ? rf_out[i] : nullptr;
     SB_CUDA(cudaMemcpy(p->dFrames, p->hFrames.data(), p->hFrames.size() * sizeof(BatchFrameDev), cudaMemcpyHostToDevice));
+    freePacks(p);  // pack tables embed the output pointers
+    dropGraph(p);
     return SB_OK;
 }
 
 int sb_batch_run(sb_batch_plan* p, int use_graph, sb_stream stream) {
     SB_REQUIRE(p, "sb_batch_run: null plan");
     cudaStream_t st = S(stream);
-    if (!use_graph) return launchBatch(p, p->nt, p->ctasPerSm, st);
-    if (!p->graphExec || p->graphNt != p->nt || p->graphCtas != p->ctasPerSm) {
+    if (!use_graph) return launchBatch(p, p->nt, p->ctasPerSm, p->fp, st);
+    if (p->fp > 1) {
+        int e = buildPacks(p, p->fp);  // outside the capture: it allocates
+        if (e != SB_OK) return e;
+    }
+    if (!p->graphExec || p->graphNt != p->nt || p->graphCtas != p->ctasPerSm || p->graphFp != p->fp) {
         dropGraph(p);
         // capture on a private stream so that the caller's stream may be the legacy default stream
         cudaStream_t cap;
         SB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         int r = SB_OK;
-        if (e == cudaSuccess) r = launchBatch(p, p->nt, p->ctasPerSm, cap);
+        if (e == cudaSuccess) r = launchBatch(p, p->nt, p->ctasPerSm, p->fp, cap);
         cudaGraph_t g = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(cap, &g);
         cudaStreamDestroy(cap);
@@ -367,45 +534,54 @@ int sb_batch_run(sb_batch_plan* p, int use_graph, sb_stream stream) {
         SB_CUDA(cudaGraphInstantiate(&p->graphExec, g, 0));
         p->graphNt = p->nt;
         p->graphCtas = p->ctasPerSm;
+        p->graphFp = p->fp;
     }
     SB_CUDA(cudaGraphLaunch(p->graphExec, st));
     return SB_OK;
 }
 
 int sb_batch_autotune(sb_batch_plan* p, const char* cache_path, int32_t* ctas_per_sm, int32_t* depth_tile,
-                      sb_stream stream) {
+                      int32_t* frames_per_pack, sb_stream stream) {
     SB_REQUIRE(p, "sb_batch_autotune: null plan");
     cudaStream_t st = S(stream);
+    auto report = [&]() {
+        if (ctas_per_sm) *ctas_per_sm = p->ctasPerSm;
+        if (depth_tile) *depth_tile = p->nt;
+        if (frames_per_pack) *frames_per_pack = p->fp;
+    };
     // cached choice for this problem signature?
     if (cache_path) {
         std::ifstream in(cache_path);
         std::string key, line;
         while (std::getline(in, line)) {
             std::istringstream ls(line);
-            int c = 0, t = 0;
-            if (ls >> key >> c >> t && key == p->signature && (t == 128 || t == 256) && c >= 1 && c <= 3 &&
-                batchMaxW(p->maxCh, p->maxD, c) >= 64) {
+            int c = 0, t = 0, f = 0;
+            if (!(ls >> key >> c >> t >> f) || key != p->signature) continue;
+            const bool okPack = f > 1 && packSlot(f) >= 0 && (t == 128 || t == 256) && c >= 1 && c <= 8;
+            const bool okPipe = f == 1 && (t == 128 || t == 256 || t == 384 || t == 512) && c >= 1 && c <= 3 &&
+                                batchMaxW(p->maxCh, p->maxD, c) >= 64;
+            if (okPack || okPipe) {
                 p->ctasPerSm = c;
                 p->nt = t;
-                if (ctas_per_sm) *ctas_per_sm = c;
-                if (depth_tile) *depth_tile = t;
+                p->fp = f;
+                report();
                 return SB_OK;
             }
         }
     }
-    const int shapes[][2] = {{1, 256}, {2, 256}, {1, 128}, {2, 128}, {3, 128}};
+    const int shapes[][3] = {{1, 384, 1}, {1, 256, 1}, {4, 256, 4}, {4, 256, 8}, {6, 128, 8}, {8, 128, 4}, {2, 256, 8}};
     float best = 1e30f;
-    int bestC = p->ctasPerSm, bestT = p->nt;
+    int bestC = p->ctasPerSm, bestT = p->nt, bestF = p->fp;
     cudaEvent_t e0, e1;
     SB_CUDA(cudaEventCreate(&e0));
     SB_CUDA(cudaEventCreate(&e1));
     for (const auto& sh : shapes) {
-        if (batchMaxW(p->maxCh, p->maxD, sh[0]) < 64) continue;
-        int r = launchBatch(p, sh[1], sh[0], st);  // warm-up
+        if (sh[2] == 1 && batchMaxW(p->maxCh, p->maxD, sh[0]) < 64) continue;
+        int r = launchBatch(p, sh[1], sh[0], sh[2], st);  // warm-up (builds pack tables)
         if (r != SB_OK) continue;
         SB_CUDA(cudaEventRecord(e0, st));
         for (int i = 0; i < 3; i++) {
-            r = launchBatch(p, sh[1], sh[0], st);
+            r = launchBatch(p, sh[1], sh[0], sh[2], st);
             if (r != SB_OK) break;
         }
         SB_CUDA(cudaEventRecord(e1, st));
@@ -417,17 +593,18 @@ int sb_batch_autotune(sb_batch_plan* p, const char* cache_path, int32_t* ctas_pe
             best = ms;
             bestC = sh[0];
             bestT = sh[1];
+            bestF = sh[2];
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     p->ctasPerSm = bestC;
     p->nt = bestT;
-    if (ctas_per_sm) *ctas_per_sm = bestC;
-    if (depth_tile) *depth_tile = bestT;
+    p->fp = bestF;
+    report();
     if (cache_path) {
         std::ofstream out(cache_path, std::ios::app);
-        if (out) out << p->signature << " " << bestC << " " << bestT << "\n";
+        if (out) out << p->signature << " " << bestC << " " << bestT << " " << bestF << "\n";
     }
     return SB_OK;
 }

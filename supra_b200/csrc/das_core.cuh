@@ -26,7 +26,7 @@ namespace sb {
 constexpr int kMaxApertureElems = 256;   // elements per aperture handled by the staged kernels
 constexpr uint32_t kWaitLimit = 1u << 22; // mbarrier polls before a staged load is declared lost
 
-struct ElemRec {
+struct __align__(16) ElemRec {
     float xel;    // element x (units of c dt)
     float dx;     // xel - line x, exact
     float wDeep;  // window weight once the aperture covers maxElementDistance
