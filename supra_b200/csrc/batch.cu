@@ -323,11 +323,17 @@ int launchBatch(sb_batch_plan* p, int nt, int ctas, int fp, cudaStream_t st) {
         a.lut = p->args.lut;
         for (int j = 0; j <= kIqMaxTaps; j++) a.lp[j] = p->args.lp[j];
         SB_CUDA(cudaMemsetAsync(p->dCounter, 0, sizeof(uint32_t), st));
-#define SB_PACK_LAUNCH(FPV, NTV) batchPackKernel<FPV, NTV><<<grid, NTV, 0, st>>>(a)
+#define SB_PACK_LAUNCH(FPV, NTV, MB) batchPackKernel<FPV, NTV, MB><<<grid, NTV, 0, st>>>(a)
         if (nt != 128 && nt != 256) return fail(SB_ERR_INVALID_ARG, "sb_batch: pack kernel block %d not in {128, 256}", nt);
-        if (fp == 2) { if (nt == 128) SB_PACK_LAUNCH(2, 128); else SB_PACK_LAUNCH(2, 256); }
-        else if (fp == 4) { if (nt == 128) SB_PACK_LAUNCH(4, 128); else SB_PACK_LAUNCH(4, 256); }
-        else { if (nt == 128) SB_PACK_LAUNCH(8, 128); else SB_PACK_LAUNCH(8, 256); }
+        // register budget: `ctas` resident CTAs of nt threads per SM
+        const int mb = std::max(1, std::min(ctas, 2048 / nt));
+        if (fp == 2) { if (nt == 128) SB_PACK_LAUNCH(2, 128, 8); else SB_PACK_LAUNCH(2, 256, 4); }
+        else if (fp == 4) {
+            if (nt == 128) { if (mb >= 12) SB_PACK_LAUNCH(4, 128, 12); else SB_PACK_LAUNCH(4, 128, 8); }
+            else { if (mb >= 6) SB_PACK_LAUNCH(4, 256, 6); else if (mb >= 5) SB_PACK_LAUNCH(4, 256, 5); else SB_PACK_LAUNCH(4, 256, 4); }
+        } else {
+            if (nt == 128) SB_PACK_LAUNCH(8, 128, 8); else { if (mb >= 5) SB_PACK_LAUNCH(8, 256, 5); else SB_PACK_LAUNCH(8, 256, 4); }
+        }
 #undef SB_PACK_LAUNCH
         SB_CHECK_LAUNCH("batchPackKernel");
         return SB_OK;
@@ -569,7 +575,7 @@ int sb_batch_autotune(sb_batch_plan* p, const char* cache_path, int32_t* ctas_pe
             }
         }
     }
-    const int shapes[][3] = {{1, 384, 1}, {1, 256, 1}, {4, 256, 4}, {4, 256, 8}, {6, 128, 8}, {8, 128, 4}, {2, 256, 8}};
+    const int shapes[][3] = {{1, 384, 1}, {4, 256, 4}, {5, 256, 4}, {6, 256, 4}, {12, 128, 4}, {4, 256, 8}, {5, 256, 8}};
     float best = 1e30f;
     int bestC = p->ctasPerSm, bestT = p->nt, bestF = p->fp;
     cudaEvent_t e0, e1;

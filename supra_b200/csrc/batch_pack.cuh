@@ -12,7 +12,9 @@
 // Depth segments of SEG depths (multiple of the decimation) are beamformed with a halo of `half`
 // depths on both sides so that the low-pass of the IQ stage sees all its taps; the beamformed
 // depths go to a two-block ring in shared memory and the IQ outputs whose taps are complete are
-// written after each block. The arithmetic per (depth, element, frame) is the reference's.
+// written after each block. The aperture test, window-LUT entry and sample index are the reference's
+// bit for bit; the per-frame accumulation is contracted into FMAs (w(1-f) and w f computed once per
+// element), so sums differ from the per-frame kernel by float rounding only (~1e-7 relative).
 #pragma once
 
 #include "das_core.cuh"
@@ -85,33 +87,103 @@ __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float*
         float fl;
         const int32_t delay = floorIdx(delayf, fl);
         const float frac = __fsub_rn(delayf, fl);
-        const size_t off = static_cast<size_t>(e.ch) * nS + static_cast<uint32_t>(delay);
-        if (static_cast<uint32_t>(delay) < nS - 1) {
-            const float om = __fsub_rn(1.0f, frac);
+        // The reference's three cases (RxSampleBeamformerDelayAndSum.h:178-188). Fast path when every
+        // lane of the warp has an interior sample (the common case); otherwise a branch-free form:
+        // last sample with zero fraction -> lerp(nS - 2, nS - 1) with weights (0, 1) = RF[nS - 1];
+        // no sample -> weight 0 on an in-range index.
+        const bool interior = static_cast<uint32_t>(delay) < nS - 1;
+        uint32_t idx;
+        float wA, wB;
+        if (__all_sync(__activemask(), interior)) {  // vote among the lanes present here (the loop and the depth range diverge)
+            idx = static_cast<uint32_t>(delay);
+            wB = __fmul_rn(w, frac);
+            wA = __fmul_rn(w, __fsub_rn(1.0f, frac));
+        } else {
+            const bool lastOne = !interior && static_cast<uint32_t>(delay) < nS && frac == 0.0f;
+            idx = interior ? static_cast<uint32_t>(delay) : (lastOne ? nS - 2 : 0u);
+            wB = interior ? __fmul_rn(w, frac) : (lastOne ? w : 0.0f);
+            wA = interior ? __fmul_rn(w, __fsub_rn(1.0f, frac)) : 0.0f;
+        }
+        const uint32_t off = static_cast<uint32_t>(e.ch) * nS + idx;
 #pragma unroll
-            for (int f = 0; f < FP; f++) {
-                if (f < nf) {
-                    const int16_t* p = tb[f] + off;
-                    const float v0 = static_cast<float>(__ldg(p));
-                    const float v1 = s16ToFloat(__ldg(p + 1));
-                    acc.v[f] = __fadd_rn(acc.v[f], __fmul_rn(w, __fadd_rn(__fmul_rn(om, v0), __fmul_rn(frac, v1))));
-                }
-            }
-        } else if (static_cast<uint32_t>(delay) < nS && frac == 0.0f) {
-#pragma unroll
-            for (int f = 0; f < FP; f++) {
-                if (f < nf) {
-                    const float v0 = static_cast<float>(__ldg(tb[f] + off));
-                    // the reference adds weight * RF[delay]; (1 - 0) * v0 + 0 * v1 with v1 = 0 is the same value
-                    acc.v[f] = __fadd_rn(acc.v[f], __fmul_rn(w, __fadd_rn(__fmul_rn(1.0f, v0), 0.0f)));
-                }
+        for (int f = 0; f < FP; f++) {
+            if (f < nf) {
+                const int16_t* p = tb[f] + off;
+                const float v0 = static_cast<float>(__ldg(p));
+                const float v1 = s16ToFloat(__ldg(p + 1));
+                acc.v[f] = fmaf(wB, v1, fmaf(wA, v0, acc.v[f]));
             }
         }
     }
 }
 
-template <int FP, int NT>
-__global__ void __launch_bounds__(NT) batchPackKernel(PackArgs a) {
+// Deep depths (every element active, weights precomputed): the same sum as packDepth<FP, true, .>,
+// software-pipelined so that the gathers of element j+1 are in flight while element j is accumulated
+// and element j+2's geometry is computed.
+template <int FP, bool USE_OFFSET>
+__device__ __forceinline__ void packDepthDeepPipelined(const ElemRec* el, int n, const PackDev& P, const LineK& s,
+                                                       const int16_t* const (&tb)[FP], int nf, float d,
+                                                       PackAcc<FP>& acc) {
+    const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
+    const float dyy = __fmul_rn(s.dirY, d);
+    const float dy2 = __fmul_rn(dyy, dyy);
+    const uint32_t nS = P.nS;
+    struct G {
+        uint32_t off;
+        float wA, wB;
+    };
+    auto geom = [&](int j) -> G {
+        const ElemRec e = el[j];
+        const float ex = __fsub_rn(e.xel, xz);
+        float t = __fadd_rn(s.iD, __fadd_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2)), d));
+        const float delayf = USE_OFFSET ? __fadd_rn(t, P.offset) : t;
+        float fl;
+        const int32_t delay = floorIdx(delayf, fl);
+        const float frac = __fsub_rn(delayf, fl);
+        const bool interior = static_cast<uint32_t>(delay) < nS - 1;
+        const bool lastOne = !interior && static_cast<uint32_t>(delay) < nS && frac == 0.0f;
+        G g;
+        const uint32_t idx = interior ? static_cast<uint32_t>(delay) : (lastOne ? nS - 2 : 0u);
+        g.wB = interior ? __fmul_rn(e.wDeep, frac) : (lastOne ? e.wDeep : 0.0f);
+        g.wA = interior ? __fmul_rn(e.wDeep, __fsub_rn(1.0f, frac)) : 0.0f;
+        g.off = static_cast<uint32_t>(e.ch) * nS + idx;
+        return g;
+    };
+    int16_t a0[FP], b0[FP], a1[FP], b1[FP];
+    G g0 = geom(0);
+    G g1 = n > 1 ? geom(1) : g0;
+#pragma unroll
+    for (int f = 0; f < FP; f++) {
+        a0[f] = b0[f] = 0;
+        if (f < nf) {
+            a0[f] = __ldg(tb[f] + g0.off);
+            b0[f] = __ldg(tb[f] + g0.off + 1);
+        }
+    }
+    for (int j = 0; j < n; j++) {
+        const bool more = j + 1 < n;
+#pragma unroll
+        for (int f = 0; f < FP; f++) {
+            a1[f] = b1[f] = 0;
+            if (f < nf && more) {
+                a1[f] = __ldg(tb[f] + g1.off);
+                b1[f] = __ldg(tb[f] + g1.off + 1);
+            }
+        }
+        const G g2 = j + 2 < n ? geom(j + 2) : g1;
+#pragma unroll
+        for (int f = 0; f < FP; f++) {
+            if (f < nf) acc.v[f] = fmaf(g0.wB, s16ToFloat(b0[f]), fmaf(g0.wA, static_cast<float>(a0[f]), acc.v[f]));
+            a0[f] = a1[f];
+            b0[f] = b1[f];
+        }
+        g0 = g1;
+        g1 = g2;
+    }
+}
+
+template <int FP, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
     __shared__ ElemRec el[kMaxApertureElems];
     __shared__ float lut[64];
     __shared__ float ring[2][FP][NT];
@@ -190,9 +262,9 @@ __global__ void __launch_bounds__(NT) batchPackKernel(PackArgs a) {
                 const bool useOffset = P.offset != 0.0f;
                 float wsum = 0.0f;
                 int cnt = 0;
-                if (deepOk && aDT >= s.maxDistX) {
-                    if (useOffset) packDepth<FP, true, true>(el, n, lut, P, s, tb, nf, d, aDT, 0.0f, wsum, cnt, acc);
-                    else packDepth<FP, true, false>(el, n, lut, P, s, tb, nf, d, aDT, 0.0f, wsum, cnt, acc);
+                if (deepOk && aDT >= s.maxDistX && n > 0) {
+                    if (useOffset) packDepthDeepPipelined<FP, true>(el, n, P, s, tb, nf, d, acc);
+                    else packDepthDeepPipelined<FP, false>(el, n, P, s, tb, nf, d, acc);
                     wsum = sumDeep;
                     cnt = cntDeep;
                 } else {

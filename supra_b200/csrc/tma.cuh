@@ -52,4 +52,9 @@ __device__ __forceinline__ void bulkCopyG2S(void* dst, const void* src, uint32_t
         : "memory");
 }
 
+// Bulk prefetch of a global range into L2 (no shared memory involved). addr and bytes multiples of 16.
+__device__ __forceinline__ void bulkPrefetchL2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 }  // namespace sb

@@ -30,9 +30,15 @@ def test_batch_rf_matches_per_frame(small_batch, shape, use_graph):
     b.run(use_graph=use_graph)  # a second replay must give the same result
     torch.cuda.synchronize()
     for k, p in enumerate(probe):
-        ref = plans[p].beamform(rfs[k], 1.0, 1540e3, 1).cpu().numpy()
-        got = b.rf_outputs[k].cpu().numpy()
-        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), f"frame {k}"
+        ref = plans[p].beamform(rfs[k], 1.0, 1540e3, 1).cpu().numpy().astype(np.float64)
+        got = b.rf_outputs[k].cpu().numpy().astype(np.float64)
+        if shape[2] == 1:  # per-frame pipeline: same arithmetic as sb_das_run, bit-identical
+            assert np.array_equal(got, ref), f"frame {k}"
+        else:  # frame packs: FMA-contracted sums, identical decisions
+            big = np.abs(ref) >= np.finfo(np.float32).max
+            assert np.array_equal(got[big], ref[big])
+            peak = np.max(np.abs(ref[~big]))
+            assert np.max(np.abs(got[~big] - ref[~big])) <= 1e-6 * peak, f"frame {k}"
 
 
 def test_batch_iq_vs_fp64(small_batch, oracle):
