@@ -268,19 +268,20 @@ def fir_design(length: int, ftype: int, window: int, fs=2.0, f=0.0, bw=0.0) -> n
 
 
 def mv_beamform(raw_delayed: torch.Tensor, subarray_size=0, temporal_smoothing=3, subarray_scaling_power=1.5,
-                compute_means=False, loading_scale=1.0, fp64_threshold=1e6, out_dtype=None):
+                compute_means=False, loading_scale=1.0, fp64_threshold=1e6, out_dtype=None, with_stats=True):
     """RxBeamformerMV::performRxBeamforming (Beamformer/RxBeamformerMV.cu:382-622).
-    raw_delayed [num_rx][num_channels][num_depths] float32 or complex64 -> ([num_depths][num_rx], stats)."""
+    raw_delayed [num_rx][num_channels][num_depths] float32, int16 or complex64 -> ([num_depths][num_rx], stats).
+    with_stats=False skips the statistics read-back (no host synchronisation; stats is then None)."""
     lib = load_library()
     nRx, nCh, nS = raw_delayed.shape
     if out_dtype is None:
         out_dtype = torch.complex64 if raw_delayed.dtype == torch.complex64 else torch.float32
     out = torch.empty((nS, nRx), dtype=out_dtype, device=raw_delayed.device)
-    stats = sb_mv_stats()
+    stats = sb_mv_stats() if with_stats else None
     check("sb_mv_run", lib.sb_mv_run(_ptr(raw_delayed), dtype_code(raw_delayed), _ptr(out), dtype_code(out), nRx, nCh,
                                      nS, int(subarray_size), int(temporal_smoothing), float(subarray_scaling_power),
                                      int(bool(compute_means)), float(loading_scale), float(fp64_threshold),
-                                     C.byref(stats), _stream()))
+                                     C.byref(stats) if with_stats else None, _stream()))
     return out, stats
 
 
