@@ -192,27 +192,36 @@ __device__ __forceinline__ SampleMeta loadSample(const MvArgs& a, const In* xl, 
 }
 
 // Adds sign * (covariance of one sample) to the register accumulators of this lane's circulant
-// diagonals d = lane + 32q. Entry r of diagonal d is R[r][(r + d) mod L].
+// diagonals d = lane + 32q. Entry r of diagonal d is R[r][(r + d) mod L]. The first row of the
+// sample's covariance (D0[d] = R[0][d], a K-term sum) is computed when `fresh` and stored in d0,
+// otherwise read back from d0: a sample enters and later leaves the window with identical values.
 template <bool C, int NR, bool COMP, class T>
-__device__ __forceinline__ void addCov(const Elem<C>* xv, SampleMeta m, int L, int lane, T sign,
+__device__ __forceinline__ void addCov(const Elem<C>* xv, SampleMeta m, V<T>* d0, bool fresh, int L, int lane, T sign,
                                        V<T> (&hi)[NR][32 * NR], V<T> (&lo)[NR][32 * NR]) {
     const int f = m.f, K = m.K;
     V<T> D0[NR];
+    if (fresh) {
 #pragma unroll
-    for (int q = 0; q < NR; q++) {
-        const int d = lane + 32 * q;
-        const int dd = d < L ? d : 0;
-        V<T> a0 = vz<C, T>(), a1 = vz<C, T>(), a2 = vz<C, T>(), a3 = vz<C, T>();
-        int k = 0;
-        for (; k + 3 < K; k += 4) {
-            macConj<C, T>(a0, ld<C, T>(xv[f + k]), ld<C, T>(xv[f + k + dd]));
-            macConj<C, T>(a1, ld<C, T>(xv[f + k + 1]), ld<C, T>(xv[f + k + 1 + dd]));
-            macConj<C, T>(a2, ld<C, T>(xv[f + k + 2]), ld<C, T>(xv[f + k + 2 + dd]));
-            macConj<C, T>(a3, ld<C, T>(xv[f + k + 3]), ld<C, T>(xv[f + k + 3 + dd]));
+        for (int q = 0; q < NR; q++) {
+            const int d = lane + 32 * q;
+            const int dd = d < L ? d : 0;
+            V<T> a0 = vz<C, T>(), a1 = vz<C, T>(), a2 = vz<C, T>(), a3 = vz<C, T>();
+            int k = 0;
+            for (; k + 3 < K; k += 4) {
+                macConj<C, T>(a0, ld<C, T>(xv[f + k]), ld<C, T>(xv[f + k + dd]));
+                macConj<C, T>(a1, ld<C, T>(xv[f + k + 1]), ld<C, T>(xv[f + k + 1 + dd]));
+                macConj<C, T>(a2, ld<C, T>(xv[f + k + 2]), ld<C, T>(xv[f + k + 2 + dd]));
+                macConj<C, T>(a3, ld<C, T>(xv[f + k + 3]), ld<C, T>(xv[f + k + 3 + dd]));
+            }
+            for (; k < K; k++) macConj<C, T>(a0, ld<C, T>(xv[f + k]), ld<C, T>(xv[f + k + dd]));
+            D0[q].re = (a0.re + a1.re) + (a2.re + a3.re);
+            D0[q].im = (a0.im + a1.im) + (a2.im + a3.im);
+            d0[d] = D0[q];
         }
-        for (; k < K; k++) macConj<C, T>(a0, ld<C, T>(xv[f + k]), ld<C, T>(xv[f + k + dd]));
-        D0[q].re = (a0.re + a1.re) + (a2.re + a3.re);
-        D0[q].im = (a0.im + a1.im) + (a2.im + a3.im);
+        __syncwarp();
+    } else {
+#pragma unroll
+        for (int q = 0; q < NR; q++) D0[q] = d0[lane + 32 * q];
     }
     // Start of the lower segment of diagonal d (entry (L-d, 0)) = conj(D0 of diagonal L-d).
     V<T> E0[NR];
@@ -220,14 +229,9 @@ __device__ __forceinline__ void addCov(const Elem<C>* xv, SampleMeta m, int L, i
     for (int q = 0; q < NR; q++) {
         const int d = lane + 32 * q;
         const int src = (d > 0 && d < L) ? L - d : 0;
-        V<T> got = vz<C, T>();
-#pragma unroll
-        for (int q2 = 0; q2 < NR; q2++) {
-            const V<T> v = shflV<C, T>(D0[q2], src & 31);
-            if ((src >> 5) == q2) got = v;
-        }
-        E0[q].re = got.re;
-        E0[q].im = -got.im;
+        const V<T> v = d0[src];
+        E0[q].re = v.re;
+        E0[q].im = -v.im;
     }
 #pragma unroll
     for (int q = 0; q < NR; q++) {
@@ -305,13 +309,28 @@ __device__ __forceinline__ MvOut<T> solveRegs(GE* Gs, int GP, int L, int sz, T l
             acc2[q] = vz<C, T>();
         }
 #pragma unroll
-        for (int k = 0; k < j; k++) {
-            const V<T> gjk = ldG<C, T>(Gs[j * GP + k]);
+        for (int k = 0; k + 1 < j; k += 2) {
+            // rows have an even pitch: entries (j, k) and (j, k + 1) are one aligned pair
+            V<T> gjk, gjk1;
+            if constexpr (C) {
+                const float4 p = *reinterpret_cast<const float4*>(&Gs[j * GP + k]);
+                gjk = V<T>{p.x, p.y};
+                gjk1 = V<T>{p.z, p.w};
+            } else {
+                const float2 p = *reinterpret_cast<const float2*>(&Gs[j * GP + k]);
+                gjk = V<T>{p.x, T(0)};
+                gjk1 = V<T>{p.y, T(0)};
+            }
 #pragma unroll
             for (int q = 0; q < NR; q++) {
-                if (k & 1) mscConj<C, T>(acc2[q], g[q][k], gjk);
-                else mscConj<C, T>(acc[q], g[q][k], gjk);
+                mscConj<C, T>(acc[q], g[q][k], gjk);
+                mscConj<C, T>(acc2[q], g[q][k + 1], gjk1);
             }
+        }
+        if (j & 1) {
+            const V<T> gjk = ldG<C, T>(Gs[j * GP + j - 1]);
+#pragma unroll
+            for (int q = 0; q < NR; q++) mscConj<C, T>(acc[q], g[q][j - 1], gjk);
         }
 #pragma unroll
         for (int q = 0; q < NR; q++) {
@@ -323,8 +342,8 @@ __device__ __forceinline__ MvOut<T> solveRegs(GE* Gs, int GP, int L, int sz, T l
             res.ok = false;
             return res;
         }
-        const T gjj = sqrt(djj);
-        const T inv = T(1) / gjj;
+        const T inv = rsqrtf(djj);  // MUFU reciprocal square root (about 2 ulp)
+        const T gjj = djj * inv;
 #pragma unroll
         for (int q = 0; q < NR; q++) {
             const int i = lane + 32 * q;
@@ -508,19 +527,86 @@ __host__ __device__ constexpr size_t alignUp(size_t v, size_t a) { return (v + a
 
 template <bool C, int NR> struct MvLayout {
     static constexpr int GR = 32 * NR;
-    static constexpr int GP = 32 * NR + 1;
+    static constexpr int GP = 32 * NR + 2;  // even: pairs (k, k+1) of a row are 2-element aligned
     __host__ __device__ static size_t ringBytes(uint32_t slots, uint32_t pitch) {
         return alignUp(static_cast<size_t>(slots) * pitch * sizeof(Elem<C>), 16);
     }
     __host__ __device__ static size_t metaBytes(uint32_t slots) { return alignUp(slots * sizeof(SampleMeta), 16); }
+    __host__ __device__ static size_t d0Bytes(uint32_t slots) {
+        return alignUp(static_cast<size_t>(slots) * GR * sizeof(V<float>), 16);
+    }
     __host__ __device__ static size_t gBytes() { return alignUp(static_cast<size_t>(GR) * GP * sizeof(Elem<C>), 16); }
     __host__ __device__ static size_t perWarp(uint32_t slots, uint32_t pitch) {
-        return ringBytes(slots, pitch) + metaBytes(slots) + gBytes();
+        return ringBytes(slots, pitch) + metaBytes(slots) + d0Bytes(slots) + gBytes();
     }
 };
 
+__device__ __forceinline__ void cpAsync4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpAsync8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Starts the copy of sample t of one scanline into its ring slot (FP32 / complex input: cp.async,
+// no registers held; int16 input is converted, so it is loaded synchronously in sampleMeta).
+template <bool C, class In>
+__device__ __forceinline__ void issueSample(const MvArgs& a, const In* xl, uint32_t t, Elem<C>* slot, int lane) {
+    if constexpr (!std::is_same<In, int16_t>::value) {
+        for (uint32_t ch = lane; ch < a.nCh; ch += 32) {
+            const In* src = xl + static_cast<size_t>(ch) * a.nS + t;
+            if constexpr (C) cpAsync8(&slot[ch], src);
+            else cpAsync4(&slot[ch], src);
+        }
+        cpAsyncCommit();
+    }
+}
+
+// Completes sample t in its slot and derives the aperture (first / last nonzero channel,
+// computeSubArrayMasks RxBeamformerMV.cu:80-110): sz = min(L, l-f+1), and the K = l - sz - f + 2
+// active subarrays start at f, f+1, ..., f+K-1. Channels past nCh are zero padding.
+template <bool C, class In>
+__device__ __forceinline__ SampleMeta sampleMeta(const MvArgs& a, const In* xl, uint32_t t, Elem<C>* slot, int lane) {
+    if constexpr (std::is_same<In, int16_t>::value) {
+        for (uint32_t ch = lane; ch < a.nCh; ch += 32) slot[ch].re = static_cast<float>(__ldg(xl + static_cast<size_t>(ch) * a.nS + t));
+    } else {
+        cpAsyncWaitAll();
+    }
+    __syncwarp();
+    int first = -1, last = -1;
+    for (uint32_t c0 = 0; c0 < a.nCh; c0 += 32) {
+        const uint32_t ch = c0 + lane;
+        bool nz = false;
+        if (ch < a.nCh) {
+            const Elem<C> v = slot[ch];
+            nz = v.re != 0.0f;
+            if constexpr (C) nz = nz || v.im != 0.0f;
+        }
+        const uint32_t m = __ballot_sync(kFull, nz);
+        if (m) {
+            if (first < 0) first = static_cast<int>(c0) + __ffs(m) - 1;
+            last = static_cast<int>(c0) + 31 - __clz(m);
+        }
+    }
+    SampleMeta md;
+    md.f = first < 0 ? 0 : first;
+    const int l = last < 0 ? 0 : last;
+    md.sz = min(static_cast<int>(a.L), l - md.f + 1);
+    md.K = l - md.sz - md.f + 2;
+    md.pad = 0;
+    return md;
+}
+
 // One warp per run of consecutive samples of one scanline inside one 2000-sample block.
-template <bool C, int NR, bool SLIDE, class In, class Out>
+// LT != 0 fixes the subarray length at compile time (L = LT), which folds the per-entry range checks
+// of the unrolled loops.
+template <bool C, int NR, bool SLIDE, int LT, class In, class Out>
 __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     using L_ = MvLayout<C, NR>;
@@ -534,36 +620,50 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
     const uint32_t sA = b0 + j * kMvRun;
     if (sA >= bEnd) return;
     const uint32_t sB = min(sA + kMvRun, bEnd);
-    const int L = static_cast<int>(a.L), T = static_cast<int>(a.T);
+    const int L = LT ? LT : static_cast<int>(a.L), T = static_cast<int>(a.T);
+    const uint32_t R = a.ringSlots;
 
-    unsigned char* base = smem + static_cast<size_t>(warp) * L_::perWarp(a.ringSlots, a.ringPitch);
+    unsigned char* base = smem + static_cast<size_t>(warp) * L_::perWarp(R, a.ringPitch);
     Elem<C>* ring = reinterpret_cast<Elem<C>*>(base);
-    SampleMeta* meta = reinterpret_cast<SampleMeta*>(base + L_::ringBytes(a.ringSlots, a.ringPitch));
-    Elem<C>* Gs = reinterpret_cast<Elem<C>*>(base + L_::ringBytes(a.ringSlots, a.ringPitch) + L_::metaBytes(a.ringSlots));
+    SampleMeta* meta = reinterpret_cast<SampleMeta*>(base + L_::ringBytes(R, a.ringPitch));
+    V<float>* d0c = reinterpret_cast<V<float>*>(base + L_::ringBytes(R, a.ringPitch) + L_::metaBytes(R));
+    Elem<C>* Gs = reinterpret_cast<Elem<C>*>(base + L_::ringBytes(R, a.ringPitch) + L_::metaBytes(R) + L_::d0Bytes(R));
     const In* xl = static_cast<const In*>(a.in) + static_cast<size_t>(line) * a.nCh * a.nS;
     Out* out = static_cast<Out*>(a.out);
 
-    auto slotOf = [&](uint32_t t) -> Elem<C>* { return ring + static_cast<size_t>(t % a.ringSlots) * a.ringPitch; };
-    auto stage = [&](uint32_t t) {
-        const SampleMeta m = loadSample<C, In>(a, xl, t, slotOf(t), lane);
-        if (lane == 0) meta[t % a.ringSlots] = m;
+    // zero padding past nCh in every slot (written once; copies only touch channels < nCh)
+    for (uint32_t i = lane; i < R * (a.ringPitch - a.nCh); i += 32) {
+        const uint32_t sl = i / (a.ringPitch - a.nCh), ch = a.nCh + i % (a.ringPitch - a.nCh);
+        ring[static_cast<size_t>(sl) * a.ringPitch + ch].re = 0.0f;
+        if constexpr (C) ring[static_cast<size_t>(sl) * a.ringPitch + ch].im = 0.0f;
+    }
+    auto slotOf = [&](uint32_t t) -> Elem<C>* { return ring + static_cast<size_t>(t % R) * a.ringPitch; };
+    auto complete = [&](uint32_t t) {
+        const SampleMeta m = sampleMeta<C, In>(a, xl, t, slotOf(t), lane);
+        if (lane == 0) meta[t % R] = m;
         __syncwarp();
     };
 
     V<float> hi[NR][32 * NR], lo[NR][32 * NR];
-    // stage the window of the first sample
+    // the first sample's window, then the sample that enters at the second step
     const uint32_t w0 = static_cast<uint32_t>(max(static_cast<int>(b0), static_cast<int>(sA) - T));
     const uint32_t w1 = min(bEnd - 1, sA + a.T);
-    for (uint32_t t = w0; t <= w1; t++) stage(t);
+    for (uint32_t t = w0; t <= w1; t++) {
+        issueSample<C, In>(a, xl, t, slotOf(t), lane);
+        complete(t);
+    }
+    if (sA + 1 < sB && w1 + 1 <= bEnd - 1) issueSample<C, In>(a, xl, w1 + 1, slotOf(w1 + 1), lane);
 
     unsigned long long systems = 0;
     float condMax = 0.0f;
     for (uint32_t s = sA; s < sB; s++) {
         const uint32_t t0 = static_cast<uint32_t>(max(static_cast<int>(b0), static_cast<int>(s) - T));
         const uint32_t t1 = min(bEnd - 1, s + a.T);
-        if (s > sA && s + a.T <= bEnd - 1) stage(s + a.T);
+        const bool hasNew = s > sA && s + a.T <= bEnd - 1;
+        if (hasNew) complete(s + a.T);
         bool fullWindow = true;
         if constexpr (SLIDE) fullWindow = s == sA;
+        const bool hasOld = !fullWindow && static_cast<int>(s) - T - 1 >= static_cast<int>(b0);
         if (fullWindow) {
 #pragma unroll
             for (int q = 0; q < NR; q++)
@@ -572,16 +672,28 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
                     hi[q][r] = vz<C, float>();
                     lo[q][r] = vz<C, float>();
                 }
-            for (uint32_t t = t0; t <= t1; t++)
-                addCov<C, NR, SLIDE, float>(slotOf(t), meta[t % a.ringSlots], L, lane, 1.0f, hi, lo);
-        } else if constexpr (SLIDE) {
-            if (s + a.T <= bEnd - 1)
-                addCov<C, NR, true, float>(slotOf(s + a.T), meta[(s + a.T) % a.ringSlots], L, lane, 1.0f, hi, lo);
-            if (static_cast<int>(s) - T - 1 >= static_cast<int>(b0)) {
-                const uint32_t to = s - a.T - 1;
-                addCov<C, NR, true, float>(slotOf(to), meta[to % a.ringSlots], L, lane, -1.0f, hi, lo);
-            }
         }
+        // one call site for the covariance updates: the whole window, or the entering and leaving sample
+        const int nJobs = fullWindow ? static_cast<int>(t1 - t0 + 1) : static_cast<int>(hasNew) + static_cast<int>(hasOld);
+        for (int jb = 0; jb < nJobs; jb++) {
+            uint32_t t;
+            float sign = 1.0f;
+            bool fresh = true;
+            if (fullWindow) t = t0 + jb;
+            else if (jb == 0 && hasNew) t = s + a.T;
+            else {
+                t = s - a.T - 1;
+                sign = -1.0f;
+                fresh = false;
+            }
+            addCov<C, NR, SLIDE, float>(slotOf(t), meta[t % R], d0c + static_cast<size_t>(t % R) * L_::GR, fresh, L,
+                                        lane, sign, hi, lo);
+        }
+        // prefetch the sample entering at the next step; its slot held sample s - T - 1, whose
+        // subtraction above was the last use
+        __syncwarp();
+        if (s > sA && s + 1 < sB && s + a.T + 1 <= bEnd - 1)
+            issueSample<C, In>(a, xl, s + a.T + 1, slotOf(s + a.T + 1), lane);
         // transpose the window sum into rows
 #pragma unroll
         for (int q = 0; q < NR; q++) {
@@ -599,7 +711,7 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
             }
         }
         __syncwarp();
-        const SampleMeta ms = meta[s % a.ringSlots];
+        const SampleMeta ms = meta[s % R];
         const Elem<C>* xs = slotOf(s);
         // trace of the sz x sz block and the loading (RxBeamformerMV.cu:239-276)
         float tr = 0.0f;
@@ -616,13 +728,23 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
         for (int q = 0; q < NR; q++) {
             const int i = lane + 32 * q;
             const int ii = i < ms.sz ? i : 0;
-            V<float> acc = vz<C, float>();
-            for (int k = 0; k < ms.K; k++) {
-                const V<float> v = ld<C, float>(xs[ms.f + k + ii]);
-                acc.re += v.re;
-                acc.im += v.im;
+            V<float> acc0 = vz<C, float>(), acc1 = vz<C, float>();
+            int k = 0;
+            for (; k + 1 < ms.K; k += 2) {
+                const V<float> v0 = ld<C, float>(xs[ms.f + k + ii]), v1 = ld<C, float>(xs[ms.f + k + 1 + ii]);
+                acc0.re += v0.re;
+                acc0.im += v0.im;
+                acc1.re += v1.re;
+                acc1.im += v1.im;
             }
-            xbar[q] = i < ms.sz ? acc : vz<C, float>();
+            if (k < ms.K) {
+                const V<float> v0 = ld<C, float>(xs[ms.f + k + ii]);
+                acc0.re += v0.re;
+                acc0.im += v0.im;
+            }
+            acc0.re += acc1.re;
+            acc0.im += acc1.im;
+            xbar[q] = i < ms.sz ? acc0 : vz<C, float>();
         }
         V<float> y = vz<C, float>();
         bool write = true;
@@ -740,7 +862,10 @@ int launchMv(MvArgs& a, cudaStream_t st) {
                     a.nCh, a.T, perWarp);
     const size_t smemBytes = perWarp * warps;
     constexpr bool SLIDE = NR == 1;
-    auto kern = mvKernel<C, NR, SLIDE, In, Out>;
+    // L = 32 (one row per lane) is specialised; for two rows per lane the folded variant exceeds the
+    // register file, so it keeps the runtime length
+    auto kern = (NR == 1 && a.L == 32u) ? mvKernel<C, NR, SLIDE, NR == 1 ? 32 : 0, In, Out>
+                                         : mvKernel<C, NR, SLIDE, 0, In, Out>;
     SB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemBytes)));
     const uint32_t grid = (a.numItems + warps - 1) / warps;
     kern<<<grid, 32 * warps, smemBytes, st>>>(a);
@@ -801,7 +926,8 @@ extern "C" int sb_mv_run(const void* raw_delayed, int in_dtype, void* out, int o
     a.L = L;
     a.T = temporal_smoothing;
     a.ringSlots = 2 * temporal_smoothing + 2;
-    a.ringPitch = (num_channels + 64 + 31) / 32 * 32;
+    // channel reads reach index nCh - 1 + L - 1 (apertures narrower than L); padding is zero
+    a.ringPitch = (num_channels + (L <= 32 ? 32 : 64) + 31) / 32 * 32;
     a.runsPerBlock = (kMvBlock + kMvRun - 1) / kMvRun;
     const uint32_t nBlocks = (num_samples + kMvBlock - 1) / kMvBlock;
     a.runsPerLine = nBlocks * a.runsPerBlock;
