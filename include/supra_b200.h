@@ -168,6 +168,10 @@ int sb_hilbert_plan_destroy(sb_hilbert_plan* plan);
  * reference; here that tap is 0. */
 int sb_hilbert_env_run(const sb_hilbert_plan* plan, const void* in, int in_dtype, void* out, int out_dtype,
                        uint32_t num_scanlines, uint32_t num_samples, sb_stream stream);
+/* Extension without a reference counterpart: adjoint of sb_hilbert_env_run for FP32 input.
+ * grad_env, in, grad_in: [num_samples][num_scanlines]; grad_in is overwritten. */
+int sb_hilbert_env_adjoint(const sb_hilbert_plan* plan, const float* in, const float* grad_env, float* grad_in,
+                           uint32_t num_scanlines, uint32_t num_samples, sb_stream stream);
 
 /* Replaces LogCompressor::compress (Beamformer/LogCompressor.cu:44-66). */
 int sb_logcompress_run(const void* in, int in_dtype, void* out, int out_dtype, size_t num_values,
@@ -294,16 +298,20 @@ int sb_check_device_errors(int reset);
 
 /* Extension without a reference counterpart. Forward with per-element apodisation:
  *   s = sum_e apod[e] w_e lerp(rf_e, tau_e(c)) / sum_e apod[e] w_e * n_active
- * (apod == NULL means 1, which equals sb_das_run). FP32 rf [num_tx][num_channels][num_samples]. */
-int sb_das_forward_apod(const sb_das_plan* plan, const float* rf, const float* apod, float* out,
+ * (apod == NULL means 1, which equals sb_das_run). 2D geometries, highest-weight transmit.
+ * rf: FP32 [num_frames][num_tx][num_channels][num_samples]; out: [num_frames][num_depths][num_rx]. */
+int sb_das_forward_apod(const sb_das_plan* plan, const float* rf, const float* apod, float* out, uint32_t num_frames,
                         double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
                         sb_stream stream);
-/* Adjoint of sb_das_forward_apod: given grad_out [num_depths][num_rx] accumulates into grad_rf
- * (same shape as rf; may be NULL), grad_apod [num_elements] (may be NULL) and grad_c (one float,
- * derivative w.r.t. the speed of sound in mm/s; may be NULL). Outputs are overwritten, not accumulated. */
-int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, const float* grad_out,
-                   float* grad_rf, float* grad_apod, float* grad_c, double f_number, double speed_of_sound_mm_s,
-                   int window_type, float window_parameter, sb_stream stream);
+/* Adjoint of sb_das_forward_apod. Given grad_out [num_frames][num_depths][num_rx] writes grad_rf
+ * (same shape as rf; may be NULL), grad_apod [num_elements] (summed over frames; may be NULL) and
+ * grad_c (one float: derivative w.r.t. the speed of sound in mm/s, summed over frames; may be NULL).
+ * forward_out is the forward result for the same arguments (NULL: recomputed). Outputs are
+ * overwritten, not accumulated. */
+int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, const float* forward_out,
+                   const float* grad_out, float* grad_rf, float* grad_apod, float* grad_c, uint32_t num_frames,
+                   double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
+                   sb_stream stream);
 
 #ifdef __cplusplus
 }

@@ -117,6 +117,23 @@ def das(geom, rf: np.ndarray, f_number=1.0, c_mm_s=None, window=1, window_param=
     return out.reshape(geom.num_depths, geom.num_rx)
 
 
+def das_adjoint64(geom, rf: np.ndarray, apod, gout: np.ndarray, c_mm_s=None, f_number=1.0, window=1, window_param=0.0):
+    """FP64 reference gradient of the apodised 2D DAS: (grad_rf, grad_apod, grad_c)."""
+    g = geom.ctypes()
+    rf32 = np.ascontiguousarray(rf, dtype=np.float32)
+    c = geom.speed_of_sound_mm_s if c_mm_s is None else c_mm_s
+    go = np.ascontiguousarray(gout, dtype=np.float64)
+    grf = np.zeros(rf32.size, np.float64)
+    gap = np.zeros(geom.num_elements, np.float64)
+    gc = np.zeros(1, np.float64)
+    ap = None if apod is None else np.ascontiguousarray(apod, dtype=np.float32)
+    st = lib().orc_das_adjoint64(C.byref(g), _vp(_p(rf32)), None if ap is None else _vp(_p(ap)), _vp(_p(go)),
+                                 _vp(_p(grf)), _vp(_p(gap)), _vp(_p(gc)), C.c_double(f_number), C.c_double(c),
+                                 C.c_int(window), C.c_float(window_param))
+    assert st == 0
+    return grf.reshape(rf32.shape), gap, float(gc[0])
+
+
 def rawdelay(geom, rf: np.ndarray, f_number=1.0, c_mm_s=None, window=1, window_param=0.0, threads=None):
     g = geom.ctypes()
     rf32 = np.ascontiguousarray(rf, dtype=np.float32)

@@ -554,6 +554,95 @@ int orc_das(const sb_geometry* g, const float* rf, float* out_f32, double* out_f
     return 0;
 }
 
+// FP64 reference gradient of the apodised 2D DAS (extension without a reference counterpart): the
+// transpose of sampleBeamform2D<double> with apodisation (same discrete decisions: aperture, window
+// index, sample index), highest-weight transmit. For a pixel with upstream g, W_e = w_e a_e,
+// D = sum W_e, n active elements, v_e = lerp(rf, tau_e), s = n / D sum W_e v_e:
+//   grad_rf[delta] += g n / D W_e (1 - frac), grad_rf[delta + 1] += g n / D W_e frac,
+//   grad_apod[e] += g w_e (n v_e - s) / D,
+//   grad_c += g n / D sum_e W_e (rf[delta + 1] - rf[delta]) * (-(path_e) / c), path = dist + depth (DT units).
+// Single-threaded (the scatter is not partitioned). grad_rf has rf's shape.
+int orc_das_adjoint64(const sb_geometry* g, const float* rf, const float* apod, const double* gout, double* grad_rf,
+                      double* grad_apod, double* grad_c, double fNumber, double c, int windowType,
+                      float windowParameter) {
+    if (!g || !rf || !gout) return -1;
+    GeomDT G = toDtSpace(g, c);
+    Window win(windowType, windowParameter, 64);
+    const float F = static_cast<float>(fNumber);
+    const float speedOfSound = G.c, dt = G.dt;
+    const uint32_t nS = g->num_samples, nCh = g->num_channels;
+    if (grad_rf) std::fill(grad_rf, grad_rf + static_cast<size_t>(g->num_tx) * nCh * nS, 0.0);
+    if (grad_apod) std::fill(grad_apod, grad_apod + g->num_elements, 0.0);
+    double gc = 0.0;
+    for (uint32_t line = 0; line < g->num_rx; line++) {
+        const LineDT& s = G.lines[line];
+        const int k = highestWeightIndex(s);
+        if (!(s.txWeights[k] > 0.0) || s.txIdx[k] >= g->num_tx) continue;
+        for (uint32_t r = 0; r < g->num_depths; r++) {
+            const float d = G.depths[r];
+            const float aDT = ((d * dt) * speedOfSound) / (2 * F) / speedOfSound / dt;
+            const float inv = 1 / std::min(aDT, s.maxDistX);
+            const double gp = gout[static_cast<size_t>(r) * g->num_rx + line];
+            if (gp == 0.0) continue;
+            struct Term { uint32_t e; size_t base; int32_t delay; double w, W, frac, v, slope, path; int kind; };
+            std::vector<Term> terms;
+            double D = 0.0, num = 0.0;
+            int n = 0;
+            for (int32_t e = s.firstX[k]; e < s.lastX[k]; e++) {
+                int32_t ch = channelOf(g, static_cast<uint32_t>(e));
+                if (ch < 0) continue;
+                float x_elem = G.xe[e];
+                if (!(std::fabs(x_elem - s.x) <= aDT)) continue;
+                Term t{};
+                t.e = static_cast<uint32_t>(e);
+                t.w = win.get((x_elem - s.x) * inv);
+                t.W = apod ? t.w * static_cast<double>(apod[e]) : t.w;
+                D += t.W;
+                n++;
+                float a = s.x + s.dirX * d;
+                float dx = x_elem - a;
+                float dy = s.dirY * d;
+                float delayf = s.initialDelay[k] + (std::sqrt(dx * dx + dy * dy) + d);
+                t.delay = static_cast<int32_t>(std::floor(delayf));
+                t.path = std::sqrt(static_cast<double>(dx) * dx + static_cast<double>(dy) * dy) + d;
+                double dd = static_cast<double>(s.initialDelay[k]) + t.path;
+                t.frac = dd - t.delay;
+                t.base = static_cast<size_t>(ch) * nS + static_cast<size_t>(s.txIdx[k]) * nCh * nS;
+                t.kind = 0;
+                if (static_cast<uint32_t>(t.delay) < nS - 1) {
+                    double v0 = rf[t.base + t.delay], v1 = rf[t.base + t.delay + 1];
+                    t.v = (1 - t.frac) * v0 + t.frac * v1;
+                    t.slope = v1 - v0;
+                    t.kind = 1;
+                } else if (static_cast<uint32_t>(t.delay) < nS && static_cast<float>(delayf - static_cast<float>(t.delay)) == 0.0f) {
+                    t.v = rf[t.base + t.delay];
+                    t.kind = 2;
+                }
+                num += t.W * t.v;
+                terms.push_back(t);
+            }
+            if (n == 0 || gp == 0.0 || !(D != 0.0)) continue;
+            const double sv = num / D * n;
+            if (!std::isfinite(sv)) continue;
+            const double G1 = gp * n / D;
+            for (const Term& t : terms) {
+                if (t.kind == 1) {
+                    if (grad_rf) {
+                        grad_rf[t.base + t.delay] += G1 * t.W * (1 - t.frac);
+                        grad_rf[t.base + t.delay + 1] += G1 * t.W * t.frac;
+                    }
+                    gc += G1 * t.W * t.slope * (-t.path / c);
+                } else if (t.kind == 2 && grad_rf) {
+                    grad_rf[t.base + t.delay] += G1 * t.W;
+                }
+                if (grad_apod) grad_apod[t.e] += gp * t.w * (n * t.v - sv) / D;
+            }
+        }
+    }
+    if (grad_c) *grad_c = gc;
+    return 0;
+}
+
 int orc_rawdelay(const sb_geometry* g, const float* rf, float* out, double fNumber, double c, int windowType,
                  float windowParameter, int nthreads) {
     if (!g || !rf || !out) return -1;

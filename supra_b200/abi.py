@@ -169,8 +169,9 @@ _SIGNATURES = {
     "sb_batch_set_rf_outputs": (_int, [_vp, _vp]),
     "sb_batch_autotune": (_int, [_vp, C.c_char_p, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), _vp]),
     "sb_check_device_errors": (_int, [_int]),
-    "sb_das_forward_apod": (_int, [_vp, _vp, _vp, _vp, _f64, _f64, _int, _f32, _vp]),
-    "sb_das_adjoint": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _f64, _f64, _int, _f32, _vp]),
+    "sb_hilbert_env_adjoint": (_int, [_vp, _vp, _vp, _vp, _u32, _u32, _vp]),
+    "sb_das_forward_apod": (_int, [_vp, _vp, _vp, _vp, _u32, _f64, _f64, _int, _f32, _vp]),
+    "sb_das_adjoint": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _f64, _f64, _int, _f32, _vp]),
 }
 
 EXPORTED = tuple(_SIGNATURES)

@@ -85,6 +85,46 @@ class RxBeamformer:
         return out
 
 
+    def forward_apod(self, rf: torch.Tensor, apod: Optional[torch.Tensor], speed_of_sound_mm_s: float, f_number=1.0,
+                     window_type=1, window_parameter=0.0) -> torch.Tensor:
+        """Differentiable-path forward: rf FP32 [frames][num_tx][num_channels][num_samples] (or without the
+        frame axis), per-element apodisation apod [num_elements] (None = 1) -> [frames][num_depths][num_rx]."""
+        g = self.geometry
+        squeeze = rf.dim() == 3
+        if squeeze:
+            rf = rf.unsqueeze(0)
+        if rf.dtype != torch.float32:
+            raise ValueError("forward_apod takes float32 channel data")
+        frames = rf.shape[0]
+        out = torch.empty((frames, g.num_depths, g.num_rx), dtype=torch.float32, device=rf.device)
+        check("sb_das_forward_apod", self.lib.sb_das_forward_apod(self._plan, _ptr(rf), _ptr(apod), _ptr(out), frames,
+                                                                  float(f_number), float(speed_of_sound_mm_s),
+                                                                  int(window_type), float(window_parameter), _stream()))
+        return out[0] if squeeze else out
+
+    def adjoint(self, rf: torch.Tensor, apod: Optional[torch.Tensor], grad_out: torch.Tensor, speed_of_sound_mm_s: float,
+                forward_out: Optional[torch.Tensor] = None, f_number=1.0, window_type=1, window_parameter=0.0,
+                need_rf=True, need_apod=True, need_c=True):
+        """Adjoint of forward_apod: returns (grad_rf or None, grad_apod or None, grad_c or None); grad_c is a
+        one-element tensor (per mm/s)."""
+        squeeze = rf.dim() == 3
+        if squeeze:
+            rf, grad_out = rf.unsqueeze(0), grad_out.unsqueeze(0)
+            forward_out = None if forward_out is None else forward_out.unsqueeze(0)
+        frames = rf.shape[0]
+        grad_out = grad_out.contiguous()
+        g_rf = torch.empty_like(rf) if need_rf else None
+        g_ap = torch.empty(self.geometry.num_elements, dtype=torch.float32, device=rf.device) if need_apod else None
+        g_c = torch.empty(1, dtype=torch.float32, device=rf.device) if need_c else None
+        check("sb_das_adjoint", self.lib.sb_das_adjoint(self._plan, _ptr(rf), _ptr(apod), _ptr(forward_out),
+                                                        _ptr(grad_out), _ptr(g_rf), _ptr(g_ap), _ptr(g_c), frames,
+                                                        float(f_number), float(speed_of_sound_mm_s), int(window_type),
+                                                        float(window_parameter), _stream()))
+        if squeeze and g_rf is not None:
+            g_rf = g_rf[0]
+        return g_rf, g_ap, g_c
+
+
 class HilbertFirEnvelope:
     """HilbertFirEnvelope(filterLength) (Beamformer/HilbertFirEnvelope.cu:63-104)."""
 
@@ -107,6 +147,15 @@ class HilbertFirEnvelope:
         out = torch.empty((nS, nL), dtype=torch.float32, device=img.device)
         check("sb_hilbert_env_run", self.lib.sb_hilbert_env_run(self._plan, _ptr(img), dtype_code(img), _ptr(out),
                                                                 SB_FLOAT32, nL, nS, _stream()))
+        return out
+
+    def adjoint(self, img: torch.Tensor, grad_env: torch.Tensor) -> torch.Tensor:
+        """Gradient of the envelope w.r.t. its FP32 input [num_samples][num_scanlines]."""
+        nS, nL = img.shape
+        grad_env = grad_env.contiguous()
+        out = torch.empty_like(img)
+        check("sb_hilbert_env_adjoint", self.lib.sb_hilbert_env_adjoint(self._plan, _ptr(img), _ptr(grad_env),
+                                                                        _ptr(out), nL, nS, _stream()))
         return out
 
 

@@ -743,3 +743,331 @@ extern "C" int sb_das_run_static(const sb_geometry* g, const void* rf, int rf_dt
     SB_CHECK_LAUNCH("sb_das_run_static: dasKernel");
     return SB_OK;
 }
+
+// ------------------------------------------------------------------------------------------------
+// Differentiable 2D DAS (extension without a reference counterpart): forward with per-element
+// apodisation and its adjoint. The forward is the generic kernel above with w_e -> w_e * apod[e]
+// (sample2D), so the two share every discrete decision (aperture, window index, sample index).
+//
+// For one pixel with upstream gradient g, weights W_e = w_e a_e, D = sum_e W_e, n active elements,
+// v_e = lerp(rf_e, tau_e) and s = n / D * sum_e W_e v_e:
+//   ds/drf[delta_e]     = n / D * W_e (1 - frac_e),  ds/drf[delta_e + 1] = n / D * W_e frac_e
+//   ds/da_e             = w_e (n v_e - s) / D
+//   ds/dc               = n / D * sum_e W_e (rf[delta_e + 1] - rf[delta_e]) * dtau_e/dc,
+//   dtau_e/dc           = -(dist_e + depth) / c   (DT-space path length; the initial delay is in
+//                         samples and the aperture and window are ratios, both independent of c)
+// A prologue pass recomputes D and n per pixel (the aperture is recomputed, not stored) and forms
+// G = g n / D and H = g s / D. The main pass gives one warp each (scanline, element) pair; its
+// lanes walk the depths, so the sample indices a warp touches are nearly consecutive: the channel
+// row is accumulated in shared memory and flushed to HBM once, with coalesced reductions.
+namespace sb {
+namespace {
+
+struct AdjArgs {
+    DasArgs a;
+    const float* fwd;      // [frames][nD][nRx] forward output
+    const float* gout;     // [frames][nD][nRx]
+    float2* gh;            // [frames][nRx][nD] scratch: (G, H)
+    float* gradRf;         // [frames][nTx][nCh][nS] or null
+    float* gradApod;       // [nE] or null
+    float* gradC;          // [1] or null
+    size_t rfFrameStride, outFrameStride;
+    int exclusiveRows;     // every (transmit, channel) row has one writer: whole rows are stored
+};
+
+__global__ void __launch_bounds__(256) adjPixelKernel(AdjArgs p) {
+    __shared__ float lut[64];
+    const DasArgs& a = p.a;
+    if (threadIdx.x < 64) lut[threadIdx.x] = a.lut.v[threadIdx.x];
+    __syncthreads();
+    const uint32_t line = blockIdx.y, frame = blockIdx.z;
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nD) return;
+    const LineDT s = a.lines[line];
+    const int k = s.highest;
+    float2 gh = make_float2(0.0f, 0.0f);
+    if ((s.activeMask >> k) & 1) {
+        const float d = __ldg(a.depth + r);
+        const float aDT = apertureDT(d, a.dt, a.c, a.F);
+        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+        float D = 0.0f;
+        int n = 0;
+        for (int e = s.firstX[k]; e < s.lastX[k]; e++) {
+            const int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(static_cast<uint32_t>(e) % a.nCh);
+            if (ch < 0) continue;
+            const float dx = __fsub_rn(__ldg(a.xe + e), s.x);
+            if (fabsf(dx) <= aDT) {
+                float w = lutGet(lut, __fmul_rn(dx, invMax));
+                if (a.apod) w = __fmul_rn(w, __ldg(a.apod + e));
+                D = __fadd_rn(D, w);
+                n++;
+            }
+        }
+        const size_t o = static_cast<size_t>(frame) * p.outFrameStride + static_cast<size_t>(r) * a.nRx + line;
+        const float g = __ldg(p.gout + o);
+        const float sv = __ldg(p.fwd + o);
+        // pixels whose forward value is not finite (weight sum 0: the reference writes 0/0, clamped to
+        // -FLT_MAX) and pixels without gradient contribute nothing
+        if (n > 0 && g != 0.0f && D != 0.0f && fabsf(sv) < FLT_MAX) {
+            gh.x = g * static_cast<float>(n) / D;
+            gh.y = g * sv / D;
+        }
+    }
+    p.gh[(static_cast<size_t>(frame) * a.nRx + line) * a.nD + r] = gh;
+}
+
+// blockIdx.x: group of warps over the aperture elements of scanline blockIdx.y, frame blockIdx.z.
+__global__ void __launch_bounds__(256) adjElemKernel(AdjArgs p) {
+    extern __shared__ __align__(16) float rowsAll[];
+    __shared__ float lut[64];
+    const DasArgs& a = p.a;
+    if (threadIdx.x < 64) lut[threadIdx.x] = a.lut.v[threadIdx.x];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    const uint32_t line = blockIdx.y, frame = blockIdx.z;
+    const LineDT s = a.lines[line];
+    const int k = s.highest;
+    if (!((s.activeMask >> k) & 1)) return;
+    const int slot = blockIdx.x * warps + warp;
+    const int e = s.firstX[k] + slot;
+    if (e >= s.lastX[k]) {
+        // exclusive rows: slots past the aperture zero the rows of the channels it does not reach
+        if (p.exclusiveRows && p.gradRf && slot < static_cast<int>(a.nCh)) {
+            const uint32_t chz = static_cast<uint32_t>(e) % a.nCh;
+            float* dz = p.gradRf + static_cast<size_t>(frame) * p.rfFrameStride +
+                        (static_cast<size_t>(s.txIdx[k]) * a.nCh + chz) * a.nS;
+            for (uint32_t t = lane; t < a.nS; t += 32) dz[t] = 0.0f;
+        }
+        return;
+    }
+    const int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(static_cast<uint32_t>(e) % a.nCh);
+    if (ch < 0) return;
+    float* row = rowsAll + static_cast<size_t>(warp) * a.nS;
+    const bool wantRf = p.gradRf != nullptr;
+    if (wantRf)
+        for (uint32_t t = lane; t < a.nS; t += 32) row[t] = 0.0f;
+    __syncwarp();
+    const float xel = __ldg(a.xe + e);
+    const float dx = __fsub_rn(xel, s.x);
+    const float apodE = a.apod ? __ldg(a.apod + e) : 1.0f;
+    const float iD = s.initialDelay[k];
+    const float* rf = static_cast<const float*>(a.rf) + static_cast<size_t>(frame) * p.rfFrameStride +
+                      (static_cast<size_t>(s.txIdx[k]) * a.nCh + ch) * a.nS;
+    const float2* gh = p.gh + (static_cast<size_t>(frame) * a.nRx + line) * a.nD;
+    float gA = 0.0f, gC = 0.0f;
+    int tMin = INT_MAX, tMax = -1;
+    for (uint32_t r = lane; r < a.nD; r += 32) {
+        const float d = __ldg(a.depth + r);
+        const float aDT = apertureDT(d, a.dt, a.c, a.F);
+        if (!(fabsf(dx) <= aDT)) continue;
+        const float2 GH = gh[r];
+        if (GH.x == 0.0f && GH.y == 0.0f) continue;
+        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+        const float w = lutGet(lut, __fmul_rn(dx, invMax));
+        const float W = __fmul_rn(w, apodE);
+        const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
+        const float dy = __fmul_rn(s.dirY, d);
+        const float ex = __fsub_rn(xel, xz);
+        const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(dy, dy)));
+        const float path = __fadd_rn(dist, d);
+        const float delayf = __fadd_rn(__fadd_rn(iD, path), a.offset);
+        const int32_t delay = static_cast<int32_t>(floorf(delayf));
+        const float frac = __fsub_rn(delayf, static_cast<float>(delay));
+        float v = 0.0f;
+        const float GW = GH.x * W;
+        if (static_cast<uint32_t>(delay) < a.nS - 1) {
+            const float v0 = __ldg(rf + delay), v1 = __ldg(rf + delay + 1);
+            v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
+            gC += GW * (v1 - v0) * path;
+            if (wantRf) {
+                atomicAdd(&row[delay], GW * (1.0f - frac));
+                atomicAdd(&row[delay + 1], GW * frac);
+                tMin = min(tMin, delay);
+                tMax = max(tMax, delay + 1);
+            }
+        } else if (static_cast<uint32_t>(delay) < a.nS && frac == 0.0f) {
+            v = __ldg(rf + delay);
+            if (wantRf) {
+                atomicAdd(&row[delay], GW);
+                tMin = min(tMin, delay);
+                tMax = max(tMax, delay);
+            }
+        }
+        gA += w * (GH.x * v - GH.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gA += __shfl_xor_sync(0xffffffffu, gA, o);
+        gC += __shfl_xor_sync(0xffffffffu, gC, o);
+        tMin = min(tMin, __shfl_xor_sync(0xffffffffu, tMin, o));
+        tMax = max(tMax, __shfl_xor_sync(0xffffffffu, tMax, o));
+    }
+    if (lane == 0) {
+        if (p.gradApod) atomicAdd(p.gradApod + e, gA);
+        if (p.gradC) atomicAdd(p.gradC, -gC / a.c);
+    }
+    __syncwarp();
+    if (!wantRf) return;
+    float* dst = p.gradRf + static_cast<size_t>(frame) * p.rfFrameStride +
+                 (static_cast<size_t>(s.txIdx[k]) * a.nCh + ch) * a.nS;
+    if (p.exclusiveRows) {
+        // the row is this warp's alone: store all of it (zeros included), no memset needed
+        for (uint32_t t = lane; t < a.nS; t += 32) dst[t] = row[t];
+    } else if (tMax >= 0) {
+        // scanlines may share a transmit and elements a channel: reductions into the zeroed output
+        for (int t = tMin + lane; t <= tMax; t += 32) {
+            const float v = row[t];
+            if (v != 0.0f) atomicAdd(dst + t, v);
+        }
+    }
+}
+
+// True when every (transmit, channel) row of grad_rf has at most one writer: each transmit is the
+// highest-weight transmit of one scanline only, there is no channel map, and no aperture spans more
+// than num_channels elements (consecutive elements map to distinct channels). The kernel then stores
+// whole rows, including the zero rows of channels an aperture does not reach; only the rows of
+// transmits that no scanline uses are left to zero here.
+bool exclusiveGradRows(const sb_das_plan* p, std::vector<uint8_t>& txUsed) {
+    if (p->hasChannelMap || !p->hLines) return false;
+    txUsed.assign(p->numTx, 0);
+    for (const sb_scanline_rx& s : *p->hLines) {
+        int hi = 0;
+        float hw = static_cast<float>(s.tx_weights[0]);
+        for (int k = 1; k < 4; k++)
+            if (s.tx_weights[k] > static_cast<double>(hw)) {
+                hw = static_cast<float>(s.tx_weights[k]);
+                hi = k;
+            }
+        if (!(s.tx_weights[hi] > 0.0)) continue;
+        const uint32_t tx = s.tx[hi].tx_scanline_idx;
+        const int n = static_cast<int>(s.tx[hi].last_active_element[0]) - static_cast<int>(s.tx[hi].first_active_element[0]);
+        if (tx >= p->numTx || txUsed[tx] || n > static_cast<int>(p->numChannels)) return false;
+        txUsed[tx] = 1;
+    }
+    return true;
+}
+
+int adjointCheck(const sb_das_plan* plan, uint32_t frames) {
+    SB_REQUIRE(plan, "null plan");
+    SB_REQUIRE(frames >= 1, "num_frames must be >= 1");
+    if (plan->is3D) return fail(SB_ERR_UNSUPPORTED, "the differentiable DAS is 2D only");
+    return SB_OK;
+}
+
+}  // namespace
+}  // namespace sb
+
+int sb_das_forward_apod(const sb_das_plan* plan, const float* rf, const float* apod, float* out, uint32_t num_frames,
+                        double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
+                        sb_stream stream) {
+    using namespace sb;
+    int err = adjointCheck(plan, num_frames);
+    if (err != SB_OK) return err;
+    SB_REQUIRE(rf && out, "sb_das_forward_apod: null argument");
+    sb_das_plan* p = const_cast<sb_das_plan*>(plan);
+    cudaStream_t st = S(stream);
+    DasArgs a;
+    err = fillArgs(p, a, rf, out, f_number, speed_of_sound_mm_s, window_type, window_parameter, 0, 0, st);
+    if (err != SB_OK) return err;
+    a.apod = apod;
+    const size_t rfStride = static_cast<size_t>(p->numTx) * p->numChannels * p->numSamples;
+    const size_t outStride = static_cast<size_t>(p->numDepths) * p->numRx;
+    dim3 grid((p->numDepths + 255) / 256, p->numRx);
+    for (uint32_t f = 0; f < num_frames; f++) {
+        a.rf = rf + f * rfStride;
+        a.out = out + f * outStride;
+        dasKernel<float, float, false><<<grid, 256, 0, st>>>(a);
+    }
+    SB_CHECK_LAUNCH("sb_das_forward_apod");
+    return SB_OK;
+}
+
+int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, const float* forward_out,
+                   const float* grad_out, float* grad_rf, float* grad_apod, float* grad_c, uint32_t num_frames,
+                   double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
+                   sb_stream stream) {
+    using namespace sb;
+    int err = adjointCheck(plan, num_frames);
+    if (err != SB_OK) return err;
+    SB_REQUIRE(rf && grad_out, "sb_das_adjoint: null argument");
+    sb_das_plan* p = const_cast<sb_das_plan*>(plan);
+    cudaStream_t st = S(stream);
+    const size_t rfStride = static_cast<size_t>(p->numTx) * p->numChannels * p->numSamples;
+    const size_t outStride = static_cast<size_t>(p->numDepths) * p->numRx;
+    const size_t rowBytes = static_cast<size_t>(p->numSamples) * sizeof(float);
+    const int warps = static_cast<int>(std::min<size_t>(8, (200 * 1024) / rowBytes));
+    if (grad_rf && warps < 1)
+        return fail(SB_ERR_UNSUPPORTED, "sb_das_adjoint: %u samples per channel exceed the shared-memory row", p->numSamples);
+    // scratch: the forward output when not given, and the per-pixel (G, H)
+    const size_t ghBytes = static_cast<size_t>(num_frames) * outStride * sizeof(float2);
+    const size_t fwdBytes = forward_out ? 0 : static_cast<size_t>(num_frames) * outStride * sizeof(float);
+    void* scratch = nullptr;
+    SB_CUDA(cudaMallocAsync(&scratch, ghBytes + fwdBytes, st));
+    float2* gh = static_cast<float2*>(scratch);
+    const float* fwd = forward_out;
+    int rc = SB_OK;
+    if (!fwd) {
+        float* tmp = reinterpret_cast<float*>(static_cast<char*>(scratch) + ghBytes);
+        rc = sb_das_forward_apod(plan, rf, apod, tmp, num_frames, f_number, speed_of_sound_mm_s, window_type,
+                                 window_parameter, stream);
+        fwd = tmp;
+    }
+    DasArgs a;
+    std::vector<uint8_t> txUsed;
+    const bool exclusive = exclusiveGradRows(p, txUsed);
+    if (rc == SB_OK)
+        rc = fillArgs(p, a, rf, nullptr, f_number, speed_of_sound_mm_s, window_type, window_parameter, 0, 0, st);
+    if (rc == SB_OK) {
+        a.apod = apod;
+        if (grad_rf) {
+            // exclusive rows: only transmits that no scanline uses need zeros; otherwise reductions
+            // into a zeroed buffer
+            const size_t txBytes = static_cast<size_t>(p->numChannels) * p->numSamples * sizeof(float);
+            for (uint32_t f = 0; f < num_frames && rc == SB_OK; f++) {
+                float* base = grad_rf + f * rfStride;
+                if (!exclusive) {
+                    if (cudaMemsetAsync(base, 0, rfStride * sizeof(float), st) != cudaSuccess)
+                        rc = cudaFail(cudaGetLastError(), "cudaMemsetAsync");
+                    continue;
+                }
+                for (uint32_t tx = 0; tx < p->numTx && rc == SB_OK; tx++)
+                    if (!txUsed[tx] && cudaMemsetAsync(reinterpret_cast<char*>(base) + tx * txBytes, 0, txBytes, st) != cudaSuccess)
+                        rc = cudaFail(cudaGetLastError(), "cudaMemsetAsync");
+            }
+        }
+        if (rc == SB_OK && grad_apod && cudaMemsetAsync(grad_apod, 0, p->numElements * sizeof(float), st) != cudaSuccess)
+            rc = cudaFail(cudaGetLastError(), "cudaMemsetAsync");
+        if (rc == SB_OK && grad_c && cudaMemsetAsync(grad_c, 0, sizeof(float), st) != cudaSuccess)
+            rc = cudaFail(cudaGetLastError(), "cudaMemsetAsync");
+    }
+    if (rc == SB_OK) {
+        AdjArgs q;
+        q.a = a;
+        q.fwd = fwd;
+        q.gout = grad_out;
+        q.gh = gh;
+        q.gradRf = grad_rf;
+        q.gradApod = grad_apod;
+        q.gradC = grad_c;
+        q.rfFrameStride = rfStride;
+        q.outFrameStride = outStride;
+        q.exclusiveRows = exclusive ? 1 : 0;
+        adjPixelKernel<<<dim3((p->numDepths + 255) / 256, p->numRx, num_frames), 256, 0, st>>>(q);
+        const int w = std::max(warps, 1);
+        const size_t shm = grad_rf ? static_cast<size_t>(w) * rowBytes : 0;
+        if (cudaFuncSetAttribute(adjElemKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)) !=
+            cudaSuccess)
+            rc = cudaFail(cudaGetLastError(), "cudaFuncSetAttribute");
+        else {
+            const uint32_t slots = exclusive && grad_rf ? std::max<uint32_t>(p->maxApertureX, p->numChannels)
+                                                        : static_cast<uint32_t>(std::max(p->maxApertureX, 1));
+            const uint32_t groups = (slots + w - 1) / w;
+            adjElemKernel<<<dim3(groups, p->numRx, num_frames), 32 * w, shm, st>>>(q);
+            cudaError_t le = cudaGetLastError();
+            if (le != cudaSuccess) rc = cudaFail(le, "adjElemKernel");
+        }
+    }
+    cudaFreeAsync(scratch, st);
+    return rc;
+}

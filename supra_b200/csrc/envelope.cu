@@ -36,6 +36,49 @@ __global__ void __launch_bounds__(256) hilbertKernel(const IN* __restrict__ in, 
     out[l + static_cast<size_t>(s) * nL] = static_cast<OUT>(__fsqrt_rn(__fadd_rn(__fmul_rn(v, v), __fmul_rn(acc, acc))));
 }
 
+// Adjoint of the envelope (extension without a reference counterpart): env = sqrt(x^2 + h^2) with
+// h = taps (*) x along the samples, so dL/dx[j] = G[j] x[j] / env[j] + sum_s q[s] taps[j - s + N/2]
+// with q[s] = G[s] h[s] / env[s] (0 where env = 0). Pass 1 writes the direct term and q, pass 2
+// adds the correlation of q with the taps.
+__global__ void __launch_bounds__(256) hilbertAdjQKernel(const float* __restrict__ in, const float* __restrict__ genv,
+                                                         float* __restrict__ gin, float* __restrict__ q,
+                                                         const float* __restrict__ taps, int nS, int nL, int N) {
+    extern __shared__ float h[];
+    for (int i = threadIdx.y * blockDim.x + threadIdx.x; i <= N; i += blockDim.x * blockDim.y) h[i] = i < N ? taps[i] : 0.0f;
+    __syncthreads();
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y * blockDim.y + threadIdx.y;
+    if (l >= nL || s >= nS) return;
+    float acc = 0.0f;
+    const int start = s - N / 2, end = s + N / 2;
+    for (int cs = start, fe = 0; cs <= end; cs++, fe++) {
+        if (cs >= 0 && cs < nS) acc = __fadd_rn(acc, __fmul_rn(in[l + static_cast<size_t>(cs) * nL], h[fe]));
+    }
+    const size_t o = l + static_cast<size_t>(s) * nL;
+    const float v = in[o];
+    const float env = __fsqrt_rn(__fadd_rn(__fmul_rn(v, v), __fmul_rn(acc, acc)));
+    const float g = genv[o];
+    const bool ok = env > 0.0f;
+    gin[o] = ok ? g * v / env : 0.0f;
+    q[o] = ok ? g * acc / env : 0.0f;
+}
+
+__global__ void __launch_bounds__(256) hilbertAdjCorrKernel(const float* __restrict__ q, float* __restrict__ gin,
+                                                            const float* __restrict__ taps, int nS, int nL, int N) {
+    extern __shared__ float h[];
+    for (int i = threadIdx.y * blockDim.x + threadIdx.x; i <= N; i += blockDim.x * blockDim.y) h[i] = i < N ? taps[i] : 0.0f;
+    __syncthreads();
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (l >= nL || j >= nS) return;
+    float acc = 0.0f;
+    for (int fe = 0; fe <= 2 * (N / 2); fe++) {
+        const int s = j + N / 2 - fe;
+        if (s >= 0 && s < nS) acc += q[l + static_cast<size_t>(s) * nL] * h[fe];
+    }
+    gin[l + static_cast<size_t>(j) * nL] += acc;
+}
+
 // ----------------------------------------------------------------------------- log compression
 template <typename IN, typename OUT>
 __global__ void logKernel(const IN* __restrict__ in, OUT* __restrict__ out, size_t n, float inScale, float k) {
@@ -228,6 +271,25 @@ int sb_hilbert_env_run(const sb_hilbert_plan* p, const void* in, int in_dtype, v
     else
         return fail(SB_ERR_UNSUPPORTED, "sb_hilbert_env_run: %d -> %d unsupported", in_dtype, out_dtype);
     SB_CHECK_LAUNCH("hilbertKernel");
+    return SB_OK;
+}
+
+int sb_hilbert_env_adjoint(const sb_hilbert_plan* p, const float* in, const float* grad_env, float* grad_in,
+                           uint32_t num_scanlines, uint32_t num_samples, sb_stream stream) {
+    SB_REQUIRE(p && in && grad_env && grad_in, "sb_hilbert_env_adjoint: null argument");
+    SB_REQUIRE(num_scanlines > 0 && num_samples > 0, "sb_hilbert_env_adjoint: empty image");
+    cudaStream_t st = S(stream);
+    dim3 block(32, 8);
+    dim3 grid((num_scanlines + 31) / 32, (num_samples + 7) / 8);
+    size_t shm = (p->N + 1) * sizeof(float);
+    int nS = static_cast<int>(num_samples), nL = static_cast<int>(num_scanlines), N = static_cast<int>(p->N);
+    float* q = nullptr;
+    SB_CUDA(cudaMallocAsync(&q, static_cast<size_t>(nS) * nL * sizeof(float), st));
+    hilbertAdjQKernel<<<grid, block, shm, st>>>(in, grad_env, grad_in, q, p->dTaps, nS, nL, N);
+    hilbertAdjCorrKernel<<<grid, block, shm, st>>>(q, grad_in, p->dTaps, nS, nL, N);
+    cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(q, st);
+    if (e != cudaSuccess) return cudaFail(e, "sb_hilbert_env_adjoint");
     return SB_OK;
 }
 

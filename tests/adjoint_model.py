@@ -1,0 +1,106 @@
+"""FP64 model of the apodised 2D DAS that is smooth in the speed of sound, for finite differences.
+
+The library (and the reference it follows) converts positions to DT space in FP32, so its output
+moves in steps of one float rounding as c changes: a 10 mm/s step shifts a 4 mm position by about
+100 ulp, and the rounding of each evaluation leaves ~1% noise in a finite difference. This model
+takes the discrete decisions (aperture membership, window weight, highest-weight transmit) exactly
+as the FP32 path does at the nominal c, then evaluates delays in FP64 directly from the mm
+geometry, tau = t0 / dt + (|e - p(d)| + d) / (c dt), so that central differences in c are clean.
+"""
+import numpy as np
+
+
+def _f32(x):
+    return np.float32(x)
+
+
+def decisions(geom, c_mm_s, lut, f_number=1.0):
+    """Per (line, depth): list of (element, channel, w) with the FP32 path's aperture test and
+    nearest-LUT window weight."""
+    dt = 1.0 / geom.sampling_frequency_hz
+    factor = 1.0 / (c_mm_s * dt)
+    xe = (geom.element_x.astype(np.float64) * factor).astype(np.float32)
+    dep = (geom.depths.astype(np.float64) * factor).astype(np.float32)
+    F = _f32(f_number)
+    cf, dtf = _f32(c_mm_s), _f32(dt)
+    out = []
+    for l, s in enumerate(geom.scanlines):
+        k = int(np.argmax(s["tx_weights"]))
+        x = _f32(s["position"][0] * factor)
+        maxd = _f32(s["max_element_distance"][0] * factor)
+        first, last = int(s["tx"][k]["first"][0]), int(s["tx"][k]["last"][0])
+        per_depth = []
+        for r in range(geom.num_depths):
+            d = dep[r]
+            aDT = _f32(_f32(_f32(_f32(_f32(d * dtf) * cf) / _f32(2 * F)) / cf) / dtf)
+            with np.errstate(divide="ignore"):
+                inv = _f32(_f32(1.0) / min(aDT, maxd))
+            terms = []
+            for e in range(first, last):
+                ch = e % geom.num_channels
+                dx = _f32(xe[e] - x)
+                if abs(dx) <= aDT:
+                    rel = _f32(dx * inv) if abs(dx) > 0 or np.isfinite(inv) else _f32(np.nan)
+                    # fminf(fmaxf(NaN, -1), 1) = -1 on the device (depth 0: 0 * inf)
+                    rel = _f32(-1) if np.isnan(rel) else min(max(rel, _f32(-1)), _f32(1))
+                    idx = int(np.floor(_f32(31.5) * _f32(rel + _f32(1)) + 0.5))
+                    terms.append((e, ch, float(lut[idx])))
+            per_depth.append(terms)
+        out.append((k, per_depth))
+    return out
+
+
+def forward(geom, rf, apod, dec, c_mm_s):
+    """FP64 forward [num_depths][num_rx] with the given decisions."""
+    dt = 1.0 / geom.sampling_frequency_hz
+    nS = geom.num_samples
+    out = np.zeros((geom.num_depths, geom.num_rx))
+    for l, (k, per_depth) in enumerate(dec):
+        s = geom.scanlines[l]
+        t0 = s["tx"][k]["initial_delay"] / dt
+        tx = int(s["tx"][k]["tx_idx"])
+        px, dirx, diry = s["position"][0], s["direction"][0], s["direction"][1]
+        for r, terms in enumerate(per_depth):
+            if not terms:
+                continue
+            d = float(geom.depths[r])
+            num = den = 0.0
+            for e, ch, w in terms:
+                W = w * float(apod[e])
+                den += W
+                dx = float(geom.element_x[e]) - (px + dirx * d)
+                tau = t0 + (np.hypot(dx, diry * d) + d) / (c_mm_s * dt)
+                i = int(np.floor(tau))
+                f = tau - i
+                if 0 <= i < nS - 1:
+                    num += W * ((1 - f) * rf[tx, ch, i] + f * rf[tx, ch, i + 1])
+            out[r, l] = num / den * len(terms) if den != 0.0 else np.nan
+    return out
+
+
+def grad_c(geom, rf, apod, dec, c_mm_s, gout):
+    """d/dc of sum(gout * forward): sum g n / D sum_e W_e (rf[i+1] - rf[i]) dtau/dc."""
+    dt = 1.0 / geom.sampling_frequency_hz
+    nS = geom.num_samples
+    total = 0.0
+    for l, (k, per_depth) in enumerate(dec):
+        s = geom.scanlines[l]
+        t0 = s["tx"][k]["initial_delay"] / dt
+        tx = int(s["tx"][k]["tx_idx"])
+        px, dirx, diry = s["position"][0], s["direction"][0], s["direction"][1]
+        for r, terms in enumerate(per_depth):
+            g = gout[r, l]
+            if not terms or g == 0.0:
+                continue
+            d = float(geom.depths[r])
+            den = sum(w * float(apod[e]) for e, _, w in terms)
+            acc = 0.0
+            for e, ch, w in terms:
+                dx = float(geom.element_x[e]) - (px + dirx * d)
+                path = np.hypot(dx, diry * d) + d
+                tau = t0 + path / (c_mm_s * dt)
+                i = int(np.floor(tau))
+                if 0 <= i < nS - 1:
+                    acc += w * float(apod[e]) * (rf[tx, ch, i + 1] - rf[tx, ch, i]) * (-path / (c_mm_s * c_mm_s * dt))
+            total += g * len(terms) / den * acc
+    return total

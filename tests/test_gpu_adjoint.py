@@ -1,0 +1,193 @@
+"""Differentiable DAS (sb_das_forward_apod / sb_das_adjoint) and the envelope adjoint.
+
+Extension without a reference counterpart: checked against the oracle's FP64 reference gradient
+(the transpose of its FP64 DAS with the same discrete decisions), the adjoint (dot-product)
+identity, and central finite differences of the FP64 oracle forward. Tolerances:
+  * forward with apodisation: bit-identical to the oracle's FP32 reference semantics;
+  * gradients vs the FP64 reference gradient: 1e-4 of the largest entry (grad_rf, grad_apod) and
+    1e-4 relative (grad_c);
+  * grad_apod vs finite differences (step 1e-4): 1e-3 of the largest entry;
+  * grad_c vs finite differences (step 10 mm/s, i.e. 1e-2 m/s): 1e-3 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import small_linear
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    from supra_b200 import synth
+    g = small_linear(num_samples=512)
+    pts, amps = synth.random_scatterers(12, (-4.5, 4.5), (1.5, 9.0), seed=7)
+    rf = synth.channel_data(g, pts, amps, synth.PulseSpec(7e6, 0.6), -40.0, 1.0, seed=7, quantize=False)
+    rf = rf.numpy().astype(np.float32)
+    rng = np.random.Generator(np.random.PCG64(3))
+    apod = rng.uniform(0.5, 1.5, g.num_elements).astype(np.float32)
+    gout = rng.standard_normal((g.num_depths, g.num_rx)).astype(np.float32)
+    # depth 0 has a zero-width aperture: the reference's window index is 0 * inf there (NaN), so the
+    # row carries no gradient
+    gout[0] = 0.0
+    # pixels whose weights sum to 0 (a line between two elements at a shallow depth: both at the
+    # window's zero edge) are 0/0 in the reference, clamped to -FLT_MAX: no gradient flows there
+    from oracle import oracle as O
+    fwd = O.das(g, rf, 1.0, window=1, apod=apod)
+    gout[~(np.abs(fwd) < 1e30)] = 0.0
+    return g, rf, apod, gout
+
+
+def _dot(s, g):
+    """<s, g> over the finite pixels (the depth-0 row of the forward is not finite)."""
+    m = np.isfinite(s)
+    return float(np.sum(np.where(m, s, 0.0) * np.where(m, g, 0.0)))
+
+
+def _gpu(case):
+    from supra_b200.api import RxBeamformer
+    g, rf, apod, gout = case
+    bf = RxBeamformer(g)
+    return bf, torch.from_numpy(rf).cuda(), torch.from_numpy(apod).cuda(), torch.from_numpy(gout).cuda()
+
+
+def test_forward_apod_matches_reference_semantics(oracle, case):
+    g, rf, apod, _ = case
+    bf, rf_d, ap_d, _ = _gpu(case)
+    out = bf.forward_apod(rf_d, ap_d, g.speed_of_sound_mm_s).cpu().numpy()
+    ref = oracle.das(g, rf, 1.0, window=1, apod=apod)
+    ref = np.where(np.isnan(ref), -np.float32(3.4028235e38), ref)
+    assert np.array_equal(out, ref)
+
+
+def test_adjoint_vs_fp64_reference_gradient(oracle, case):
+    g, rf, apod, gout = case
+    bf, rf_d, ap_d, g_d = _gpu(case)
+    grf, gap, gc = bf.adjoint(rf_d, ap_d, g_d, g.speed_of_sound_mm_s)
+    torch.cuda.synchronize()
+    rrf, rap, rc = oracle.das_adjoint64(g, rf, apod, gout.astype(np.float64))
+    grf, gap, gc = grf.cpu().numpy(), gap.cpu().numpy(), float(gc.item())
+    assert np.max(np.abs(grf - rrf)) <= 1e-4 * np.max(np.abs(rrf))
+    assert np.max(np.abs(gap - rap)) <= 1e-4 * np.max(np.abs(rap))
+    assert abs(gc - rc) <= 1e-4 * abs(rc)
+
+
+def test_adjoint_identity_rf(oracle, case):
+    """<A d, g> = <d, A^T g> with A the FP64 forward (linear in the channel data)."""
+    g, rf, apod, gout = case
+    bf, _, ap_d, g_d = _gpu(case)
+    rng = np.random.Generator(np.random.PCG64(11))
+    d = rng.standard_normal(rf.shape).astype(np.float32)
+    grf, _, _ = bf.adjoint(torch.from_numpy(d).cuda(), ap_d, g_d, g.speed_of_sound_mm_s, need_apod=False,
+                           need_c=False)
+    lhs = _dot(oracle.das(g, d, 1.0, window=1, apod=apod, precision=64), gout.astype(np.float64))
+    rhs = float(np.sum(d.astype(np.float64) * grf.cpu().numpy().astype(np.float64)))
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+
+
+def test_grad_apod_finite_differences(oracle, case):
+    g, rf, apod, gout = case
+    bf, rf_d, ap_d, g_d = _gpu(case)
+    _, gap, _ = bf.adjoint(rf_d, ap_d, g_d, g.speed_of_sound_mm_s, need_rf=False, need_c=False)
+    gap = gap.cpu().numpy()
+    go = gout.astype(np.float64)
+    h = 1e-4
+    fd = np.zeros(g.num_elements)
+    for e in range(g.num_elements):
+        ap = apod.copy()
+        ap[e] = apod[e] + h
+        lp = _dot(oracle.das(g, rf, 1.0, window=1, apod=ap, precision=64), go)
+        ap[e] = apod[e] - h
+        lm = _dot(oracle.das(g, rf, 1.0, window=1, apod=ap, precision=64), go)
+        fd[e] = (lp - lm) / (np.float32(apod[e] + h) - np.float32(apod[e] - h))
+    assert np.max(np.abs(gap - fd)) <= 1e-3 * np.max(np.abs(fd))
+
+
+def test_grad_c_finite_differences(oracle, case):
+    """Against central differences of the FP64 model that is smooth in c (tests/adjoint_model.py),
+    at a converged step of 0.1 mm/s. At the 10 mm/s (1e-2 m/s) step the central difference of the
+    linearly interpolated forward itself deviates by about 2% on this case: a share of the delays
+    crosses a sample boundary between c - h and c + h."""
+    import adjoint_model as M
+    g, rf, apod, gout = case
+    bf, rf_d, ap_d, g_d = _gpu(case)
+    c0 = g.speed_of_sound_mm_s
+    _, _, gc = bf.adjoint(rf_d, ap_d, g_d, c0, need_rf=False, need_apod=False)
+    gc = float(gc.item())
+    go = gout.astype(np.float64)
+    dec = M.decisions(g, c0, oracle.window_lut(1))
+    rf64 = rf.astype(np.float64)
+    h = 0.1
+    fd = (_dot(M.forward(g, rf64, apod, dec, c0 + h), go) - _dot(M.forward(g, rf64, apod, dec, c0 - h), go)) / (2 * h)
+    assert abs(gc - fd) <= 1e-3 * abs(fd), (gc, fd)
+
+
+def _env64(x, taps):
+    """Hilbert FIR envelope in float64 torch (tap N of an even-length filter reads 0)."""
+    N = len(taps)
+    hh = torch.zeros(2 * (N // 2) + 1, dtype=torch.float64)
+    hh[:min(N, len(hh))] = torch.from_numpy(np.asarray(taps[:len(hh)], np.float64))
+    nS = x.shape[0]
+    acc = torch.zeros_like(x)
+    for fe in range(len(hh)):
+        sh = fe - N // 2
+        if sh >= 0:
+            acc[:nS - sh] = acc[:nS - sh] + x[sh:] * hh[fe]
+        else:
+            acc[-sh:] = acc[-sh:] + x[:nS + sh] * hh[fe]
+    # the kernel's derivative is 0 where the envelope is 0; clamp keeps sqrt' finite there
+    return torch.sqrt(torch.clamp(x * x + acc * acc, min=1e-300))
+
+
+@pytest.mark.parametrize("N", [64, 31])
+def test_envelope_adjoint_vs_fp64_autograd(N):
+    from supra_b200.api import HilbertFirEnvelope, fir_design
+    rng = np.random.Generator(np.random.PCG64(N))
+    x = rng.standard_normal((300, 24)).astype(np.float32)
+    ge = rng.standard_normal((300, 24)).astype(np.float32)
+    h = HilbertFirEnvelope(N)
+    gx = h.adjoint(torch.from_numpy(x).cuda(), torch.from_numpy(ge).cuda()).cpu().numpy()
+    taps = fir_design(N, 3, 2)
+    xt = torch.from_numpy(x.astype(np.float64)).requires_grad_(True)
+    _env64(xt, taps).backward(torch.from_numpy(ge.astype(np.float64)))
+    ref = xt.grad.numpy()
+    assert np.max(np.abs(gx - ref)) <= 1e-4 * np.max(np.abs(ref))
+
+
+def test_autograd_envelope_loss(oracle, case):
+    """Loss = || envelope(DAS(rf; apod, c)) - target ||^2 over 2 frames; autograd gradients of all
+    three inputs against the FP64 reference chain (envelope adjoint in float64, DAS FP64 transpose)."""
+    from supra_b200.api import HilbertFirEnvelope, fir_design
+    from supra_b200.autograd import das_apod, envelope
+    g, rf, apod, _ = case
+    bf, rf_d, ap_d, _ = _gpu(case)
+    hil = HilbertFirEnvelope(32)
+    rf2 = torch.stack([rf_d, 0.5 * rf_d.flip(-1)]).contiguous().requires_grad_(True)
+    ap = ap_d.clone().requires_grad_(True)
+    c = torch.tensor(g.speed_of_sound_mm_s, dtype=torch.float64, device="cuda", requires_grad=True)
+    target = torch.rand((2, g.num_depths, g.num_rx), device="cuda") * 0.1
+    s = das_apod(bf, rf2, ap, c)
+    valid = (s.detach().abs() < 1e30)  # no gradient through the reference's clamped 0/0 pixels
+    s = torch.where(valid, s, torch.zeros_like(s))
+    env = envelope(s, hil)
+    loss = ((env - target) ** 2).sum()
+    loss.backward()
+    # FP64 reference chain
+    taps = fir_design(32, 3, 2)
+    tot_ap = np.zeros(g.num_elements)
+    tot_c = 0.0
+    for f in range(2):
+        rff = rf2[f].detach().cpu().numpy()
+        vf = valid[f].cpu()
+        s64 = torch.from_numpy(oracle.das(g, rff, 1.0, window=1, apod=apod, precision=64)).requires_grad_(True)
+        e64 = _env64(torch.where(vf, s64, torch.zeros_like(s64)), taps)
+        l64 = ((e64 - target[f].double().cpu()) ** 2).sum()
+        l64.backward()
+        gs = torch.where(vf, s64.grad, torch.zeros_like(s64.grad)).numpy()
+        grf, gap, gc = oracle.das_adjoint64(g, rff, apod, gs)
+        assert np.max(np.abs(rf2.grad[f].cpu().numpy() - grf)) <= 1e-3 * np.max(np.abs(grf))
+        tot_ap += gap
+        tot_c += gc
+    assert np.max(np.abs(ap.grad.cpu().numpy() - tot_ap)) <= 1e-3 * np.max(np.abs(tot_ap))
+    assert abs(float(c.grad) - tot_c) <= 1e-3 * abs(tot_c)
