@@ -28,9 +28,10 @@ METRIC = "beamformed px/s"
 UNIT = "px/s"
 WORKLOAD = ("c1 batched DAS+IQ: 64 frames/launch (22x P64/1024 smp, 21x P128/2048, 21x P192/3072), 0.3 mm, "
             "fs 40 MHz, 64-ch aperture, F#1 Hann, int16 in; IQ 5 MHz mix, 32-tap LPF, /4, complex64 out")
-# DRAM bytes per beamformed pixel of batchDasIqKernel measured by ncu on a 6-frame case of this workload
-# (dram__bytes_read.sum + dram__bytes_write.sum / pixels); the summary is in profiles/.
-TRAFFIC_BYTES_PER_PX = None
+# DRAM bytes per beamformed pixel of batchPackKernel measured by ncu on a 6-frame case of this workload
+# ((dram__bytes_read.sum + dram__bytes_write.sum) / pixels = 193.2 MB / 1,835,008 px), scaled by pixels;
+# profiles/batchPackKernel_c1_6frames_full.md has the capture.
+TRAFFIC_BYTES_PER_PX = 105.3
 
 
 def peaks():
@@ -140,6 +141,98 @@ def run_reference(args, rank):
     }), flush=True)
 
 
+def _event_ms(fn, n, warm=2):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(n):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / n
+
+
+def extras(wl, plans):
+    """Secondary measurements of the other rows (N = 1 only; device time with CUDA events)."""
+    import torch
+    from supra_b200.api import RxBeamformer, iq_complex, mv_beamform
+    from supra_b200 import workloads as W
+    res = {}
+    # plain per-frame GPU path on the same 64 frames: per-frame DAS kernel + IQ kernel, one frame at a time
+    outs = [torch.empty((wl.geometries[p].num_depths, wl.geometries[p].num_rx), device="cuda") for p in wl.frame_probe]
+
+    def per_frame():
+        for k, p in enumerate(wl.frame_probe):
+            plans[p].beamform(wl.rf[k], 1.0, window_type=1, out=outs[k])
+            iq_complex(outs[k], 40e6, 5e6, 2.5e6, 32, 4)
+    ms = _event_ms(per_frame, 3)
+    res["per_frame_path"] = {"px_per_s": wl.beamformed_px / ms * 1e3, "frames_per_s": len(wl.rf) / ms * 1e3,
+                             "ms_per_batch": ms, "what": "same 64 frames, per-frame DAS + IQ launches"}
+    # c0: one 128-line x 2048-depth frame through the per-frame DAS path
+    from supra_b200 import synth
+    g0, rf0 = synth.c0_frame(0, device="cuda")
+    bf0 = RxBeamformer(g0)
+    o0 = torch.empty((g0.num_depths, g0.num_rx), device="cuda")
+    ms = _event_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0), 20)
+    res["das_c0"] = {"px_per_s": g0.num_rx * g0.num_depths / ms * 1e3, "frames_per_s": 1e3 / ms, "ms": ms}
+    # c2: 3D volume, 32 x 32 lines x 1024 depths from 1024 transmits x 256 channels x 1024 samples
+    g2 = W.c2_geometry()
+    rf2 = W.c2_volume(g2)
+    bf2 = RxBeamformer(g2)
+    o2 = torch.empty((g2.num_depths, g2.num_rx), device="cuda")
+    ms = _event_ms(lambda: bf2.beamform(rf2, 1.0, window_type=1, out=o2), 3, warm=1)
+    res["das3d_c2"] = {"vox_per_s": g2.num_rx * g2.num_depths / ms * 1e3, "volumes_per_s": 1e3 / ms, "ms": ms}
+    del rf2
+    # c3: complex MV, 128 x 2048 systems of 32 x 32, FP64 re-solve above 1e6
+    g3, x3 = W.c3_raw_delayed()
+    ms = _event_ms(lambda: mv_beamform(x3, W.C3_L, W.C3_T, 1.5, False, W.C3_LOADING, 1e6, with_stats=False), 3, warm=1)
+    _, st = mv_beamform(x3, W.C3_L, W.C3_T, 1.5, False, W.C3_LOADING, 1e6)
+    res["mv_c3"] = {"px_per_s": x3.shape[0] * x3.shape[2] / ms * 1e3, "frames_per_s": 1e3 / ms, "ms": ms,
+                    "fp64_systems": int(st.fp64_systems), "max_condition_estimate": float(st.max_condition_estimate)}
+    del x3
+    # c4: differentiable DAS, 16 frames: adjoint (all three gradients) vs forward
+    g4, rf4 = W.c4_batch()
+    bf4 = RxBeamformer(g4)
+    apod = torch.ones(g4.num_elements, device="cuda")
+    c = g4.speed_of_sound_mm_s
+    fwd = bf4.forward_apod(rf4, apod, c)
+    gout = torch.randn_like(fwd)
+    ms_f = _event_ms(lambda: bf4.forward_apod(rf4, apod, c), 5)
+    ms_a = _event_ms(lambda: bf4.adjoint(rf4, apod, gout, c, forward_out=fwd), 5)
+    res["adjoint_c4"] = {"forward_ms": ms_f, "adjoint_ms": ms_a, "adjoint_to_forward": ms_a / ms_f,
+                         "frames": int(rf4.shape[0])}
+    return res
+
+
+def profile_case(case: str):
+    """One small invocation for an ncu capture (no timing)."""
+    import torch
+    from supra_b200.api import BatchedDasIq, RxBeamformer, mv_beamform
+    from supra_b200.workloads import c1_workload
+    if case == "batch":
+        wl = c1_workload(num_frames=6, device="cuda")
+        plans = [RxBeamformer(g) for g in wl.geometries]
+        b = BatchedDasIq([(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)], ctas_per_sm=8, depth_tile=128,
+                         frames_per_pack=4)
+        for _ in range(2):
+            b.run(use_graph=False)
+    elif case == "mv":
+        x = torch.randn((16, 128, 2048), dtype=torch.complex64, device="cuda")
+        mv_beamform(x, 32, 5, 1.5, False, 0.01, 1e6)
+    elif case == "adjoint":
+        from supra_b200 import workloads as W
+        g4, rf4 = W.c4_batch(frames=2)
+        bf4 = RxBeamformer(g4)
+        apod = torch.ones(g4.num_elements, device="cuda")
+        fwd = bf4.forward_apod(rf4, apod, g4.speed_of_sound_mm_s)
+        bf4.adjoint(rf4, apod, torch.randn_like(fwd), g4.speed_of_sound_mm_s, forward_out=fwd)
+    torch.cuda.synchronize()
+    print("profile case done:", case)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -148,7 +241,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements (c0, c2, c3, c4)")
+    ap.add_argument("--frames", type=int, default=64, help="frames per launch (64 = the named workload)")
+    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint"], help="run one small case for ncu and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        return profile_case(args.profile_case)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -167,7 +267,7 @@ def main():
     from supra_b200.api import BatchedDasIq, RxBeamformer, check_device_errors
     from supra_b200.workloads import c1_workload
 
-    wl = c1_workload(device="cuda", seed0=1000 + 100 * rank)
+    wl = c1_workload(num_frames=args.frames, device="cuda", seed0=1000 + 100 * rank)
     plans = [RxBeamformer(g) for g in wl.geometries]
     frames = [(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)]
     batch = BatchedDasIq(frames, 1.0, 1540e3, 1, 0.0, 5e6, 2.5e6, 32, 4)
@@ -235,6 +335,11 @@ def main():
         dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
     e2e_value = px * args.e2e_steps * world / (float(e_ms.item()) / 1e3)
 
+    extra = None
+    if world == 1 and not args.no_extras:
+        extra = extras(wl, plans)
+        extra["per_frame_path"]["batched_speedup"] = value / extra["per_frame_path"]["px_per_s"]
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -264,6 +369,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
+            "rows": extra,
         }
         print(json.dumps(out), flush=True)
     del batch

@@ -307,7 +307,8 @@ int sb_das_forward_apod(const sb_das_plan* plan, const float* rf, const float* a
  * (same shape as rf; may be NULL), grad_apod [num_elements] (summed over frames; may be NULL) and
  * grad_c (one float: derivative w.r.t. the speed of sound in mm/s, summed over frames; may be NULL).
  * forward_out is the forward result for the same arguments (NULL: recomputed). Outputs are
- * overwritten, not accumulated. */
+ * overwritten, not accumulated. The plan keeps the adjoint's device scratch: calls that share a plan
+ * must be ordered on one stream. */
 int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, const float* forward_out,
                    const float* grad_out, float* grad_rf, float* grad_apod, float* grad_c, uint32_t num_frames,
                    double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,

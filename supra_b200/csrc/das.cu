@@ -504,6 +504,7 @@ int sb_das_plan_destroy(sb_das_plan* p) {
     cudaFree(p->dYe);
     cudaFree(p->dDepth);
     cudaFree(p->dLines);
+    cudaFree(p->adjScratch);
     delete p->hLines;
     delete p->hXeMM;
     delete p->hDepthMM;
@@ -1002,8 +1003,15 @@ int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, 
     // scratch: the forward output when not given, and the per-pixel (G, H)
     const size_t ghBytes = static_cast<size_t>(num_frames) * outStride * sizeof(float2);
     const size_t fwdBytes = forward_out ? 0 : static_cast<size_t>(num_frames) * outStride * sizeof(float);
-    void* scratch = nullptr;
-    SB_CUDA(cudaMallocAsync(&scratch, ghBytes + fwdBytes, st));
+    if (p->adjScratchBytes < ghBytes + fwdBytes) {
+        // growing the cached scratch synchronises once (cudaFree); later calls reuse it
+        cudaFree(p->adjScratch);
+        p->adjScratch = nullptr;
+        p->adjScratchBytes = 0;
+        SB_CUDA(cudaMalloc(&p->adjScratch, ghBytes + fwdBytes));
+        p->adjScratchBytes = ghBytes + fwdBytes;
+    }
+    void* scratch = p->adjScratch;
     float2* gh = static_cast<float2*>(scratch);
     const float* fwd = forward_out;
     int rc = SB_OK;
@@ -1068,6 +1076,5 @@ int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, 
             if (le != cudaSuccess) rc = cudaFail(le, "adjElemKernel");
         }
     }
-    cudaFreeAsync(scratch, st);
     return rc;
 }

@@ -49,6 +49,10 @@ struct sb_das_plan {
     std::vector<float>* hXeMM = nullptr;
     std::vector<float>* hDepthMM = nullptr;
     int32_t maxApertureX = 0, maxApertureY = 0;  // largest (last - first) over lines and transmits
+    // device scratch of the adjoint (per-pixel factors, recomputed forward), grown on demand and kept
+    // with the plan so that repeated calls allocate nothing
+    void* adjScratch = nullptr;
+    size_t adjScratchBytes = 0;
 };
 
 namespace sb {
