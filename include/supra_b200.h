@@ -314,6 +314,61 @@ int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, 
                    double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
                    sb_stream stream);
 
+/* ---------------------------------------------------------------- element type conversion */
+
+/* clampCast of n values (SupraLib/utilities/cudaUtility.h:111-147): clamp to the output type's range,
+ * then truncate. in: SB_FLOAT32 or SB_INT16; out: SB_FLOAT32, SB_INT16, SB_UINT8 or SB_UINT16. */
+int sb_convert_run(const void* in, int in_dtype, void* out, int out_dtype, size_t n, sb_stream stream);
+
+/* ---------------------------------------------------------------- nodes
+ * The node layer (C++ API in supra_b200_nodes.hpp) re-hosts SUPRA's receive-path nodes:
+ * BeamformingNode, RawDelayNode, BeamformingMVNode, HilbertFirEnvelopeNode, IQDemodulatorNode,
+ * LogCompressorNode, ScanConverterNode, with the reference's parameter names, types, ranges and
+ * defaults (invalid values fall back to the default and the call returns SB_ERR_INVALID_ARG). These
+ * C entry points expose it to non-C++ hosts and tests. */
+typedef struct sb_node sb_node;
+typedef struct sb_graph sb_graph;
+typedef struct sb_record {
+    int is_image;      /* 1: USImage [size[2]][size[1]][size[0]], x (scanlines) fastest;
+                          0: USRawData [size[2] tx or scanlines][size[1] channels][size[0] samples] */
+    int dtype;         /* sb_dtype */
+    int state;         /* 0 raw, 1 raw-delayed, 2 RF, 3 envelope, 4 log-compressed, 5 scan-converted */
+    uint32_t size[3];
+    void* data;        /* device memory, owned by the node / graph until its next call or destruction */
+} sb_record;
+
+int sb_node_create(const char* type, const char* node_id, sb_node** node);
+int sb_node_destroy(sb_node* node);
+int sb_node_set_param(sb_node* node, const char* name, const char* value);
+int sb_node_get_param(const sb_node* node, const char* name, char* value, size_t value_len);
+int sb_node_param_count(const sb_node* node);
+/* name, type (double, uint32_t, int32_t, bool, string, DataType), range ("min..max" or "a|b|c") and
+ * default of parameter `index`; each buffer holds `len` bytes. */
+int sb_node_param_info(const sb_node* node, int index, char* name, char* type, char* range, char* default_value,
+                       size_t len);
+int sb_node_type_count(void);
+int sb_node_type_name(int index, char* name, size_t len);
+/* Runs the node on caller-owned channel data (delayed = 0: [num_tx][num_channels][num_samples] for
+ * BeamformingNode / RawDelayNode; delayed = 1: RawDelay output [scanline][channel][depth] for
+ * BeamformingMVNode) on `stream`. depth_mm and image_resolution_mm are the image properties the
+ * scan converter reads (depth_mm <= 0: the last receive depth). */
+int sb_node_process_raw(sb_node* node, const sb_geometry* geometry, const void* data, int dtype, int delayed,
+                        uint32_t num_tx, uint32_t num_channels, uint32_t num_samples, double depth_mm,
+                        double image_resolution_mm, sb_stream stream, sb_record* out);
+/* Runs the node on the last output of `upstream`. */
+int sb_node_process_last(sb_node* node, sb_node* upstream, sb_record* out);
+
+/* Graph from the text of a SUPRA XML configuration (inputs, nodes with params, connections). Nodes of
+ * types outside the receive path are passed through. */
+int sb_graph_create_xml(const char* xml_text, sb_graph** graph);
+int sb_graph_destroy(sb_graph* graph);
+/* Comma-separated node IDs in processing order; returns their count. */
+int sb_graph_chain(const sb_graph* graph, char* ids, size_t len);
+int sb_graph_node_get_param(const sb_graph* graph, const char* node_id, const char* name, char* value, size_t len);
+int sb_graph_process_raw(sb_graph* graph, const sb_geometry* geometry, const void* data, int dtype, uint32_t num_tx,
+                         uint32_t num_channels, uint32_t num_samples, double depth_mm, double image_resolution_mm,
+                         sb_stream stream, sb_record* out);
+
 #ifdef __cplusplus
 }
 #endif

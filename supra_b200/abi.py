@@ -122,6 +122,11 @@ class sb_batch_params(C.Structure):
     ]
 
 
+class sb_record(C.Structure):
+    _fields_ = [("is_image", C.c_int), ("dtype", C.c_int), ("state", C.c_int), ("size", C.c_uint32 * 3),
+                ("data", C.c_void_p)]
+
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libsupra_b200.so")
 
@@ -172,6 +177,24 @@ _SIGNATURES = {
     "sb_hilbert_env_adjoint": (_int, [_vp, _vp, _vp, _vp, _u32, _u32, _vp]),
     "sb_das_forward_apod": (_int, [_vp, _vp, _vp, _vp, _u32, _f64, _f64, _int, _f32, _vp]),
     "sb_das_adjoint": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _f64, _f64, _int, _f32, _vp]),
+    "sb_convert_run": (_int, [_vp, _int, _vp, _int, _sz, _vp]),
+    "sb_node_create": (_int, [C.c_char_p, C.c_char_p, C.POINTER(_vp)]),
+    "sb_node_destroy": (_int, [_vp]),
+    "sb_node_set_param": (_int, [_vp, C.c_char_p, C.c_char_p]),
+    "sb_node_get_param": (_int, [_vp, C.c_char_p, C.c_char_p, _sz]),
+    "sb_node_param_count": (_int, [_vp]),
+    "sb_node_param_info": (_int, [_vp, _int, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, _sz]),
+    "sb_node_type_count": (_int, []),
+    "sb_node_type_name": (_int, [_int, C.c_char_p, _sz]),
+    "sb_node_process_raw": (_int, [_vp, C.POINTER(sb_geometry), _vp, _int, _int, _u32, _u32, _u32, _f64, _f64, _vp,
+                                   C.POINTER(sb_record)]),
+    "sb_node_process_last": (_int, [_vp, _vp, C.POINTER(sb_record)]),
+    "sb_graph_create_xml": (_int, [C.c_char_p, C.POINTER(_vp)]),
+    "sb_graph_destroy": (_int, [_vp]),
+    "sb_graph_chain": (_int, [_vp, C.c_char_p, _sz]),
+    "sb_graph_node_get_param": (_int, [_vp, C.c_char_p, C.c_char_p, C.c_char_p, _sz]),
+    "sb_graph_process_raw": (_int, [_vp, C.POINTER(sb_geometry), _vp, _int, _u32, _u32, _u32, _f64, _f64, _vp,
+                                    C.POINTER(sb_record)]),
 }
 
 EXPORTED = tuple(_SIGNATURES)

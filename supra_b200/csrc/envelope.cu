@@ -79,6 +79,14 @@ __global__ void __launch_bounds__(256) hilbertAdjCorrKernel(const float* __restr
     gin[l + static_cast<size_t>(j) * nL] += acc;
 }
 
+// clampCast of a buffer (element type conversion between nodes).
+template <typename IN, typename OUT>
+__global__ void convertKernel(const IN* __restrict__ in, OUT* __restrict__ out, size_t n) {
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+        out[i] = clampCast<OUT>(toFloat(in[i]));
+}
+
 // ----------------------------------------------------------------------------- log compression
 template <typename IN, typename OUT>
 __global__ void logKernel(const IN* __restrict__ in, OUT* __restrict__ out, size_t n, float inScale, float k) {
@@ -290,6 +298,25 @@ int sb_hilbert_env_adjoint(const sb_hilbert_plan* p, const float* in, const floa
     cudaError_t e = cudaGetLastError();
     cudaFreeAsync(q, st);
     if (e != cudaSuccess) return cudaFail(e, "sb_hilbert_env_adjoint");
+    return SB_OK;
+}
+
+int sb_convert_run(const void* in, int in_dtype, void* out, int out_dtype, size_t n, sb_stream stream) {
+    SB_REQUIRE(in && out, "sb_convert_run: null argument");
+    if (n == 0) return SB_OK;
+    cudaStream_t st = S(stream);
+    const int threads = 256;
+    const int blocks = static_cast<int>(std::min<size_t>((n + threads - 1) / threads, 148u * 16u));
+#define SB_CONVERT(IT, OT) convertKernel<IT, OT><<<blocks, threads, 0, st>>>(static_cast<const IT*>(in), static_cast<OT*>(out), n)
+    if (in_dtype == SB_FLOAT32 && out_dtype == SB_FLOAT32) SB_CONVERT(float, float);
+    else if (in_dtype == SB_FLOAT32 && out_dtype == SB_INT16) SB_CONVERT(float, int16_t);
+    else if (in_dtype == SB_FLOAT32 && out_dtype == SB_UINT8) SB_CONVERT(float, uint8_t);
+    else if (in_dtype == SB_FLOAT32 && out_dtype == SB_UINT16) SB_CONVERT(float, uint16_t);
+    else if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_CONVERT(int16_t, float);
+    else if (in_dtype == SB_INT16 && out_dtype == SB_UINT8) SB_CONVERT(int16_t, uint8_t);
+    else return fail(SB_ERR_UNSUPPORTED, "sb_convert_run: %d -> %d unsupported", in_dtype, out_dtype);
+#undef SB_CONVERT
+    SB_CHECK_LAUNCH("convertKernel");
     return SB_OK;
 }
 
