@@ -213,7 +213,7 @@ def profile_case(case: str):
     from supra_b200.api import BatchedDasIq, RxBeamformer, mv_beamform
     from supra_b200.workloads import c1_workload
     if case == "batch":
-        wl = c1_workload(num_frames=6, device="cuda")
+        wl = c1_workload(num_frames=12, device="cuda")  # packs of 4 frames are full
         plans = [RxBeamformer(g) for g in wl.geometries]
         b = BatchedDasIq([(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)], ctas_per_sm=8, depth_tile=128,
                          frames_per_pack=4)
@@ -359,11 +359,13 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "frames_per_launch": len(wl.rf), "beamformed_px_per_launch": px,
                        "parallelism": f"replicas x{world}", "l2": "inputs 2.47 GB per launch > L2, no flush",
-                       "tile_shape": {"ctas_per_sm": shape[0], "depth_tile": shape[1], "frames_per_pack": shape[2]},
+                       "tile_shape": {"ctas_per_sm": shape[0], "depth_tile": shape[1], "frames_per_pack": shape[2],
+                                      "staged": shape[3]},
                        "graph_captured": True},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "batchPackKernel" if shape[2] > 1 else "batchDasIqKernel",
+                         "kernel": ("batchPackStagedKernel" if shape[3] else "batchPackKernel") if shape[2] > 1
+                         else "batchDasIqKernel",
                          "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -274,6 +274,8 @@ typedef struct sb_batch_params {
     int32_t depth_tile;        /* depths per chunk / per CTA block: 128, 256, 384 or 512 (0 = default) */
     int32_t frames_per_pack;   /* 1: per-frame TMA-staged pipeline; 2, 4 or 8: frames of one probe share the
                                   per-element geometry work (0 = default / autotuned) */
+    int32_t staged;            /* with frames_per_pack 2 or 4: 1 stages each depth block's channel samples in
+                                  shared memory with cp.async (ctas_per_sm 1 or 2, depth_tile 128); 0: gathers */
 } sb_batch_params;
 
 /* Persistent batched DAS + complex IQ over frames of uneven probes in one launch. Frames whose
@@ -288,7 +290,7 @@ int sb_batch_set_rf_outputs(sb_batch_plan* plan, float* const* rf_out);
 /* Time candidate tile shapes on the device and keep the fastest; cache_path (may be NULL) stores
  * the choice per problem signature and is consulted first. Returns the chosen shape. Synchronises. */
 int sb_batch_autotune(sb_batch_plan* plan, const char* cache_path, int32_t* ctas_per_sm, int32_t* depth_tile,
-                      int32_t* frames_per_pack, sb_stream stream);
+                      int32_t* frames_per_pack, int32_t* staged, sb_stream stream);
 
 /* Device-side failure flag shared by the kernels with bounded waits: returns SB_ERR_TIMEOUT if any
  * wait gave up since the last call (and clears the flag when reset != 0). Synchronises the device. */

@@ -119,6 +119,7 @@ class sb_batch_params(C.Structure):
         ("ctas_per_sm", C.c_int32),
         ("depth_tile", C.c_int32),
         ("frames_per_pack", C.c_int32),
+        ("staged", C.c_int32),
     ]
 
 
@@ -172,7 +173,8 @@ _SIGNATURES = {
     "sb_batch_plan_destroy": (_int, [_vp]),
     "sb_batch_run": (_int, [_vp, _int, _vp]),
     "sb_batch_set_rf_outputs": (_int, [_vp, _vp]),
-    "sb_batch_autotune": (_int, [_vp, C.c_char_p, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), _vp]),
+    "sb_batch_autotune": (_int, [_vp, C.c_char_p, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32),
+                                 C.POINTER(_i32), _vp]),
     "sb_check_device_errors": (_int, [_int]),
     "sb_hilbert_env_adjoint": (_int, [_vp, _vp, _vp, _vp, _u32, _u32, _vp]),
     "sb_das_forward_apod": (_int, [_vp, _vp, _vp, _vp, _u32, _f64, _f64, _int, _f32, _vp]),

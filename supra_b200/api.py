@@ -343,7 +343,7 @@ class BatchedDasIq:
 
     def __init__(self, frames, f_number=1.0, speed_of_sound_mm_s=1540e3, window_type=1, window_parameter=0.0,
                  mixing_frequency=5e6, cutoff_frequency=2.5e6, lowpass_length=32, decimation=4, ctas_per_sm=0,
-                 depth_tile=0, frames_per_pack=0):
+                 depth_tile=0, frames_per_pack=0, staged=0):
         self.lib = load_library()
         self.frames = frames
         self.outputs = []
@@ -367,6 +367,7 @@ class BatchedDasIq:
         prm.ctas_per_sm = ctas_per_sm
         prm.depth_tile = depth_tile
         prm.frames_per_pack = frames_per_pack
+        prm.staged = staged
         self._plan = C.c_void_p()
         check("sb_batch_plan_create", self.lib.sb_batch_plan_create(arr, len(frames), C.byref(prm), C.byref(self._plan)))
         self.rf_outputs = None
@@ -388,13 +389,12 @@ class BatchedDasIq:
         return self.outputs
 
     def autotune(self, cache_path=None):
-        """Times the candidate shapes and keeps the fastest: (ctas_per_sm, depth_tile, frames_per_pack)."""
-        c = C.c_int32()
-        t = C.c_int32()
-        f = C.c_int32()
+        """Times the candidate shapes and keeps the fastest: (ctas_per_sm, depth_tile, frames_per_pack, staged)."""
+        c, t, f, g = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
         check("sb_batch_autotune", self.lib.sb_batch_autotune(self._plan, cache_path.encode() if cache_path else None,
-                                                              C.byref(c), C.byref(t), C.byref(f), _stream()))
-        return int(c.value), int(t.value), int(f.value)
+                                                              C.byref(c), C.byref(t), C.byref(f), C.byref(g),
+                                                              _stream()))
+        return int(c.value), int(t.value), int(f.value), int(g.value)
 
 
 def check_device_errors(reset=True):

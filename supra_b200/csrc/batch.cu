@@ -23,6 +23,7 @@
 #include "das_core.cuh"
 #include "das_ws.cuh"
 #include "batch_pack.cuh"
+#include "batch_stage.cuh"
 #include "design.h"
 #include "envelope.cuh"
 
@@ -205,10 +206,10 @@ struct sb_batch_plan {
     uint32_t nItems = 0, maxCh = 0, maxD = 0;
     std::vector<BatchFrameDev> hFrames;
     BatchArgs args;
-    int nt = 256, ctasPerSm = 2;
+    int nt = 256, ctasPerSm = 2, staged = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
-    int graphNt = 0, graphCtas = 0, graphFp = 0;
+    int graphNt = 0, graphCtas = 0, graphFp = 0, graphStaged = -1;
     std::string signature;
 };
 
@@ -305,7 +306,20 @@ void freePacks(sb_batch_plan* p) {
     }
 }
 
-int launchBatch(sb_batch_plan* p, int nt, int ctas, int fp, cudaStream_t st) {
+template <int FP, int MINB> int launchStagedPack(const PackArgs& a, int grid, cudaStream_t st) {
+    constexpr size_t shm = stagedSmemBytes<FP>();
+    static bool attrSet = false;  // per instantiation; the attribute is per function and device-independent here
+    if (!attrSet) {
+        SB_CUDA(cudaFuncSetAttribute(batchPackStagedKernel<FP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(shm)));
+        attrSet = true;
+    }
+    batchPackStagedKernel<FP, MINB><<<grid, kStageThreads, shm, st>>>(a);
+    SB_CHECK_LAUNCH("batchPackStagedKernel");
+    return SB_OK;
+}
+
+int launchBatch(sb_batch_plan* p, int nt, int ctas, int fp, int staged, cudaStream_t st) {
     const int grid = smCount() * ctas;
     if (fp > 1) {
         int e = buildPacks(p, fp);
@@ -323,6 +337,13 @@ int launchBatch(sb_batch_plan* p, int nt, int ctas, int fp, cudaStream_t st) {
         a.lut = p->args.lut;
         for (int j = 0; j <= kIqMaxTaps; j++) a.lp[j] = p->args.lp[j];
         SB_CUDA(cudaMemsetAsync(p->dCounter, 0, sizeof(uint32_t), st));
+        if (staged) {
+            if (nt != kStageDepths || (fp != 2 && fp != 4) || ctas < 1 || ctas > 2 || (fp == 4 && ctas > 1))
+                return fail(SB_ERR_INVALID_ARG, "sb_batch: staged packs take depth_tile %d, frames_per_pack 2 (1-2 CTAs/SM) "
+                            "or 4 (1 CTA/SM)", kStageDepths);
+            if (fp == 4) return launchStagedPack<4, 1>(a, grid, st);
+            return ctas == 2 ? launchStagedPack<2, 2>(a, grid, st) : launchStagedPack<2, 1>(a, grid, st);
+        }
 #define SB_PACK_LAUNCH(FPV, NTV, MB) batchPackKernel<FPV, NTV, MB><<<grid, NTV, 0, st>>>(a)
         if (nt != 128 && nt != 256) return fail(SB_ERR_INVALID_ARG, "sb_batch: pack kernel block %d not in {128, 256}", nt);
         // register budget: `ctas` resident CTAs of nt threads per SM
@@ -482,6 +503,11 @@ int sb_batch_plan_create(const sb_batch_frame* frames, uint32_t num_frames, cons
     p->fp = params->frames_per_pack ? params->frames_per_pack : 8;
     p->nt = params->depth_tile ? params->depth_tile : (p->fp > 1 ? 256 : 384);
     p->ctasPerSm = params->ctas_per_sm ? params->ctas_per_sm : (p->fp > 1 ? 4 : 1);
+    p->staged = params->staged ? 1 : 0;
+    if (p->staged && (p->fp != 2 && p->fp != 4))
+        return bad(fail(SB_ERR_INVALID_ARG, "sb_batch_plan_create: staged packs need frames_per_pack 2 or 4"));
+    if (p->staged && !params->depth_tile) p->nt = kStageDepths;
+    if (p->staged && !params->ctas_per_sm) p->ctasPerSm = 1;
     sig << "F" << params->f_number << "L" << params->lowpass_length << "D" << params->decimation;
     p->signature = sig.str();
     if (p->fp == 1 && batchMaxW(p->maxCh, p->maxD, p->ctasPerSm) < 64)
@@ -514,19 +540,20 @@ int sb_batch_set_rf_outputs(sb_batch_plan* p, float* const* rf_out) {
 int sb_batch_run(sb_batch_plan* p, int use_graph, sb_stream stream) {
     SB_REQUIRE(p, "sb_batch_run: null plan");
     cudaStream_t st = S(stream);
-    if (!use_graph) return launchBatch(p, p->nt, p->ctasPerSm, p->fp, st);
+    if (!use_graph) return launchBatch(p, p->nt, p->ctasPerSm, p->fp, p->staged, st);
     if (p->fp > 1) {
         int e = buildPacks(p, p->fp);  // outside the capture: it allocates
         if (e != SB_OK) return e;
     }
-    if (!p->graphExec || p->graphNt != p->nt || p->graphCtas != p->ctasPerSm || p->graphFp != p->fp) {
+    if (!p->graphExec || p->graphNt != p->nt || p->graphCtas != p->ctasPerSm || p->graphFp != p->fp ||
+        p->graphStaged != p->staged) {
         dropGraph(p);
         // capture on a private stream so that the caller's stream may be the legacy default stream
         cudaStream_t cap;
         SB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         int r = SB_OK;
-        if (e == cudaSuccess) r = launchBatch(p, p->nt, p->ctasPerSm, p->fp, cap);
+        if (e == cudaSuccess) r = launchBatch(p, p->nt, p->ctasPerSm, p->fp, p->staged, cap);
         cudaGraph_t g = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(cap, &g);
         cudaStreamDestroy(cap);
@@ -541,53 +568,60 @@ int sb_batch_run(sb_batch_plan* p, int use_graph, sb_stream stream) {
         p->graphNt = p->nt;
         p->graphCtas = p->ctasPerSm;
         p->graphFp = p->fp;
+        p->graphStaged = p->staged;
     }
     SB_CUDA(cudaGraphLaunch(p->graphExec, st));
     return SB_OK;
 }
 
 int sb_batch_autotune(sb_batch_plan* p, const char* cache_path, int32_t* ctas_per_sm, int32_t* depth_tile,
-                      int32_t* frames_per_pack, sb_stream stream) {
+                      int32_t* frames_per_pack, int32_t* staged, sb_stream stream) {
     SB_REQUIRE(p, "sb_batch_autotune: null plan");
     cudaStream_t st = S(stream);
     auto report = [&]() {
         if (ctas_per_sm) *ctas_per_sm = p->ctasPerSm;
         if (depth_tile) *depth_tile = p->nt;
         if (frames_per_pack) *frames_per_pack = p->fp;
+        if (staged) *staged = p->staged;
     };
-    // cached choice for this problem signature?
+    // cached choice for this problem signature? (lines: signature ctas tile frames [staged])
     if (cache_path) {
         std::ifstream in(cache_path);
         std::string key, line;
         while (std::getline(in, line)) {
             std::istringstream ls(line);
-            int c = 0, t = 0, f = 0;
+            int c = 0, t = 0, f = 0, g = 0;
             if (!(ls >> key >> c >> t >> f) || key != p->signature) continue;
-            const bool okPack = f > 1 && packSlot(f) >= 0 && (t == 128 || t == 256) && c >= 1 && c <= 8;
-            const bool okPipe = f == 1 && (t == 128 || t == 256 || t == 384 || t == 512) && c >= 1 && c <= 3 &&
+            if (!(ls >> g)) g = 0;
+            const bool okStaged = g == 1 && t == kStageDepths && ((f == 2 && (c == 1 || c == 2)) || (f == 4 && c == 1));
+            const bool okPack = g == 0 && f > 1 && packSlot(f) >= 0 && (t == 128 || t == 256) && c >= 1 && c <= 12;
+            const bool okPipe = g == 0 && f == 1 && (t == 128 || t == 256 || t == 384 || t == 512) && c >= 1 && c <= 3 &&
                                 batchMaxW(p->maxCh, p->maxD, c) >= 64;
-            if (okPack || okPipe) {
+            if (okStaged || okPack || okPipe) {
                 p->ctasPerSm = c;
                 p->nt = t;
                 p->fp = f;
+                p->staged = g;
                 report();
                 return SB_OK;
             }
         }
     }
-    const int shapes[][3] = {{1, 384, 1}, {4, 256, 4}, {5, 256, 4}, {6, 256, 4}, {12, 128, 4}, {4, 256, 8}, {5, 256, 8}};
+    // {ctas per SM, depth tile, frames per pack, staged}
+    const int shapes[][4] = {{1, 384, 1, 0},  {4, 256, 4, 0},  {5, 256, 4, 0}, {6, 256, 4, 0}, {12, 128, 4, 0},
+                             {4, 256, 8, 0},  {5, 256, 8, 0},  {1, 128, 4, 1}, {1, 128, 2, 1}, {2, 128, 2, 1}};
     float best = 1e30f;
-    int bestC = p->ctasPerSm, bestT = p->nt, bestF = p->fp;
+    int bestC = p->ctasPerSm, bestT = p->nt, bestF = p->fp, bestG = p->staged;
     cudaEvent_t e0, e1;
     SB_CUDA(cudaEventCreate(&e0));
     SB_CUDA(cudaEventCreate(&e1));
     for (const auto& sh : shapes) {
         if (sh[2] == 1 && batchMaxW(p->maxCh, p->maxD, sh[0]) < 64) continue;
-        int r = launchBatch(p, sh[1], sh[0], sh[2], st);  // warm-up (builds pack tables)
+        int r = launchBatch(p, sh[1], sh[0], sh[2], sh[3], st);  // warm-up (builds pack tables)
         if (r != SB_OK) continue;
         SB_CUDA(cudaEventRecord(e0, st));
         for (int i = 0; i < 3; i++) {
-            r = launchBatch(p, sh[1], sh[0], sh[2], st);
+            r = launchBatch(p, sh[1], sh[0], sh[2], sh[3], st);
             if (r != SB_OK) break;
         }
         SB_CUDA(cudaEventRecord(e1, st));
@@ -600,6 +634,7 @@ int sb_batch_autotune(sb_batch_plan* p, const char* cache_path, int32_t* ctas_pe
             bestC = sh[0];
             bestT = sh[1];
             bestF = sh[2];
+            bestG = sh[3];
         }
     }
     cudaEventDestroy(e0);
@@ -607,10 +642,11 @@ int sb_batch_autotune(sb_batch_plan* p, const char* cache_path, int32_t* ctas_pe
     p->ctasPerSm = bestC;
     p->nt = bestT;
     p->fp = bestF;
+    p->staged = bestG;
     report();
     if (cache_path) {
         std::ofstream out(cache_path, std::ios::app);
-        if (out) out << p->signature << " " << bestC << " " << bestT << " " << bestF << "\n";
+        if (out) out << p->signature << " " << bestC << " " << bestT << " " << bestF << " " << bestG << "\n";
     }
     return SB_OK;
 }

@@ -104,15 +104,15 @@ __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float*
             wB = interior ? __fmul_rn(w, frac) : (lastOne ? w : 0.0f);
             wA = interior ? __fmul_rn(w, __fsub_rn(1.0f, frac)) : 0.0f;
         }
-        const uint32_t off = static_cast<uint32_t>(e.ch) * nS + idx;
+        const uint32_t off = static_cast<uint32_t>(e.ch) + idx;  // e.ch holds the row offset
+        // every slot of a partial pack points at valid data (frame 0): no per-frame predicate; the sums
+        // of empty slots are never written
 #pragma unroll
         for (int f = 0; f < FP; f++) {
-            if (f < nf) {
-                const int16_t* p = tb[f] + off;
-                const float v0 = static_cast<float>(__ldg(p));
-                const float v1 = s16ToFloat(__ldg(p + 1));
-                acc.v[f] = fmaf(wB, v1, fmaf(wA, v0, acc.v[f]));
-            }
+            const int16_t* p = tb[f] + off;
+            const float v0 = static_cast<float>(__ldg(p));
+            const float v1 = s16ToFloat(__ldg(p + 1));
+            acc.v[f] = fmaf(wB, v1, fmaf(wA, v0, acc.v[f]));
         }
     }
 }
@@ -146,34 +146,29 @@ __device__ __forceinline__ void packDepthDeepPipelined(const ElemRec* el, int n,
         const uint32_t idx = interior ? static_cast<uint32_t>(delay) : (lastOne ? nS - 2 : 0u);
         g.wB = interior ? __fmul_rn(e.wDeep, frac) : (lastOne ? e.wDeep : 0.0f);
         g.wA = interior ? __fmul_rn(e.wDeep, __fsub_rn(1.0f, frac)) : 0.0f;
-        g.off = static_cast<uint32_t>(e.ch) * nS + idx;
+        g.off = static_cast<uint32_t>(e.ch) + idx;  // e.ch holds the row offset
         return g;
     };
     int16_t a0[FP], b0[FP], a1[FP], b1[FP];
     G g0 = geom(0);
     G g1 = n > 1 ? geom(1) : g0;
+    // all slots load valid addresses (empty pack slots alias frame 0, the step past the last element
+    // repeats it), so the loads carry no predicate
 #pragma unroll
     for (int f = 0; f < FP; f++) {
-        a0[f] = b0[f] = 0;
-        if (f < nf) {
-            a0[f] = __ldg(tb[f] + g0.off);
-            b0[f] = __ldg(tb[f] + g0.off + 1);
-        }
+        a0[f] = __ldg(tb[f] + g0.off);
+        b0[f] = __ldg(tb[f] + g0.off + 1);
     }
     for (int j = 0; j < n; j++) {
-        const bool more = j + 1 < n;
 #pragma unroll
         for (int f = 0; f < FP; f++) {
-            a1[f] = b1[f] = 0;
-            if (f < nf && more) {
-                a1[f] = __ldg(tb[f] + g1.off);
-                b1[f] = __ldg(tb[f] + g1.off + 1);
-            }
+            a1[f] = __ldg(tb[f] + g1.off);
+            b1[f] = __ldg(tb[f] + g1.off + 1);
         }
         const G g2 = j + 2 < n ? geom(j + 2) : g1;
 #pragma unroll
         for (int f = 0; f < FP; f++) {
-            if (f < nf) acc.v[f] = fmaf(g0.wB, s16ToFloat(b0[f]), fmaf(g0.wA, static_cast<float>(a0[f]), acc.v[f]));
+            acc.v[f] = fmaf(g0.wB, s16ToFloat(b0[f]), fmaf(g0.wA, static_cast<float>(a0[f]), acc.v[f]));
             a0[f] = a1[f];
             b0[f] = b1[f];
         }
@@ -225,8 +220,9 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             float sum = 0.0f;
             if (valid) {
                 for (int j = 0; j < n0; j++) {
-                    const ElemRec r = el[j];
+                    ElemRec r = el[j];
                     if (r.ch < 0) continue;
+                    r.ch = r.ch * static_cast<int>(P.nS);  // from here on: the channel's row offset
                     el[m++] = r;
                     sum = __fadd_rn(sum, r.wDeep);
                     if (!(fabsf(r.dx) <= s.maxDistX)) ok = 0;
@@ -242,7 +238,7 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         const int16_t* tb[FP];
 #pragma unroll
         for (int f = 0; f < FP; f++)
-            tb[f] = (f < nf) ? P.rf[f] + static_cast<size_t>(s.txIdx) * P.nCh * P.nS : P.rf[0];
+            tb[f] = P.rf[f < nf ? f : 0] + static_cast<size_t>(s.txIdx) * P.nCh * P.nS;
         const int nD = static_cast<int>(P.nD);
         const int rStart = max(0, static_cast<int>(pi.seg0) - a.half);
         const int rEnd = min(nD, static_cast<int>(pi.seg1) + a.half + 1);

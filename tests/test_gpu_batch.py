@@ -17,14 +17,14 @@ def small_batch():
     return geoms, plans, probe, rfs
 
 
-@pytest.mark.parametrize("shape", [(1, 256, 1), (1, 384, 1), (2, 128, 1), (4, 256, 4), (4, 256, 8), (6, 128, 8),
-                                   (3, 128, 2)])
+@pytest.mark.parametrize("shape", [(1, 256, 1, 0), (1, 384, 1, 0), (2, 128, 1, 0), (4, 256, 4, 0), (4, 256, 8, 0),
+                                   (6, 128, 8, 0), (3, 128, 2, 0), (1, 128, 4, 1), (1, 128, 2, 1), (2, 128, 2, 1)])
 @pytest.mark.parametrize("use_graph", [False, True])
 def test_batch_rf_matches_per_frame(small_batch, shape, use_graph):
     from supra_b200.api import BatchedDasIq
     geoms, plans, probe, rfs = small_batch
     b = BatchedDasIq([(plans[p], rf) for p, rf in zip(probe, rfs)], ctas_per_sm=shape[0], depth_tile=shape[1],
-                     frames_per_pack=shape[2])
+                     frames_per_pack=shape[2], staged=shape[3])
     b.enable_rf_outputs()
     b.run(use_graph=use_graph)
     b.run(use_graph=use_graph)  # a second replay must give the same result
@@ -62,10 +62,10 @@ def test_batch_autotune_and_cache(small_batch, tmp_path):
     geoms, plans, probe, rfs = small_batch
     b = BatchedDasIq([(plans[p], rf) for p, rf in zip(probe, rfs)])
     cache = str(tmp_path / "tune.txt")
-    c, t, f = b.autotune(cache)
-    assert 1 <= c <= 8 and t in (128, 256, 384, 512) and f in (1, 2, 4, 8)
+    c, t, f, g = b.autotune(cache)
+    assert 1 <= c <= 12 and t in (128, 256, 384, 512) and f in (1, 2, 4, 8) and g in (0, 1)
     b2 = BatchedDasIq([(plans[p], rf) for p, rf in zip(probe, rfs)])
-    assert b2.autotune(cache) == (c, t, f)
+    assert b2.autotune(cache) == (c, t, f, g)
     b2.run()
     torch.cuda.synchronize()
 
