@@ -758,9 +758,10 @@ extern "C" int sb_das_run_static(const sb_geometry* g, const void* rf, int rf_dt
 //   dtau_e/dc           = -(dist_e + depth) / c   (DT-space path length; the initial delay is in
 //                         samples and the aperture and window are ratios, both independent of c)
 // A prologue pass recomputes D and n per pixel (the aperture is recomputed, not stored) and forms
-// G = g n / D and H = g s / D. The main pass gives one warp each (scanline, element) pair; its
-// lanes walk the depths, so the sample indices a warp touches are nearly consecutive: the channel
-// row is accumulated in shared memory and flushed to HBM once, with coalesced reductions.
+// G = g n / D and H = g s / D, with the pixel's aperture and window scale. The main pass gives one
+// warp each (scanline, element) pair; its lanes walk the depths in order, so the channel samples it
+// touches advance with the delays: they are accumulated in a small ring in shared memory and
+// written to HBM once, in order, as they become final.
 namespace sb {
 namespace {
 
@@ -768,7 +769,7 @@ struct AdjArgs {
     DasArgs a;
     const float* fwd;      // [frames][nD][nRx] forward output
     const float* gout;     // [frames][nD][nRx]
-    float2* gh;            // [frames][nRx][nD] scratch: (G, H)
+    float4* gh;            // [frames][nRx][nD] scratch: (G, H, aperture aDT, 1 / min(aDT, maxDist))
     float* gradRf;         // [frames][nTx][nCh][nS] or null
     float* gradApod;       // [nE] or null
     float* gradC;          // [1] or null
@@ -786,11 +787,13 @@ __global__ void __launch_bounds__(256) adjPixelKernel(AdjArgs p) {
     if (r >= a.nD) return;
     const LineDT s = a.lines[line];
     const int k = s.highest;
-    float2 gh = make_float2(0.0f, 0.0f);
+    float4 gh = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if ((s.activeMask >> k) & 1) {
         const float d = __ldg(a.depth + r);
         const float aDT = apertureDT(d, a.dt, a.c, a.F);
         const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+        gh.z = aDT;
+        gh.w = invMax;
         float D = 0.0f;
         int n = 0;
         for (int e = s.firstX[k]; e < s.lastX[k]; e++) {
@@ -818,8 +821,14 @@ __global__ void __launch_bounds__(256) adjPixelKernel(AdjArgs p) {
 }
 
 // blockIdx.x: group of warps over the aperture elements of scanline blockIdx.y, frame blockIdx.z.
+// A warp walks the depths of its (scanline, element) in chunks of 32. Delays grow with depth, so the
+// channel samples a chunk touches lie just ahead of those already final: the warp accumulates them
+// in a ring of kAdjRing floats in shared memory and, after each chunk, writes out every sample below
+// the next chunk's first delay (whole rows in order, zeros included, when rows are exclusive).
+constexpr int kAdjRing = 128;
+
 __global__ void __launch_bounds__(256) adjElemKernel(AdjArgs p) {
-    extern __shared__ __align__(16) float rowsAll[];
+    __shared__ float ringAll[8][kAdjRing];
     __shared__ float lut[64];
     const DasArgs& a = p.a;
     if (threadIdx.x < 64) lut[threadIdx.x] = a.lut.v[threadIdx.x];
@@ -844,10 +853,9 @@ __global__ void __launch_bounds__(256) adjElemKernel(AdjArgs p) {
     }
     const int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(static_cast<uint32_t>(e) % a.nCh);
     if (ch < 0) return;
-    float* row = rowsAll + static_cast<size_t>(warp) * a.nS;
+    float* ring = ringAll[warp];
     const bool wantRf = p.gradRf != nullptr;
-    if (wantRf)
-        for (uint32_t t = lane; t < a.nS; t += 32) row[t] = 0.0f;
+    for (int i = lane; i < kAdjRing; i += 32) ring[i] = 0.0f;
     __syncwarp();
     const float xel = __ldg(a.xe + e);
     const float dx = __fsub_rn(xel, s.x);
@@ -855,72 +863,93 @@ __global__ void __launch_bounds__(256) adjElemKernel(AdjArgs p) {
     const float iD = s.initialDelay[k];
     const float* rf = static_cast<const float*>(a.rf) + static_cast<size_t>(frame) * p.rfFrameStride +
                       (static_cast<size_t>(s.txIdx[k]) * a.nCh + ch) * a.nS;
-    const float2* gh = p.gh + (static_cast<size_t>(frame) * a.nRx + line) * a.nD;
+    float* dst = wantRf ? p.gradRf + static_cast<size_t>(frame) * p.rfFrameStride +
+                              (static_cast<size_t>(s.txIdx[k]) * a.nCh + ch) * a.nS
+                        : nullptr;
+    const float4* gh = p.gh + (static_cast<size_t>(frame) * a.nRx + line) * a.nD;
+    const int nS = static_cast<int>(a.nS);
     float gA = 0.0f, gC = 0.0f;
-    int tMin = INT_MAX, tMax = -1;
-    for (uint32_t r = lane; r < a.nD; r += 32) {
-        const float d = __ldg(a.depth + r);
-        const float aDT = apertureDT(d, a.dt, a.c, a.F);
-        if (!(fabsf(dx) <= aDT)) continue;
-        const float2 GH = gh[r];
-        if (GH.x == 0.0f && GH.y == 0.0f) continue;
-        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
-        const float w = lutGet(lut, __fmul_rn(dx, invMax));
-        const float W = __fmul_rn(w, apodE);
-        const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
-        const float dy = __fmul_rn(s.dirY, d);
-        const float ex = __fsub_rn(xel, xz);
-        const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(dy, dy)));
-        const float path = __fadd_rn(dist, d);
-        const float delayf = __fadd_rn(__fadd_rn(iD, path), a.offset);
-        const int32_t delay = static_cast<int32_t>(floorf(delayf));
-        const float frac = __fsub_rn(delayf, static_cast<float>(delay));
-        float v = 0.0f;
-        const float GW = GH.x * W;
-        if (static_cast<uint32_t>(delay) < a.nS - 1) {
-            const float v0 = __ldg(rf + delay), v1 = __ldg(rf + delay + 1);
-            v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
-            gC += GW * (v1 - v0) * path;
-            if (wantRf) {
-                atomicAdd(&row[delay], GW * (1.0f - frac));
-                atomicAdd(&row[delay + 1], GW * frac);
-                tMin = min(tMin, delay);
-                tMax = max(tMax, delay + 1);
-            }
-        } else if (static_cast<uint32_t>(delay) < a.nS && frac == 0.0f) {
-            v = __ldg(rf + delay);
-            if (wantRf) {
-                atomicAdd(&row[delay], GW);
-                tMin = min(tMin, delay);
-                tMax = max(tMax, delay);
+    int flushed = 0;  // samples below `flushed` are final and written out
+    // contribution c to sample t: into the ring while it is within reach, else directly to HBM
+    auto add = [&](int t, float c) {
+        if (t >= flushed && t < flushed + kAdjRing) atomicAdd(&ring[t & (kAdjRing - 1)], c);
+        else atomicAdd(dst + t, c);
+    };
+    // writes samples [flushed, upTo) from the ring (all of them, zeros included, when rows are exclusive)
+    auto flush = [&](int upTo) {
+        upTo = min(upTo, nS);
+        if (upTo <= flushed) return;
+        __syncwarp();
+        for (int t = flushed + lane; t < upTo; t += 32) {
+            float* rs = &ring[t & (kAdjRing - 1)];
+            const float v = *rs;
+            *rs = 0.0f;
+            if (p.exclusiveRows) dst[t] = v;
+            else if (v != 0.0f) atomicAdd(dst + t, v);
+        }
+        __syncwarp();
+        flushed = upTo;
+    };
+    for (uint32_t r0 = 0; r0 < a.nD; r0 += 32) {
+        const uint32_t r = r0 + lane;
+        if (r < a.nD) {
+            const float4 GH = gh[r];  // per-pixel factors and the aperture, from the prologue
+            const float aDT = GH.z;
+            if (fabsf(dx) <= aDT && (GH.x != 0.0f || GH.y != 0.0f)) {
+                const float d = __ldg(a.depth + r);
+                const float w = lutGet(lut, __fmul_rn(dx, GH.w));
+                const float W = __fmul_rn(w, apodE);
+                const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
+                const float dy = __fmul_rn(s.dirY, d);
+                const float ex = __fsub_rn(xel, xz);
+                const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(dy, dy)));
+                const float path = __fadd_rn(dist, d);
+                const float delayf = __fadd_rn(__fadd_rn(iD, path), a.offset);
+                const int32_t delay = static_cast<int32_t>(floorf(delayf));
+                const float frac = __fsub_rn(delayf, static_cast<float>(delay));
+                float v = 0.0f;
+                const float GW = GH.x * W;
+                if (static_cast<uint32_t>(delay) < a.nS - 1) {
+                    const float v0 = __ldg(rf + delay), v1 = __ldg(rf + delay + 1);
+                    v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
+                    gC += GW * (v1 - v0) * path;
+                    if (wantRf) {
+                        add(delay, GW * (1.0f - frac));
+                        add(delay + 1, GW * frac);
+                    }
+                } else if (static_cast<uint32_t>(delay) < a.nS && frac == 0.0f) {
+                    v = __ldg(rf + delay);
+                    if (wantRf) add(delay, GW);
+                }
+                gA += w * (GH.x * v - GH.y);
             }
         }
-        gA += w * (GH.x * v - GH.y);
+        if (wantRf) {
+            // the next chunk's delays start at its first depth's delay (less one sample of slack for
+            // float rounding): everything below is final
+            int safe = nS;
+            const uint32_t rn = r0 + 32;
+            if (rn < a.nD) {
+                const float d = __ldg(a.depth + rn);
+                const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
+                const float dy = __fmul_rn(s.dirY, d);
+                const float ex = __fsub_rn(xel, xz);
+                const float t = __fadd_rn(__fadd_rn(iD, __fadd_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(dy, dy))), d)),
+                                          a.offset);
+                safe = t > -1e9f ? static_cast<int>(floorf(fminf(t, 1e9f))) - 2 : 0;
+            }
+            flush(safe);
+        }
     }
+    if (wantRf) flush(nS);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         gA += __shfl_xor_sync(0xffffffffu, gA, o);
         gC += __shfl_xor_sync(0xffffffffu, gC, o);
-        tMin = min(tMin, __shfl_xor_sync(0xffffffffu, tMin, o));
-        tMax = max(tMax, __shfl_xor_sync(0xffffffffu, tMax, o));
     }
     if (lane == 0) {
         if (p.gradApod) atomicAdd(p.gradApod + e, gA);
         if (p.gradC) atomicAdd(p.gradC, -gC / a.c);
-    }
-    __syncwarp();
-    if (!wantRf) return;
-    float* dst = p.gradRf + static_cast<size_t>(frame) * p.rfFrameStride +
-                 (static_cast<size_t>(s.txIdx[k]) * a.nCh + ch) * a.nS;
-    if (p.exclusiveRows) {
-        // the row is this warp's alone: store all of it (zeros included), no memset needed
-        for (uint32_t t = lane; t < a.nS; t += 32) dst[t] = row[t];
-    } else if (tMax >= 0) {
-        // scanlines may share a transmit and elements a channel: reductions into the zeroed output
-        for (int t = tMin + lane; t <= tMax; t += 32) {
-            const float v = row[t];
-            if (v != 0.0f) atomicAdd(dst + t, v);
-        }
     }
 }
 
@@ -996,12 +1025,8 @@ int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, 
     cudaStream_t st = S(stream);
     const size_t rfStride = static_cast<size_t>(p->numTx) * p->numChannels * p->numSamples;
     const size_t outStride = static_cast<size_t>(p->numDepths) * p->numRx;
-    const size_t rowBytes = static_cast<size_t>(p->numSamples) * sizeof(float);
-    const int warps = static_cast<int>(std::min<size_t>(8, (200 * 1024) / rowBytes));
-    if (grad_rf && warps < 1)
-        return fail(SB_ERR_UNSUPPORTED, "sb_das_adjoint: %u samples per channel exceed the shared-memory row", p->numSamples);
     // scratch: the forward output when not given, and the per-pixel (G, H)
-    const size_t ghBytes = static_cast<size_t>(num_frames) * outStride * sizeof(float2);
+    const size_t ghBytes = static_cast<size_t>(num_frames) * outStride * sizeof(float4);
     const size_t fwdBytes = forward_out ? 0 : static_cast<size_t>(num_frames) * outStride * sizeof(float);
     if (p->adjScratchBytes < ghBytes + fwdBytes) {
         // growing the cached scratch synchronises once (cudaFree); later calls reuse it
@@ -1012,7 +1037,7 @@ int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, 
         p->adjScratchBytes = ghBytes + fwdBytes;
     }
     void* scratch = p->adjScratch;
-    float2* gh = static_cast<float2*>(scratch);
+    float4* gh = static_cast<float4*>(scratch);
     const float* fwd = forward_out;
     int rc = SB_OK;
     if (!fwd) {
@@ -1062,19 +1087,13 @@ int sb_das_adjoint(const sb_das_plan* plan, const float* rf, const float* apod, 
         q.outFrameStride = outStride;
         q.exclusiveRows = exclusive ? 1 : 0;
         adjPixelKernel<<<dim3((p->numDepths + 255) / 256, p->numRx, num_frames), 256, 0, st>>>(q);
-        const int w = std::max(warps, 1);
-        const size_t shm = grad_rf ? static_cast<size_t>(w) * rowBytes : 0;
-        if (cudaFuncSetAttribute(adjElemKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shm)) !=
-            cudaSuccess)
-            rc = cudaFail(cudaGetLastError(), "cudaFuncSetAttribute");
-        else {
-            const uint32_t slots = exclusive && grad_rf ? std::max<uint32_t>(p->maxApertureX, p->numChannels)
-                                                        : static_cast<uint32_t>(std::max(p->maxApertureX, 1));
-            const uint32_t groups = (slots + w - 1) / w;
-            adjElemKernel<<<dim3(groups, p->numRx, num_frames), 32 * w, shm, st>>>(q);
-            cudaError_t le = cudaGetLastError();
-            if (le != cudaSuccess) rc = cudaFail(le, "adjElemKernel");
-        }
+        const int w = 8;
+        const uint32_t slots = exclusive && grad_rf ? std::max<uint32_t>(p->maxApertureX, p->numChannels)
+                                                    : static_cast<uint32_t>(std::max(p->maxApertureX, 1));
+        const uint32_t groups = (slots + w - 1) / w;
+        adjElemKernel<<<dim3(groups, p->numRx, num_frames), 32 * w, 0, st>>>(q);
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) rc = cudaFail(le, "adjElemKernel");
     }
     return rc;
 }
