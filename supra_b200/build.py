@@ -65,5 +65,30 @@ def build(verbose: bool = False) -> str:
     return LIB
 
 
+TORCH_EXT_SRC = os.path.join(HERE, "torch_ext", "autograd_ops.cpp")
+TORCH_EXT = os.path.join(LIBDIR, "supra_b200_torch_ops.so")
+
+
+def build_torch_ops() -> str:
+    """Builds the libtorch autograd operators (torch.ops.supra_b200.*) in-tree, linked to the library
+    by rpath. Needs torch's C++ headers; no device code, so it builds without a GPU."""
+    import torch.utils.cpp_extension as ext
+
+    lib = build()
+    if os.path.exists(TORCH_EXT) and os.path.getmtime(TORCH_EXT) >= max(os.path.getmtime(TORCH_EXT_SRC),
+                                                                         os.path.getmtime(lib)):
+        return TORCH_EXT
+    bdir = os.path.join(BUILD, "torch_ops")
+    os.makedirs(bdir, exist_ok=True)
+    ext.load(name="supra_b200_torch_ops", sources=[TORCH_EXT_SRC], build_directory=bdir, with_cuda=True,
+             extra_include_paths=[os.path.join(REPO, "include")],
+             extra_ldflags=[f"-L{LIBDIR}", "-lsupra_b200", f"-Wl,-rpath,{LIBDIR}", "-Wl,-rpath,$ORIGIN"],
+             is_python_module=False, verbose=False)
+    shutil.copy2(os.path.join(bdir, "supra_b200_torch_ops.so"), TORCH_EXT)
+    return TORCH_EXT
+
+
 if __name__ == "__main__":
     print(build(verbose="--verbose" in sys.argv))
+    if "--torch-ops" in sys.argv:
+        print(build_torch_ops())

@@ -191,3 +191,31 @@ def test_autograd_envelope_loss(oracle, case):
         tot_c += gc
     assert np.max(np.abs(ap.grad.cpu().numpy() - tot_ap)) <= 1e-3 * np.max(np.abs(tot_ap))
     assert abs(float(c.grad) - tot_c) <= 1e-3 * abs(tot_c)
+
+
+def test_libtorch_function_matches_python_function(case):
+    """torch.ops.supra_b200.das_apod / envelope (libtorch autograd Functions) and the Python
+    torch.autograd.Functions run the same kernels: identical loss and channel-data gradient; the
+    apodisation and speed-of-sound gradients are sums of float atomics across warps (order not
+    fixed), equal to 1e-5 relative."""
+    from supra_b200.api import HilbertFirEnvelope
+    from supra_b200.autograd import das_apod, das_apod_py, envelope, envelope_py
+    g, rf, apod, _ = case
+    bf, rf_d, ap_d, _ = _gpu(case)
+    hil = HilbertFirEnvelope(32)
+    target = torch.rand((2, g.num_depths, g.num_rx), device="cuda") * 0.1
+    res = []
+    for das_fn, env_fn in ((das_apod, envelope), (das_apod_py, envelope_py)):
+        rf2 = torch.stack([rf_d, 0.5 * rf_d.flip(-1)]).contiguous().requires_grad_(True)
+        ap = ap_d.clone().requires_grad_(True)
+        c = torch.tensor(g.speed_of_sound_mm_s, dtype=torch.float64, device="cuda", requires_grad=True)
+        s = das_fn(bf, rf2, ap, c)
+        s = torch.where(s.detach().abs() < 1e30, s, torch.zeros_like(s))
+        loss = ((env_fn(s, hil) - target) ** 2).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+        res.append((loss.detach(), rf2.grad, ap.grad, c.grad))
+    (l0, r0, a0, c0), (l1, r1, a1, c1) = res
+    assert torch.equal(l0, l1) and torch.equal(r0, r1)
+    assert torch.max(torch.abs(a0 - a1)) <= 1e-5 * torch.max(torch.abs(a1))
+    assert abs(float(c0) - float(c1)) <= 1e-5 * abs(float(c1))

@@ -83,3 +83,11 @@ def test_bad_transmit_index_rejected():
     plan = C.c_void_p()
     assert lib.sb_das_plan_create(C.byref(g), C.byref(plan)) == abi.SB_ERR_INVALID_ARG
     assert b"transmit index" in lib.sb_last_error()
+
+
+def test_libtorch_autograd_operators_load():
+    """The libtorch autograd Functions (torch.ops.supra_b200.*) load and register without a GPU."""
+    import torch
+    from supra_b200.autograd import load_torch_ops
+    load_torch_ops()
+    assert hasattr(torch.ops.supra_b200, "das_apod") and hasattr(torch.ops.supra_b200, "envelope")
