@@ -206,6 +206,124 @@ __global__ void __launch_bounds__(256) dasKernel(DasArgs a) {
     static_cast<OUT*>(a.out)[line + static_cast<size_t>(r) * a.nRx] = clampCast<OUT>(acc);
 }
 
+// 3D delay-and-sum with a per-scanline element table in shared memory (highest-weight transmit).
+// The table keeps the reference's summation order (x outer, y inner, RxSampleBeamformerDelayAndSum.h:
+// 55-57), each element's position, offsets from the scanline and channel. Once the aperture covers
+// maxElementDistance in both directions and every element of the table (depths where
+// sqrt(aDT^2) >= maxDistX, maxDistY and aDT^2 >= max(dx^2 + dz^2)), the window weights no longer
+// depend on depth: they and their running sum are computed once per scanline in the same order, so
+// results stay bit-identical to sample3D.
+struct __align__(16) Elem3D {
+    float xel, zel, dx, dz;
+    float wDeep;
+    int ch;
+    float r2;
+    int pad;
+};
+constexpr int kMax3DElems = 1024;
+
+template <typename RF, typename OUT>
+__global__ void __launch_bounds__(256) das3dTableKernel(DasArgs a) {
+    __shared__ float lut[64];
+    __shared__ Elem3D el[kMax3DElems];
+    __shared__ int nEl;
+    __shared__ float sumDeep, maxR2;
+    const int tid = threadIdx.x;
+    if (tid < 64) lut[tid] = a.lut.v[tid];
+    __syncthreads();
+    const uint32_t line = blockIdx.y;
+    const LineDT s = a.lines[line];
+    const int k = s.highest;
+    const bool active = (s.activeMask >> k) & 1;
+    const int nx = active ? max(static_cast<int>(s.lastX[k]) - static_cast<int>(s.firstX[k]), 0) : 0;
+    const int ny = active ? max(static_cast<int>(s.lastY[k]) - static_cast<int>(s.firstY[k]), 0) : 0;
+    const int n0 = min(nx * ny, kMax3DElems);  // the host routes larger apertures to the generic kernel
+    const float invXd = __fdiv_rn(1.0f, s.maxDistX), invYd = __fdiv_rn(1.0f, s.maxDistY);
+    for (int j = tid; j < n0; j += 256) {
+        const uint32_t ex = s.firstX[k] + j / ny, ey = s.firstY[k] + j % ny;
+        const uint32_t e = ex + ey * a.layoutX;
+        Elem3D r;
+        r.ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(e % a.nCh);
+        r.xel = __ldg(a.xe + e);
+        r.zel = __ldg(a.ye + e);
+        r.dx = __fsub_rn(r.xel, s.x);
+        r.dz = __fsub_rn(r.zel, s.z);
+        r.r2 = __fadd_rn(__fmul_rn(r.dx, r.dx), __fmul_rn(r.dz, r.dz));
+        r.wDeep = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(r.dx, invXd)), lutGet(lut, __fmul_rn(r.dz, invYd))));
+        r.pad = 0;
+        el[j] = r;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int m = 0;
+        float sum = 0.0f, mr = 0.0f;
+        for (int j = 0; j < n0; j++) {
+            const Elem3D r = el[j];
+            if (r.ch < 0) continue;
+            el[m++] = r;
+            sum = __fadd_rn(sum, r.wDeep);
+            mr = fmaxf(mr, r.r2);
+        }
+        nEl = m;
+        sumDeep = sum;
+        maxR2 = mr;
+    }
+    __syncthreads();
+    const uint32_t r = blockIdx.x * blockDim.x + tid;
+    if (r >= a.nD) return;
+    float acc = 0.0f;
+    if (active) {
+        const float d = __ldg(a.depth + r);
+        const float aDT = apertureDT(d, a.dt, a.c, a.F);
+        const float aDT2 = __fmul_rn(aDT, aDT);
+        const float sq = __fsqrt_rn(aDT2);
+        const float invX = __fdiv_rn(1.0f, fminf(sq, s.maxDistX));
+        const float invY = __fdiv_rn(1.0f, fminf(sq, s.maxDistY));
+        const bool deep = sq >= s.maxDistX && sq >= s.maxDistY && aDT2 >= maxR2;
+        const float iD = s.initialDelay[k];
+        const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
+        const float px = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
+        const float pz = __fadd_rn(s.z, __fmul_rn(s.dirZ, d));
+        const float ay = __fmul_rn(s.dirY, d);
+        const float ay2 = __fmul_rn(ay, ay);
+        const int n = nEl;
+        float sample = 0.0f, weightAcum = 0.0f;
+        int numAdds = 0;
+        for (int j = 0; j < n; j++) {
+            const Elem3D e = el[j];
+            float w;
+            if (deep) {
+                w = e.wDeep;
+            } else {
+                if (!(e.r2 <= aDT2)) continue;
+                w = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(e.dx, invX)), lutGet(lut, __fmul_rn(e.dz, invY))));
+                weightAcum = __fadd_rn(weightAcum, w);
+                numAdds++;
+            }
+            const float qx = __fsub_rn(e.xel, px), qz = __fsub_rn(e.zel, pz);
+            const float q = __fadd_rn(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qz, qz)), ay2);
+            const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(__fsqrt_rn(q), d)), a.offset);
+            const uint32_t delay = static_cast<uint32_t>(floorf(delayf));  // saturates at 0 like the reference
+            const float frac = __fsub_rn(delayf, static_cast<float>(delay));
+            const RF* p = tx + static_cast<size_t>(e.ch) * a.nS;
+            if (delay < a.nS - 1) {
+                const float v0 = toFloat(__ldg(p + delay)), v1 = toFloat(__ldg(p + delay + 1));
+                const float v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
+                sample = __fadd_rn(sample, __fmul_rn(w, v));
+            } else if (delay < a.nS && frac == 0.0f) {
+                sample = __fadd_rn(sample, __fmul_rn(w, toFloat(__ldg(p + delay))));
+            }
+        }
+        if (deep) {
+            weightAcum = sumDeep;
+            numAdds = n;
+        }
+        const float v = numAdds > 0 ? __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds)) : 0.0f;
+        acc = __fadd_rn(acc, v);
+    }
+    static_cast<OUT*>(a.out)[line + static_cast<size_t>(r) * a.nRx] = clampCast<OUT>(acc);
+}
+
 // RawDelay (Beamformer/RawDelay.cu:221-312 with the kernel :406-468): highest-weight transmit only,
 // out [line][local element][depth], normalised by numAdds / sum(w); unused slots written as 0.
 template <typename RF, typename OUT>
@@ -530,9 +648,12 @@ int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out,
                         stagedMaxW(p->numChannels, rfSize) >= 64;
     if (staged) return launchStaged(p, a, rf_dtype, out_dtype, st);
     dim3 grid((p->numDepths + 255) / 256, p->numRx);
+    const bool table3D = p->is3D && !interpolate_transmits &&
+                         static_cast<int64_t>(p->maxApertureX) * p->maxApertureY <= kMax3DElems;
 #define SB_DAS_LAUNCH(RFT, OUTT)                                                        \
     do {                                                                                \
-        if (p->is3D) dasKernel<RFT, OUTT, true><<<grid, 256, 0, st>>>(a);              \
+        if (table3D) das3dTableKernel<RFT, OUTT><<<grid, 256, 0, st>>>(a);             \
+        else if (p->is3D) dasKernel<RFT, OUTT, true><<<grid, 256, 0, st>>>(a);         \
         else dasKernel<RFT, OUTT, false><<<grid, 256, 0, st>>>(a);                     \
     } while (0)
     if (rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_DAS_LAUNCH(int16_t, float);
