@@ -28,10 +28,10 @@ METRIC = "beamformed px/s"
 UNIT = "px/s"
 WORKLOAD = ("c1 batched DAS+IQ: 64 frames/launch (22x P64/1024 smp, 21x P128/2048, 21x P192/3072), 0.3 mm, "
             "fs 40 MHz, 64-ch aperture, F#1 Hann, int16 in; IQ 5 MHz mix, 32-tap LPF, /4, complex64 out")
-# DRAM bytes per beamformed pixel of batchPackKernel measured by ncu on a 6-frame case of this workload
-# ((dram__bytes_read.sum + dram__bytes_write.sum) / pixels = 193.2 MB / 1,835,008 px), scaled by pixels;
-# profiles/batchPackKernel_c1_6frames_full.md has the capture.
-TRAFFIC_BYTES_PER_PX = 105.3
+# DRAM bytes per beamformed pixel of batchPackKernel measured by ncu on a 24-frame case of this workload
+# ((dram__bytes_read.sum + dram__bytes_write.sum) / pixels = 917.2 MB / 7,249,920 px), scaled by pixels;
+# profiles/batchPackKernel_c1_24frames_full.md has the capture.
+TRAFFIC_BYTES_PER_PX = 126.5
 
 
 def peaks():
@@ -213,15 +213,20 @@ def profile_case(case: str):
     from supra_b200.api import BatchedDasIq, RxBeamformer, mv_beamform
     from supra_b200.workloads import c1_workload
     if case == "batch":
-        wl = c1_workload(num_frames=12, device="cuda")  # packs of 4 frames are full
+        wl = c1_workload(num_frames=24, device="cuda")  # packs of 8 frames are full
         plans = [RxBeamformer(g) for g in wl.geometries]
-        b = BatchedDasIq([(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)], ctas_per_sm=8, depth_tile=128,
-                         frames_per_pack=4)
+        b = BatchedDasIq([(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)], ctas_per_sm=4, depth_tile=256,
+                         frames_per_pack=8)
         for _ in range(2):
             b.run(use_graph=False)
     elif case == "mv":
         x = torch.randn((16, 128, 2048), dtype=torch.complex64, device="cuda")
         mv_beamform(x, 32, 5, 1.5, False, 0.01, 1e6)
+    elif case == "das3d":
+        from supra_b200 import workloads as W
+        g2 = W.c2_geometry()
+        rf2 = W.c2_volume(g2)
+        RxBeamformer(g2).beamform(rf2, 1.0, window_type=1)
     elif case == "adjoint":
         from supra_b200 import workloads as W
         g4, rf4 = W.c4_batch(frames=2)
@@ -243,7 +248,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements (c0, c2, c3, c4)")
     ap.add_argument("--frames", type=int, default=64, help="frames per launch (64 = the named workload)")
-    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint"], help="run one small case for ncu and exit")
+    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d"],
+                    help="run one small case for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:
         import torch
