@@ -275,7 +275,7 @@ int buildPacks(sb_batch_plan* p, int fp) {
         }
     }
     const int dec = p->args.dec;
-    const uint32_t seg = static_cast<uint32_t>(1024 - (1024 % dec));
+    const uint32_t seg = static_cast<uint32_t>(kPackSeg - (kPackSeg % dec));
     std::vector<PackItem> items;
     for (uint32_t k = 0; k < packs.size(); k++)
         for (uint32_t l = 0; l < packs[k].nRx; l++)

@@ -9,12 +9,13 @@
 // gather and four flops. Channel samples are read through L1/L2 (each transmit's rows are used by
 // exactly one scanline, so they cross HBM once).
 //
-// Depth segments of SEG depths (multiple of the decimation) are beamformed with a halo of `half`
-// depths on both sides so that the low-pass of the IQ stage sees all its taps; the beamformed
-// depths go to a two-block ring in shared memory and the IQ outputs whose taps are complete are
-// written after each block. The aperture test, window-LUT entry and sample index are the reference's
-// bit for bit; the per-frame accumulation is contracted into FMAs (w(1-f) and w f computed once per
-// element), so sums differ from the per-frame kernel by float rounding only (~1e-7 relative).
+// Depth segments of kPackSeg depths (multiple of the decimation) are beamformed with a halo of `half`
+// depths on both sides so that the low-pass of the IQ stage sees all its taps; the beamformed depths
+// of the whole item stay in shared memory and the IQ outputs are computed once the item is complete,
+// so the CTA meets one barrier per item instead of two per depth block. The aperture test,
+// window-LUT entry and sample index are the reference's bit for bit; the per-frame accumulation is
+// contracted into FMAs (w(1-f) and w f computed once per element), so sums differ from the per-frame
+// kernel by float rounding only (~1e-7 relative).
 #pragma once
 
 #include "das_core.cuh"
@@ -23,6 +24,8 @@
 namespace sb {
 
 constexpr int kMaxPack = 8;
+constexpr int kPackSeg = 1024;                         // depths per work item (multiple of the decimation below)
+constexpr int kPackSegMax = kPackSeg + kIqMaxTaps + 2;  // + the low-pass halo on both sides
 
 struct PackDev {
     const LineDT* lines;
@@ -181,7 +184,7 @@ template <int FP, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
     __shared__ ElemRec el[kMaxApertureElems];
     __shared__ float lut[64];
-    __shared__ float ring[2][FP][NT];
+    __shared__ float seg[FP][kPackSegMax];  // the item's beamformed depths (segment + low-pass halo)
     __shared__ uint32_t itemIdx;
     __shared__ int nEl, cntDeep, deepOk;
     __shared__ float sumDeep;
@@ -245,10 +248,8 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         const int so0 = static_cast<int>(pi.seg0) / a.dec;
         const int so1 = min(static_cast<int>(pi.seg1) / a.dec, nD / a.dec);
         const int nBlocks = (rEnd - rStart + NT - 1) / NT;
-        int soNext = so0;
         for (int k = 0; k < nBlocks; k++) {
             const int r = rStart + k * NT + tid;
-            const int slot = k & 1;
             PackAcc<FP> acc;
 #pragma unroll
             for (int f = 0; f < FP; f++) acc.v[f] = 0.0f;
@@ -274,37 +275,35 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
                     acc.v[f] = clampCast<float>(v);
                 }
             }
+            if (r < rEnd) {
 #pragma unroll
-            for (int f = 0; f < FP; f++) {
-                ring[slot][f][tid] = acc.v[f];
-                if (f < nf && r < rEnd && r >= static_cast<int>(pi.seg0) && r < static_cast<int>(pi.seg1) && P.rfOut[f])
-                    P.rfOut[f][pi.line + static_cast<size_t>(r) * P.nRx] = acc.v[f];
-            }
-            __syncthreads();
-            // outputs whose last tap lies in this block (all remaining ones after the last block)
-            const int blockLast = rStart + (k + 1) * NT - 1;
-            const int soEnd = (k + 1 == nBlocks) ? so1 : min(so1, floorDiv(blockLast - a.half, a.dec) + 1);
-            const int cntOut = max(0, soEnd - soNext) * nf;
-            for (int idx = tid; idx < cntOut; idx += NT) {
-                const int so = soNext + idx / nf;
-                const int f = idx % nf;
-                float re = 0.0f, im = 0.0f;
-                const int base = so * a.dec - a.half;
-                for (int j = 0; j < a.taps; j++) {
-                    const int nn = base + j;
-                    if (nn >= 0 && nn < nD) {
-                        const int rel = nn - rStart;
-                        const float x = ring[(rel / NT) & 1][f][rel % NT] * a.lp[j];
-                        const float2 w = __ldg(a.rot + nn);
-                        re = fmaf(x, w.x, re);
-                        im = fmaf(x, w.y, im);
-                    }
+                for (int f = 0; f < FP; f++) {
+                    seg[f][r - rStart] = acc.v[f];
+                    if (f < nf && r >= static_cast<int>(pi.seg0) && r < static_cast<int>(pi.seg1) && P.rfOut[f])
+                        P.rfOut[f][pi.line + static_cast<size_t>(r) * P.nRx] = acc.v[f];
                 }
-                P.iq[f][pi.line + static_cast<size_t>(so) * P.nRx] = make_float2(re, im);
             }
-            soNext = max(soNext, soEnd);
-            __syncthreads();
         }
+        // one barrier per item: the segment's RF is complete; its IQ outputs [so0, so1) for every frame
+        __syncthreads();
+        const int cntOut = max(0, so1 - so0) * nf;
+        for (int idx = tid; idx < cntOut; idx += NT) {
+            const int so = so0 + idx / nf;
+            const int f = idx % nf;
+            float re = 0.0f, im = 0.0f;
+            const int base = so * a.dec - a.half;
+            for (int j = 0; j < a.taps; j++) {
+                const int nn = base + j;
+                if (nn >= 0 && nn < nD) {
+                    const float x = seg[f][nn - rStart] * a.lp[j];
+                    const float2 w = __ldg(a.rot + nn);
+                    re = fmaf(x, w.x, re);
+                    im = fmaf(x, w.y, im);
+                }
+            }
+            P.iq[f][pi.line + static_cast<size_t>(so) * P.nRx] = make_float2(re, im);
+        }
+        // the next item's first barrier orders these reads of seg before its writes
     }
 }
 
