@@ -608,8 +608,9 @@ int sb_batch_autotune(sb_batch_plan* p, const char* cache_path, int32_t* ctas_pe
         }
     }
     // {ctas per SM, depth tile, frames per pack, staged}
-    const int shapes[][4] = {{1, 384, 1, 0},  {4, 256, 4, 0},  {5, 256, 4, 0}, {6, 256, 4, 0}, {12, 128, 4, 0},
-                             {4, 256, 8, 0},  {5, 256, 8, 0},  {1, 128, 4, 1}, {1, 128, 2, 1}, {2, 128, 2, 1}};
+    const int shapes[][4] = {{1, 384, 1, 0}, {4, 256, 4, 0}, {5, 256, 4, 0}, {6, 256, 4, 0}, {8, 128, 4, 0},
+                             {12, 128, 4, 0}, {4, 256, 8, 0}, {5, 256, 8, 0}, {8, 128, 8, 0}, {1, 128, 4, 1},
+                             {1, 128, 2, 1},  {2, 128, 2, 1}};
     float best = 1e30f;
     int bestC = p->ctasPerSm, bestT = p->nt, bestF = p->fp, bestG = p->staged;
     cudaEvent_t e0, e1;

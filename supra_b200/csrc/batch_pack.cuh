@@ -120,13 +120,16 @@ __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float*
     }
 }
 
-// Deep depths (every element active, weights precomputed): the same sum as packDepth<FP, true, .>,
-// software-pipelined so that the gathers of element j+1 are in flight while element j is accumulated
-// and element j+2's geometry is computed.
-template <int FP, bool USE_OFFSET>
-__device__ __forceinline__ void packDepthDeepPipelined(const ElemRec* el, int n, const PackDev& P, const LineK& s,
-                                                       const int16_t* const (&tb)[FP], int nf, float d,
-                                                       PackAcc<FP>& acc) {
+// Sum over the contiguous element range [j0, j1), software-pipelined: the gathers of element j+1 are
+// in flight while element j is accumulated and element j+2's geometry is computed. DEEP: every element
+// is active with its precomputed weight. Otherwise the range is the set of elements inside the
+// aperture (contiguous when the table is ordered by x) and each weight is the window-LUT entry of
+// dx / min(aDT, maxElementDistance), summed into wsum in element order (the reference's order).
+template <int FP, bool USE_OFFSET, bool DEEP>
+__device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, int j1, const float* lut, const PackDev& P,
+                                                   const LineK& s, const int16_t* const (&tb)[FP], float d,
+                                                   float invMax, float& wsum, PackAcc<FP>& acc) {
+    if (j1 <= j0) return;
     const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
     const float dyy = __fmul_rn(s.dirY, d);
     const float dy2 = __fmul_rn(dyy, dyy);
@@ -137,6 +140,13 @@ __device__ __forceinline__ void packDepthDeepPipelined(const ElemRec* el, int n,
     };
     auto geom = [&](int j) -> G {
         const ElemRec e = el[j];
+        float w;
+        if (DEEP) {
+            w = e.wDeep;
+        } else {
+            w = lutIndexWeight(lut, __fmul_rn(e.dx, invMax));
+            wsum = __fadd_rn(wsum, w);
+        }
         const float ex = __fsub_rn(e.xel, xz);
         float t = __fadd_rn(s.iD, __fadd_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2)), d));
         const float delayf = USE_OFFSET ? __fadd_rn(t, P.offset) : t;
@@ -147,14 +157,14 @@ __device__ __forceinline__ void packDepthDeepPipelined(const ElemRec* el, int n,
         const bool lastOne = !interior && static_cast<uint32_t>(delay) < nS && frac == 0.0f;
         G g;
         const uint32_t idx = interior ? static_cast<uint32_t>(delay) : (lastOne ? nS - 2 : 0u);
-        g.wB = interior ? __fmul_rn(e.wDeep, frac) : (lastOne ? e.wDeep : 0.0f);
-        g.wA = interior ? __fmul_rn(e.wDeep, __fsub_rn(1.0f, frac)) : 0.0f;
+        g.wB = interior ? __fmul_rn(w, frac) : (lastOne ? w : 0.0f);
+        g.wA = interior ? __fmul_rn(w, __fsub_rn(1.0f, frac)) : 0.0f;
         g.off = static_cast<uint32_t>(e.ch) + idx;  // e.ch holds the row offset
         return g;
     };
     int16_t a0[FP], b0[FP], a1[FP], b1[FP];
-    G g0 = geom(0);
-    G g1 = n > 1 ? geom(1) : g0;
+    G g0 = geom(j0);
+    G g1 = j0 + 1 < j1 ? geom(j0 + 1) : g0;
     // all slots load valid addresses (empty pack slots alias frame 0, the step past the last element
     // repeats it), so the loads carry no predicate
 #pragma unroll
@@ -162,13 +172,13 @@ __device__ __forceinline__ void packDepthDeepPipelined(const ElemRec* el, int n,
         a0[f] = __ldg(tb[f] + g0.off);
         b0[f] = __ldg(tb[f] + g0.off + 1);
     }
-    for (int j = 0; j < n; j++) {
+    for (int j = j0; j < j1; j++) {
 #pragma unroll
         for (int f = 0; f < FP; f++) {
             a1[f] = __ldg(tb[f] + g1.off);
             b1[f] = __ldg(tb[f] + g1.off + 1);
         }
-        const G g2 = j + 2 < n ? geom(j + 2) : g1;
+        const G g2 = j + 2 < j1 ? geom(j + 2) : g1;
 #pragma unroll
         for (int f = 0; f < FP; f++) {
             acc.v[f] = fmaf(g0.wB, s16ToFloat(b0[f]), fmaf(g0.wA, static_cast<float>(a0[f]), acc.v[f]));
@@ -180,13 +190,31 @@ __device__ __forceinline__ void packDepthDeepPipelined(const ElemRec* el, int n,
     }
 }
 
+// [j0, j1): the elements with |dx| <= aDT in a table ordered by dx (binary searches).
+__device__ __forceinline__ void apertureRange(const ElemRec* el, int n, float aDT, int& j0, int& j1) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (el[mid].dx < -aDT) lo = mid + 1;
+        else hi = mid;
+    }
+    j0 = lo;
+    hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (el[mid].dx <= aDT) lo = mid + 1;
+        else hi = mid;
+    }
+    j1 = lo;
+}
+
 template <int FP, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
     __shared__ ElemRec el[kMaxApertureElems];
     __shared__ float lut[64];
     __shared__ float seg[FP][kPackSegMax];  // the item's beamformed depths (segment + low-pass halo)
     __shared__ uint32_t itemIdx;
-    __shared__ int nEl, cntDeep, deepOk;
+    __shared__ int nEl, cntDeep, deepOk, sortedX;
     __shared__ float sumDeep;
     const int tid = threadIdx.x;
     if (tid < 64) lut[tid] = a.lut.v[tid];
@@ -219,13 +247,14 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         }
         __syncthreads();
         if (tid == 0) {
-            int m = 0, ok = 1;
+            int m = 0, ok = 1, sorted = 1;
             float sum = 0.0f;
             if (valid) {
                 for (int j = 0; j < n0; j++) {
                     ElemRec r = el[j];
                     if (r.ch < 0) continue;
                     r.ch = r.ch * static_cast<int>(P.nS);  // from here on: the channel's row offset
+                    if (m > 0 && !(r.dx >= el[m - 1].dx)) sorted = 0;
                     el[m++] = r;
                     sum = __fadd_rn(sum, r.wDeep);
                     if (!(fabsf(r.dx) <= s.maxDistX)) ok = 0;
@@ -235,6 +264,7 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             sumDeep = sum;
             cntDeep = m;
             deepOk = ok;
+            sortedX = sorted;
         }
         __syncthreads();
         const int n = nEl;
@@ -260,10 +290,17 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
                 float wsum = 0.0f;
                 int cnt = 0;
                 if (deepOk && aDT >= s.maxDistX && n > 0) {
-                    if (useOffset) packDepthDeepPipelined<FP, true>(el, n, P, s, tb, nf, d, acc);
-                    else packDepthDeepPipelined<FP, false>(el, n, P, s, tb, nf, d, acc);
+                    if (useOffset) packDepthPipelined<FP, true, true>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
+                    else packDepthPipelined<FP, false, true>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
                     wsum = sumDeep;
                     cnt = cntDeep;
+                } else if (sortedX) {
+                    const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+                    int j0, j1;
+                    apertureRange(el, n, aDT, j0, j1);
+                    if (useOffset) packDepthPipelined<FP, true, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
+                    else packDepthPipelined<FP, false, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
+                    cnt = j1 - j0;
                 } else {
                     const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
                     if (useOffset) packDepth<FP, false, true>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
