@@ -188,7 +188,7 @@ size_t batchSmem(uint32_t maxCh, uint32_t maxW, uint32_t maxD) {
 
 using namespace sb;
 
-struct PackSet {
+struct PackSet {  // pack and item tables for one (frames per pack, depth tile)
     PackDev* dPacks = nullptr;
     PackItem* dItems = nullptr;
     uint32_t nItems = 0;
@@ -197,7 +197,7 @@ struct PackSet {
 struct sb_batch_plan {
     std::vector<sb_batch_frame> frames;
     sb_batch_params params;
-    PackSet packs[4];  // frames per pack 1 (unused), 2, 4, 8
+    PackSet packs[4][2];  // frames per pack 1 (unused), 2, 4, 8 x depth tile 128, 256
     int fp = 8;
     BatchFrameDev* dFrames = nullptr;
     BatchItem* dItems = nullptr;
@@ -233,15 +233,40 @@ uint32_t batchMaxW(uint32_t maxCh, uint32_t maxD, int ctasPerSm) {
 
 int packSlot(int fp) { return fp == 2 ? 1 : fp == 4 ? 2 : fp == 8 ? 3 : -1; }
 
-// Groups frames by probe plan into packs of up to fp frames; items (pack, line, depth segment),
-// longest first.
-int buildPacks(sb_batch_plan* p, int fp) {
+// Depth segments of one scanline of nD depths for a CTA of nt threads: each item's beamformed depths
+// (its IQ outputs' depths plus the low-pass halo of `half` on both sides, clipped to [0, nD)) fill at
+// most kPackRows depths, a whole number of nt-depth blocks; segment bounds are multiples of dec.
+std::vector<std::pair<uint32_t, uint32_t>> lineSegments(uint32_t nD, int nt, int half, int dec) {
+    const uint32_t target = static_cast<uint32_t>((kPackRows / nt) * nt);
+    std::vector<std::pair<uint32_t, uint32_t>> segs;
+    uint32_t s0 = 0;
+    while (s0 < nD) {
+        const uint32_t lo = s0 > static_cast<uint32_t>(half) ? s0 - half : 0u;
+        // largest s1 (multiple of dec, or nD) with min(nD, s1 + half + 1) - lo <= target
+        uint32_t s1 = nD;
+        if (nD - lo > target) {
+            s1 = lo + target - static_cast<uint32_t>(half) - 1;
+            s1 -= s1 % static_cast<uint32_t>(dec);
+            if (s1 <= s0) s1 = std::min(nD, s0 + static_cast<uint32_t>(dec));  // degenerate shapes: progress
+        }
+        segs.push_back({s0, s1});
+        s0 = s1;
+    }
+    return segs;
+}
+
+// Groups frames by probe plan into packs of up to fp frames; items (pack, line, depth segment) in
+// decreasing order of estimated cost: beamformed depths x receive-aperture elements (window of
+// depth / F-number over the element pitch, capped at the plan's largest aperture) x (element geometry +
+// per-frame gather work for the pack's loop width), so that the queue ends on the cheapest items.
+int buildPacks(sb_batch_plan* p, int fp, int nt) {
     const int slot = packSlot(fp);
     if (slot < 0) return fail(SB_ERR_INVALID_ARG, "sb_batch: frames_per_pack %d not in {1, 2, 4, 8}", fp);
-    PackSet& ps = p->packs[slot];
+    if (nt != 128 && nt != 256) return fail(SB_ERR_INVALID_ARG, "sb_batch: pack kernel block %d not in {128, 256}", nt);
+    PackSet& ps = p->packs[slot][nt == 128 ? 0 : 1];
     if (ps.dPacks) return SB_OK;
     std::vector<PackDev> packs;
-    std::vector<const sb_das_plan*> probes;
+    std::vector<const sb_das_plan*> probes, packProbe;
     for (const auto& fr : p->frames)
         if (std::find(probes.begin(), probes.end(), fr.probe) == probes.end()) probes.push_back(fr.probe);
     for (const sb_das_plan* probe : probes) {
@@ -272,17 +297,45 @@ int buildPacks(sb_batch_plan* p, int fp) {
                 d.rfOut[k] = fk.rfOut;
             }
             packs.push_back(d);
+            packProbe.push_back(probe);
         }
     }
-    const int dec = p->args.dec;
-    const uint32_t seg = static_cast<uint32_t>(kPackSeg - (kPackSeg % dec));
+    const int dec = p->args.dec, half = p->args.half;
+    const int kHalf = fp >= 4 ? fp / 2 : 1;
     std::vector<PackItem> items;
-    for (uint32_t k = 0; k < packs.size(); k++)
+    std::vector<double> cost;
+    for (uint32_t k = 0; k < packs.size(); k++) {
+        const sb_das_plan* pr = packProbe[k];
+        const int kw = packs[k].nf > kHalf ? fp : (packs[k].nf > 1 ? kHalf : 1);
+        const double perElem = 35.0 + 16.0 * kw;  // instructions per element: geometry + per-frame gathers
+        // receive-aperture elements per depth, from the element pitch and the F-number
+        const std::vector<float>& xe = *pr->hXeMM;
+        const std::vector<float>& dep = *pr->hDepthMM;
+        const double pitch = pr->layoutX > 1 ? std::fabs(static_cast<double>(xe[pr->layoutX - 1]) - xe[0]) / (pr->layoutX - 1) : 1.0;
+        const double maxAp = std::max(1, pr->maxApertureX) * std::max(1, pr->is3D ? pr->maxApertureY : 1);
+        const double F = packs[k].F > 0.0f ? packs[k].F : 1.0;
+        std::vector<double> prefix(packs[k].nD + 1, 0.0);  // cumulative aperture elements over depths
+        for (uint32_t r = 0; r < packs[k].nD; r++) {
+            const double w = pitch > 0.0 ? dep[r] / F / pitch + 1.0 : maxAp;
+            prefix[r + 1] = prefix[r] + std::min(maxAp, std::max(1.0, w));
+        }
+        const auto segs = lineSegments(packs[k].nD, nt, half, dec);
         for (uint32_t l = 0; l < packs[k].nRx; l++)
-            for (uint32_t s0 = 0; s0 < packs[k].nD; s0 += seg) items.push_back({k, l, s0, std::min(packs[k].nD, s0 + seg)});
-    std::stable_sort(items.begin(), items.end(), [&](const PackItem& a, const PackItem& b) {
-        return static_cast<uint64_t>(a.seg1 - a.seg0) * packs[a.pack].nf > static_cast<uint64_t>(b.seg1 - b.seg0) * packs[b.pack].nf;
-    });
+            for (const auto& sg : segs) {
+                items.push_back({k, l, sg.first, sg.second});
+                const uint32_t lo = sg.first > static_cast<uint32_t>(half) ? sg.first - half : 0u;
+                const uint32_t hi = std::min(packs[k].nD, sg.second + static_cast<uint32_t>(half) + 1);
+                if (hi - lo > static_cast<uint32_t>(kPackRows))
+                    return fail(SB_ERR_UNSUPPORTED, "sb_batch: item of %u depths exceeds %d", hi - lo, kPackRows);
+                cost.push_back((prefix[hi] - prefix[lo]) * perElem);
+            }
+    }
+    std::vector<uint32_t> order(items.size());
+    for (uint32_t i = 0; i < order.size(); i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+    std::vector<PackItem> sorted(items.size());
+    for (size_t i = 0; i < order.size(); i++) sorted[i] = items[order[i]];
+    items.swap(sorted);
     cudaError_t e = cudaMalloc(&ps.dPacks, packs.size() * sizeof(PackDev));
     if (e == cudaSuccess) e = cudaMalloc(&ps.dItems, items.size() * sizeof(PackItem));
     if (e == cudaSuccess) e = cudaMemcpy(ps.dPacks, packs.data(), packs.size() * sizeof(PackDev), cudaMemcpyHostToDevice);
@@ -299,11 +352,12 @@ int buildPacks(sb_batch_plan* p, int fp) {
 }
 
 void freePacks(sb_batch_plan* p) {
-    for (auto& ps : p->packs) {
-        cudaFree(ps.dPacks);
-        cudaFree(ps.dItems);
-        ps = PackSet();
-    }
+    for (auto& row : p->packs)
+        for (auto& ps : row) {
+            cudaFree(ps.dPacks);
+            cudaFree(ps.dItems);
+            ps = PackSet();
+        }
 }
 
 template <int FP, int MINB> int launchStagedPack(const PackArgs& a, int grid, cudaStream_t st) {
@@ -322,9 +376,11 @@ template <int FP, int MINB> int launchStagedPack(const PackArgs& a, int grid, cu
 int launchBatch(sb_batch_plan* p, int nt, int ctas, int fp, int staged, cudaStream_t st) {
     const int grid = smCount() * ctas;
     if (fp > 1) {
-        int e = buildPacks(p, fp);
+        if (staged ? nt != kStageDepths : (nt != 128 && nt != 256))
+            return fail(SB_ERR_INVALID_ARG, "sb_batch: pack kernel block %d not in {128, 256}", nt);
+        int e = buildPacks(p, fp, nt);
         if (e != SB_OK) return e;
-        const PackSet& ps = p->packs[packSlot(fp)];
+        const PackSet& ps = p->packs[packSlot(fp)][nt == 128 ? 0 : 1];
         PackArgs a;
         a.packs = ps.dPacks;
         a.items = ps.dItems;
@@ -542,7 +598,7 @@ int sb_batch_run(sb_batch_plan* p, int use_graph, sb_stream stream) {
     cudaStream_t st = S(stream);
     if (!use_graph) return launchBatch(p, p->nt, p->ctasPerSm, p->fp, p->staged, st);
     if (p->fp > 1) {
-        int e = buildPacks(p, p->fp);  // outside the capture: it allocates
+        int e = buildPacks(p, p->fp, p->staged ? kStageDepths : p->nt);  // outside the capture: it allocates
         if (e != SB_OK) return e;
     }
     if (!p->graphExec || p->graphNt != p->nt || p->graphCtas != p->ctasPerSm || p->graphFp != p->fp ||

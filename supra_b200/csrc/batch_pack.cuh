@@ -9,10 +9,12 @@
 // gather and four flops. Channel samples are read through L1/L2 (each transmit's rows are used by
 // exactly one scanline, so they cross HBM once).
 //
-// Depth segments of kPackSeg depths (multiple of the decimation) are beamformed with a halo of `half`
-// depths on both sides so that the low-pass of the IQ stage sees all its taps; the beamformed depths
-// of the whole item stay in shared memory and the IQ outputs are computed once the item is complete,
-// so the CTA meets one barrier per item instead of two per depth block. The aperture test,
+// Depth segments (multiples of the decimation) are beamformed with a halo of `half` depths on both
+// sides so that the low-pass of the IQ stage sees all its taps; the host cuts each scanline so that an
+// item's depths (halo included, at most kPackRows) fill whole blocks of the CTA's threads. The
+// beamformed depths of the whole item stay in shared memory and the IQ outputs are computed once the
+// item is complete, so the CTA meets one barrier per item instead of two per depth block. A partial
+// pack (fewer frames than slots) runs the loops of a narrower pack. The aperture test,
 // window-LUT entry and sample index are the reference's bit for bit; the per-frame accumulation is
 // contracted into FMAs (w(1-f) and w f computed once per element), so sums differ from the per-frame
 // kernel by float rounding only (~1e-7 relative).
@@ -24,8 +26,7 @@
 namespace sb {
 
 constexpr int kMaxPack = 8;
-constexpr int kPackSeg = 1024;                         // depths per work item (multiple of the decimation below)
-constexpr int kPackSegMax = kPackSeg + kIqMaxTaps + 2;  // + the low-pass halo on both sides
+constexpr int kPackRows = 1152;  // beamformed depths per work item, low-pass halo included (9 blocks of 128)
 
 struct PackDev {
     const LineDT* lines;
@@ -62,9 +63,9 @@ struct PackAcc {
     float v[FP];
 };
 
-// Sum of one depth over the element table for the FP frames of the pack (the reference's
+// Sum of one depth over the element table for the first K frames of the pack (the reference's
 // sampleBeamform2D per frame, with the per-element geometry shared).
-template <int FP, bool DEEP, bool USE_OFFSET>
+template <int FP, int K, bool DEEP, bool USE_OFFSET>
 __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float* lut, const PackDev& P, const LineK& s,
                                           const int16_t* const (&tb)[FP], int nf, float d, float aDT, float invMax,
                                           float& wsum, int& cnt, PackAcc<FP>& acc) {
@@ -111,7 +112,7 @@ __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float*
         // every slot of a partial pack points at valid data (frame 0): no per-frame predicate; the sums
         // of empty slots are never written
 #pragma unroll
-        for (int f = 0; f < FP; f++) {
+        for (int f = 0; f < K; f++) {
             const int16_t* p = tb[f] + off;
             const float v0 = static_cast<float>(__ldg(p));
             const float v1 = s16ToFloat(__ldg(p + 1));
@@ -120,12 +121,13 @@ __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float*
     }
 }
 
-// Sum over the contiguous element range [j0, j1), software-pipelined: the gathers of element j+1 are
-// in flight while element j is accumulated and element j+2's geometry is computed. DEEP: every element
-// is active with its precomputed weight. Otherwise the range is the set of elements inside the
-// aperture (contiguous when the table is ordered by x) and each weight is the window-LUT entry of
-// dx / min(aDT, maxElementDistance), summed into wsum in element order (the reference's order).
-template <int FP, bool USE_OFFSET, bool DEEP>
+// Sum over the contiguous element range [j0, j1) for the first K frames, software-pipelined: the
+// gathers of element j+1 are in flight while element j is accumulated and element j+2's geometry is
+// computed. DEEP: every element is active with its precomputed weight. Otherwise the range is the set
+// of elements inside the aperture (contiguous when the table is ordered by x) and each weight is the
+// window-LUT entry of dx / min(aDT, maxElementDistance), summed into wsum in element order (the
+// reference's order).
+template <int FP, int K, bool USE_OFFSET, bool DEEP>
 __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, int j1, const float* lut, const PackDev& P,
                                                    const LineK& s, const int16_t* const (&tb)[FP], float d,
                                                    float invMax, float& wsum, PackAcc<FP>& acc) {
@@ -162,25 +164,25 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         g.off = static_cast<uint32_t>(e.ch) + idx;  // e.ch holds the row offset
         return g;
     };
-    int16_t a0[FP], b0[FP], a1[FP], b1[FP];
+    int16_t a0[K], b0[K], a1[K], b1[K];
     G g0 = geom(j0);
     G g1 = j0 + 1 < j1 ? geom(j0 + 1) : g0;
     // all slots load valid addresses (empty pack slots alias frame 0, the step past the last element
     // repeats it), so the loads carry no predicate
 #pragma unroll
-    for (int f = 0; f < FP; f++) {
+    for (int f = 0; f < K; f++) {
         a0[f] = __ldg(tb[f] + g0.off);
         b0[f] = __ldg(tb[f] + g0.off + 1);
     }
     for (int j = j0; j < j1; j++) {
 #pragma unroll
-        for (int f = 0; f < FP; f++) {
+        for (int f = 0; f < K; f++) {
             a1[f] = __ldg(tb[f] + g1.off);
             b1[f] = __ldg(tb[f] + g1.off + 1);
         }
         const G g2 = j + 2 < j1 ? geom(j + 2) : g1;
 #pragma unroll
-        for (int f = 0; f < FP; f++) {
+        for (int f = 0; f < K; f++) {
             acc.v[f] = fmaf(g0.wB, s16ToFloat(b0[f]), fmaf(g0.wA, static_cast<float>(a0[f]), acc.v[f]));
             a0[f] = a1[f];
             b0[f] = b1[f];
@@ -208,11 +210,47 @@ __device__ __forceinline__ void apertureRange(const ElemRec* el, int n, float aD
     j1 = lo;
 }
 
+// One beamformed depth for the first K frames of the pack: the deep path (every element active
+// with its precomputed weight), the aperture range of an x-ordered table, or the element-by-element
+// aperture test; then the reference's normalisation (sum / weight sum * count) and clamped cast.
+template <int FP, int K>
+__device__ __forceinline__ void packRow(const ElemRec* el, int n, const float* lut, const PackDev& P, const LineK& s,
+                                        const int16_t* const (&tb)[FP], int nf, float d, int deepOk, int sortedX,
+                                        float sumDeep, int cntDeep, PackAcc<FP>& acc) {
+    const float aDT = apertureDTf(d, P.dt, P.c, P.F);
+    const bool useOffset = P.offset != 0.0f;
+    float wsum = 0.0f;
+    int cnt = 0;
+    if (deepOk && aDT >= s.maxDistX && n > 0) {
+        if (useOffset) packDepthPipelined<FP, K, true, true>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
+        else packDepthPipelined<FP, K, false, true>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
+        wsum = sumDeep;
+        cnt = cntDeep;
+    } else if (sortedX) {
+        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+        int j0, j1;
+        apertureRange(el, n, aDT, j0, j1);
+        if (useOffset) packDepthPipelined<FP, K, true, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
+        else packDepthPipelined<FP, K, false, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
+        cnt = j1 - j0;
+    } else {
+        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+        if (useOffset) packDepth<FP, K, false, true>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
+        else packDepth<FP, K, false, false>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
+    }
+#pragma unroll
+    for (int f = 0; f < K; f++) {
+        const float v = cnt > 0 ? __fmul_rn(__fdiv_rn(acc.v[f], wsum), static_cast<float>(cnt)) : 0.0f;
+        acc.v[f] = clampCast<float>(v);
+    }
+}
+
 template <int FP, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
     __shared__ ElemRec el[kMaxApertureElems];
     __shared__ float lut[64];
-    __shared__ float seg[FP][kPackSegMax];  // the item's beamformed depths (segment + low-pass halo)
+    constexpr int kHalf = FP >= 4 ? FP / 2 : 1;
+    __shared__ float seg[FP][kPackRows];  // the item's beamformed depths (segment + low-pass halo)
     __shared__ uint32_t itemIdx;
     __shared__ int nEl, cntDeep, deepOk, sortedX;
     __shared__ float sumDeep;
@@ -278,6 +316,8 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         const int so0 = static_cast<int>(pi.seg0) / a.dec;
         const int so1 = min(static_cast<int>(pi.seg1) / a.dec, nD / a.dec);
         const int nBlocks = (rEnd - rStart + NT - 1) / NT;
+        // frames of a partial pack take the narrower loops (a pack of 4 frames holding 1 or 2)
+        const int kw = nf > kHalf ? FP : (nf > 1 ? kHalf : 1);
         for (int k = 0; k < nBlocks; k++) {
             const int r = rStart + k * NT + tid;
             PackAcc<FP> acc;
@@ -285,32 +325,9 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             for (int f = 0; f < FP; f++) acc.v[f] = 0.0f;
             if (r < rEnd && valid) {
                 const float d = __ldg(P.depth + r);
-                const float aDT = apertureDTf(d, P.dt, P.c, P.F);
-                const bool useOffset = P.offset != 0.0f;
-                float wsum = 0.0f;
-                int cnt = 0;
-                if (deepOk && aDT >= s.maxDistX && n > 0) {
-                    if (useOffset) packDepthPipelined<FP, true, true>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
-                    else packDepthPipelined<FP, false, true>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
-                    wsum = sumDeep;
-                    cnt = cntDeep;
-                } else if (sortedX) {
-                    const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
-                    int j0, j1;
-                    apertureRange(el, n, aDT, j0, j1);
-                    if (useOffset) packDepthPipelined<FP, true, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
-                    else packDepthPipelined<FP, false, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
-                    cnt = j1 - j0;
-                } else {
-                    const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
-                    if (useOffset) packDepth<FP, false, true>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
-                    else packDepth<FP, false, false>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
-                }
-#pragma unroll
-                for (int f = 0; f < FP; f++) {
-                    const float v = cnt > 0 ? __fmul_rn(__fdiv_rn(acc.v[f], wsum), static_cast<float>(cnt)) : 0.0f;
-                    acc.v[f] = clampCast<float>(v);
-                }
+                if (kw == FP) packRow<FP, FP>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
+                else if (kw == kHalf) packRow<FP, kHalf>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
+                else packRow<FP, 1>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
             }
             if (r < rEnd) {
 #pragma unroll
