@@ -129,6 +129,21 @@ int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out,
                double f_number, double speed_of_sound_mm_s, int window_type, float window_parameter,
                int interpolate_transmits, int32_t additional_offset, sb_stream stream);
 
+/* Sample beamformers (RxBeamformerCuda::RxSampleBeamformer, Beamformer/RxBeamformerCuda.h:31-36, and the
+ * BeamformingNode parameter "beamformerType", Beamformer/BeamformingNode.cpp:46). */
+#define SB_BF_DELAY_AND_SUM 0        /* "DelayAndSum" */
+#define SB_BF_DELAY_AND_STDDEV 1     /* "DelayAndStdDev" (Beamformer/RxSampleBeamformerDelayAndStdDev.h) */
+#define SB_BF_COHERENCE_FACTOR_DAS 2 /* "CoherenceFactorDelayAndSum" (...CoherenceFactorDelayAndSum.h) */
+#define SB_BF_TEST_SIGNAL 3          /* "TestSignal" (...TestSignal.h): a geometric phantom, no RF read */
+
+/* RxBeamformerCuda::performRxBeamforming(sampleBeamformer, ...) (Beamformer/RxBeamformerCuda.cu:540-662):
+ * sb_das_run with the sample beamformer chosen. SB_BF_DELAY_AND_SUM is sb_das_run itself; the others
+ * follow the reference's reducers bit for bit in IEEE float semantics (2D and 3D, highest-weight or
+ * interpolated transmits, element-to-channel map). */
+int sb_das_run_beamformer(const sb_das_plan* plan, int sample_beamformer, const void* rf, int rf_dtype, void* out,
+                          int out_dtype, double f_number, double speed_of_sound_mm_s, int window_type,
+                          float window_parameter, int interpolate_transmits, int32_t additional_offset, sb_stream stream);
+
 /* Allocation-free delay-and-sum, for callers that cannot allocate device memory: hosts that reserve
  * their whole device budget up front and hand out buffers from their own pool (as SUPRA's container
  * pool does), or real-time frame loops that cannot afford cudaMalloc/cudaFree (cudaFree synchronises

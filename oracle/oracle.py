@@ -117,6 +117,30 @@ def das(geom, rf: np.ndarray, f_number=1.0, c_mm_s=None, window=1, window_param=
     return out.reshape(geom.num_depths, geom.num_rx)
 
 
+BEAMFORMERS = {"DelayAndSum": 0, "DelayAndStdDev": 1, "CoherenceFactorDelayAndSum": 2, "TestSignal": 3}
+
+
+def das_bf(geom, rf: np.ndarray, beamformer, f_number=1.0, c_mm_s=None, window=1, window_param=0.0, interp_tx=False,
+           additional_offset=0, threads=None, ref: bool = False) -> np.ndarray:
+    """One frame through a sample beamformer (name or RxBeamformerCuda::RxSampleBeamformer index), float
+    semantics; ref=True runs the reference's own reducers (oracle/_ref)."""
+    bf = BEAMFORMERS[beamformer] if isinstance(beamformer, str) else int(beamformer)
+    g = geom.ctypes()
+    rf32 = np.ascontiguousarray(rf, dtype=np.float32)
+    c = geom.speed_of_sound_mm_s if c_mm_s is None else c_mm_s
+    out = np.full(geom.num_depths * geom.num_rx, np.nan, np.float32)
+    if ref:
+        st = ref_lib().ref_das_bf(C.byref(g), _vp(_p(rf32)), _vp(_p(out)), C.c_double(f_number), C.c_double(c),
+                                  C.c_int(window), C.c_float(window_param), C.c_int(int(interp_tx)),
+                                  C.c_int32(additional_offset), C.c_int(bf))
+    else:
+        st = lib().orc_das_bf(C.byref(g), _vp(_p(rf32)), _vp(_p(out)), C.c_double(f_number), C.c_double(c),
+                              C.c_int(window), C.c_float(window_param), C.c_int(int(interp_tx)),
+                              C.c_int32(additional_offset), C.c_int(bf), C.c_int(threads or nthreads()))
+    assert st == 0
+    return out.reshape(geom.num_depths, geom.num_rx)
+
+
 def das_adjoint64(geom, rf: np.ndarray, apod, gout: np.ndarray, c_mm_s=None, f_number=1.0, window=1, window_param=0.0):
     """FP64 reference gradient of the apodised 2D DAS: (grad_rf, grad_apod, grad_c)."""
     g = geom.ctypes()

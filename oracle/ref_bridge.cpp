@@ -8,9 +8,10 @@
 // restatement with what the reference's code computes:
 //   - FirFilterFactory::createFilter coefficients,
 //   - WindowFunction LUTs and WindowFunctionGpu::get,
-//   - the per-sample DAS reducers sampleBeamform2D / sampleBeamform3D (called exactly as the
-//     kernels rxBeamformingDTSPACEKernel / rxBeamformingDTSPACE3DKernel call them,
-//     RxBeamformerCuda.cu:238-323 and :119-228, one (line, depth) at a time).
+//   - the per-sample reducers sampleBeamform2D / sampleBeamform3D of the four sample beamformers
+//     (DelayAndSum, DelayAndStdDev, CoherenceFactorDelayAndSum, TestSignal), called exactly as the
+//     kernels rxBeamformingDTSPACEKernel / rxBeamformingDTSPACE3DKernel call them
+//     (RxBeamformerCuda.cu:238-323 and :119-228, one (line, depth) at a time).
 // ================================================================================================
 #include <math.h>    // brings the float overloads of abs() into the global namespace
 #include <stdlib.h>
@@ -31,6 +32,9 @@ template <typename T> constexpr inline T squ(const T& x) { return x * x; }
 #include "USTransducer.h"
 #include "RxBeamformerCommon.h"
 #include "RxSampleBeamformerDelayAndSum.h"
+#include "RxSampleBeamformerDelayAndStdDev.h"
+#include "RxSampleBeamformerCoherenceFactorDelayAndSum.h"
+#include "RxSampleBeamformerTestSignal.h"
 
 #include "supra_b200.h"
 
@@ -56,10 +60,13 @@ float ref_window_get(int type, float param, uint32_t n, float rel) {
     return w.getGpu()->get(rel);
 }
 
-// One frame of DAS through the reference's per-sample reducers. The geometry conversion is the
-// first call of RxBeamformerCuda::convertToDtSpace (RxBeamformerCuda.cu:58-107).
-int ref_das(const sb_geometry* g, const float* rf, float* out, double fNumber, double speedOfSoundMMperS,
-            int windowType, float windowParameter, int interpolateTransmits, int32_t additionalOffset) {
+}  // extern "C"
+
+// One frame through the reference's per-sample reducers of SampleBeamformer. The geometry conversion
+// is the first call of RxBeamformerCuda::convertToDtSpace (RxBeamformerCuda.cu:58-107).
+template <class SampleBeamformer>
+int refDas(const sb_geometry* g, const float* rf, float* out, double fNumber, double speedOfSoundMMperS,
+           int windowType, float windowParameter, int interpolateTransmits, int32_t additionalOffset) {
     typedef float LocationType;
     double dt = 1.0 / g->sampling_frequency_hz;
     double factor = 1 / 1.0 / (speedOfSoundMMperS * dt);
@@ -129,12 +136,12 @@ int ref_das(const sb_geometry* g, const float* rf, float* out, double fNumber, d
                     if (txParams.txScanlineIdx >= g->num_tx) { invalid = true; break; }
                     float sLocal;
                     if (is3D) {
-                        sLocal = RxSampleBeamformerDelayAndSum::sampleBeamform3D<true, false, float, float, LocationType>(
+                        sLocal = SampleBeamformer::template sampleBeamform3D<true, false, float, float, LocationType>(
                             txParams, rf, elementLayout, g->num_channels, g->num_samples, xs.data(), ys.data(),
                             scanline_x, scanline_z, dirX, dirY, dirZ, aDT, d, invMax3D, speedOfSound, dtf,
                             additionalOffset, wg, functionShared.data(), nullptr);
                     } else {
-                        sLocal = RxSampleBeamformerDelayAndSum::sampleBeamform2D<true, false, float, float, LocationType>(
+                        sLocal = SampleBeamformer::template sampleBeamform2D<true, false, float, float, LocationType>(
                             txParams, rf, g->num_elements, g->num_channels, g->num_samples, xs.data(), scanline_x,
                             dirX, dirY, dirZ, aDT, d, invMax2D, speedOfSound, dtf, additionalOffset, wg, nullptr);
                     }
@@ -146,6 +153,35 @@ int ref_das(const sb_geometry* g, const float* rf, float* out, double fNumber, d
         }
     }
     return 0;
+}
+
+extern "C" {
+
+int ref_das(const sb_geometry* g, const float* rf, float* out, double fNumber, double speedOfSoundMMperS,
+            int windowType, float windowParameter, int interpolateTransmits, int32_t additionalOffset) {
+    return refDas<RxSampleBeamformerDelayAndSum>(g, rf, out, fNumber, speedOfSoundMMperS, windowType, windowParameter,
+                                                 interpolateTransmits, additionalOffset);
+}
+
+// beamformer: the order of RxBeamformerCuda::RxSampleBeamformer (RxBeamformerCuda.h:31-36).
+int ref_das_bf(const sb_geometry* g, const float* rf, float* out, double fNumber, double speedOfSoundMMperS,
+               int windowType, float windowParameter, int interpolateTransmits, int32_t additionalOffset, int beamformer) {
+    switch (beamformer) {
+    case 0:
+        return refDas<RxSampleBeamformerDelayAndSum>(g, rf, out, fNumber, speedOfSoundMMperS, windowType,
+                                                     windowParameter, interpolateTransmits, additionalOffset);
+    case 1:
+        return refDas<RxSampleBeamformerDelayAndStdDev>(g, rf, out, fNumber, speedOfSoundMMperS, windowType,
+                                                        windowParameter, interpolateTransmits, additionalOffset);
+    case 2:
+        return refDas<RxSampleBeamformerCoherenceFactorDelayAndSum>(g, rf, out, fNumber, speedOfSoundMMperS, windowType,
+                                                                    windowParameter, interpolateTransmits, additionalOffset);
+    case 3:
+        return refDas<RxSampleBeamformerTestSignal>(g, rf, out, fNumber, speedOfSoundMMperS, windowType, windowParameter,
+                                                    interpolateTransmits, additionalOffset);
+    default:
+        return -1;
+    }
 }
 
 }  // extern "C"

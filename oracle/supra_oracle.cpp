@@ -436,6 +436,196 @@ void dasFrame(const sb_geometry* g, const float* rf, Acc* out, double fNumber, d
     }
 }
 
+// --------------------------------------------------------------------------------- DAS variants
+// The other sample beamformers of RxBeamformerCuda::performRxBeamforming (BF/RxBeamformerCuda.cu:
+// 567-591), called by the same kernels in place of the delay-and-sum reducer. Float semantics only.
+enum { kBfDelayAndSum = 0, kBfDelayAndStdDev = 1, kBfCoherenceFactor = 2, kBfTestSignal = 3 };
+
+// Interpolated sample of one element (the two cases of the reference's reducers). Returns false when
+// the delay falls outside the record; `value` is then left as it was (the variants keep the previous
+// element's value).
+inline bool delayedSample2D(const float* rf, size_t base, uint32_t numTimesteps, float delayfIn, float weight,
+                            bool weighted, float& value) {
+    int32_t delay = static_cast<int32_t>(std::floor(delayfIn));
+    float delayf = delayfIn - static_cast<float>(delay);
+    if (static_cast<uint32_t>(delay) < numTimesteps - 1) {
+        float v = (1.0f - delayf) * rf[base + delay] + delayf * rf[base + delay + 1];
+        value = weighted ? weight * v : v;
+        return true;
+    } else if (static_cast<uint32_t>(delay) < numTimesteps && delayf == 0.0f) {
+        value = weighted ? weight * rf[base + delay] : rf[base + delay];
+        return true;
+    }
+    return false;
+}
+
+inline bool delayedSample3D(const float* rf, size_t base, uint32_t numTimesteps, float delayfIn, float weight,
+                            bool weighted, float& value) {
+    float fl = std::floor(delayfIn);
+    uint32_t delay = fl <= 0.0f ? 0u : static_cast<uint32_t>(fl);  // float -> uint32 saturates on the GPU
+    float delayf = delayfIn - static_cast<float>(delay);
+    if (delay < numTimesteps - 1) {
+        float v = (1.0f - delayf) * rf[base + delay] + delayf * rf[base + delay + 1];
+        value = weighted ? weight * v : v;
+        return true;
+    } else if (delay < numTimesteps && delayf == 0.0f) {
+        value = weighted ? weight * rf[base + delay] : rf[base + delay];
+        return true;
+    }
+    return false;
+}
+
+// RxSampleBeamformerDelayAndStdDev::sampleBeamform2D (BF/RxSampleBeamformerDelayAndStdDev.h:146-248) and
+// RxSampleBeamformerCoherenceFactorDelayAndSum::sampleBeamform2D (BF/RxSampleBeamformerCoherenceFactor
+// DelayAndSum.h:139-235): the DAS result, then a second pass over the aperture.
+float variant2D(int bf, const sb_geometry* g, const GeomDT& G, const Window& win, const float* rf, const LineDT& s,
+                int k, float aDT, float depth, float invMax, int32_t additionalOffset) {
+    float das = sampleBeamform2D<float>(g, G, win, rf, s, k, aDT, depth, invMax, additionalOffset, nullptr);
+    float value = 0.0f, acc = 0.0f, acc2 = 0.0f, weightAcum = 0.0f;
+    int numAdds = 0;
+    const float initialDelay = s.initialDelay[k];
+    const uint32_t nS = g->num_samples, nCh = g->num_channels;
+    for (int32_t e = s.firstX[k]; e < s.lastX[k]; e++) {
+        int32_t ch = channelOf(g, static_cast<uint32_t>(e));
+        if (ch < 0) continue;
+        float x_elem = G.xe[e];
+        if (std::fabs(x_elem - s.x) <= aDT) {
+            float weight = 0.0f;
+            if (bf == kBfDelayAndStdDev) {
+                weight = win.get((x_elem - s.x) * invMax);
+                weightAcum += weight;
+            }
+            numAdds++;
+            float a = s.x + s.dirX * depth;
+            float dx = x_elem - a;
+            float dy = s.dirY * depth;
+            float delayf = initialDelay + (std::sqrt(dx * dx + dy * dy) + depth) + static_cast<float>(additionalOffset);
+            size_t base = static_cast<size_t>(ch) * nS + static_cast<size_t>(s.txIdx[k]) * nCh * nS;
+            delayedSample2D(rf, base, nS, delayf, weight, bf == kBfDelayAndStdDev, value);
+            if (bf == kBfDelayAndStdDev) {
+                acc += squ(value - das);
+            } else {
+                acc += value;
+                acc2 += squ(value);
+            }
+        }
+    }
+    if (numAdds == 0) return 0.0f;
+    if (bf == kBfDelayAndStdDev) return std::sqrt(acc) / weightAcum * static_cast<float>(numAdds);
+    return squ(acc) / acc2 / static_cast<float>(numAdds) * das;
+}
+
+// The 3D reducers of the same classes (DelayAndStdDev.h:34-144, CoherenceFactorDelayAndSum.h:30-137).
+float variant3D(int bf, const sb_geometry* g, const GeomDT& G, const Window& win, const float* rf, const LineDT& s,
+                int k, float aDT, float depth, float invMaxX, float invMaxY, int32_t additionalOffset) {
+    float das = sampleBeamform3D<float>(g, G, win, rf, s, k, aDT, depth, invMaxX, invMaxY, additionalOffset);
+    float value = 0.0f, acc = 0.0f, acc2 = 0.0f, weightAcum = 0.0f;
+    int numAdds = 0;
+    const float initialDelay = s.initialDelay[k];
+    const uint32_t nS = g->num_samples, nCh = g->num_channels;
+    for (uint32_t ex = s.firstX[k]; ex < s.lastX[k]; ex++) {
+        for (uint32_t ey = s.firstY[k]; ey < s.lastY[k]; ey++) {
+            uint32_t elemIdx = ex + ey * g->element_layout[0];
+            int32_t ch = channelOf(g, elemIdx);
+            if (ch < 0) continue;
+            float x_elem = G.xe[elemIdx];
+            float z_elem = G.ye[elemIdx];
+            if ((squ(x_elem - s.x) + squ(z_elem - s.z)) <= aDT) {
+                float weight = 0.0f;
+                if (bf == kBfDelayAndStdDev) {
+                    float wx = win.get((x_elem - s.x) * invMaxX);
+                    float wz = win.get((z_elem - s.z) * invMaxY);
+                    weight = std::sqrt(wx * wz);
+                    weightAcum += weight;
+                }
+                numAdds++;
+                float ax = x_elem - (s.x + s.dirX * depth);
+                float az = z_elem - (s.z + s.dirZ * depth);
+                float ay = s.dirY * depth;
+                float delayf = initialDelay + (std::sqrt(squ(ax) + squ(az) + squ(ay)) + depth) +
+                               static_cast<float>(additionalOffset);
+                size_t base = static_cast<size_t>(ch) * nS + static_cast<size_t>(s.txIdx[k]) * nCh * nS;
+                delayedSample3D(rf, base, nS, delayf, weight, bf == kBfDelayAndStdDev, value);
+                if (bf == kBfDelayAndStdDev) {
+                    acc += squ(value - das);
+                } else {
+                    acc += value;
+                    acc2 += squ(value);
+                }
+            }
+        }
+    }
+    if (numAdds == 0) return 0.0f;
+    if (bf == kBfDelayAndStdDev) return std::sqrt(acc) / weightAcum * static_cast<float>(numAdds);
+    return squ(acc) / acc2 / static_cast<float>(numAdds) * das;
+}
+
+// RxSampleBeamformerTestSignal (BF/RxSampleBeamformerTestSignal.h:24-133): 2 mm cylinders every 6 mm
+// at 30 mm depth, along the elevation axis (and, in 3D, along x), value 1000 inside.
+float testSignal(const LineDT& s, float depth, float dt, float speedOfSound, bool is3D) {
+    const float spacing = 6.0f, diameter = 2.0f, cDepth = 30.0f;
+    float px = s.x + s.dirX * depth, py = s.dirY * depth, pz = is3D ? s.z + s.dirZ * depth : s.dirZ * depth;
+    px = px * dt * speedOfSound;
+    py = py * dt * speedOfSound;
+    pz = pz * dt * speedOfSound;
+    float sample = 0.0f;
+    for (int n = -3; n <= 3; n++) {
+        float dx = px - static_cast<float>(n) * spacing, dy = py - cDepth, dz = 0.0f - 0.0f;
+        if (std::sqrt(dx * dx + dy * dy + dz * dz) <= diameter) sample = 1000.0f;
+    }
+    if (is3D) {
+        for (int n = -3; n <= 3; n++) {
+            float dx = 0.0f - 0.0f, dy = py - cDepth, dz = pz - static_cast<float>(n) * spacing;
+            if (std::sqrt(dx * dx + dy * dy + dz * dz) <= diameter) sample = 1000.0f;
+        }
+    }
+    return sample;
+}
+
+void dasFrameBf(const sb_geometry* g, const float* rf, float* out, double fNumber, double c, int windowType,
+                float windowParameter, int interpolateTransmits, int32_t additionalOffset, int bf, int nthreads) {
+    GeomDT G = toDtSpace(g, c);
+    Window win(windowType, windowParameter, 64);
+    bool is3D = g->rx_layout[0] > 1 && g->rx_layout[1] > 1;
+    const float F = static_cast<float>(fNumber);
+    const float speedOfSound = G.c, dt = G.dt;
+    const int nD = static_cast<int>(g->num_depths), nRx = static_cast<int>(g->num_rx);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int line = 0; line < nRx; line++) {
+        const LineDT& s = G.lines[line];
+        for (int r = 0; r < nD; r++) {
+            float d = G.depths[r];
+            float aDT = ((d * dt) * speedOfSound) / (2 * F) / speedOfSound / dt;
+            float sInterp = 0;
+            int hw = highestWeightIndex(s);
+            bool invalid = false;
+            for (int k = 0; k < 4; k++) {
+                if (!interpolateTransmits && k != hw) continue;
+                if (!(s.txWeights[k] > 0.0)) continue;
+                if (s.txIdx[k] >= g->num_tx) { invalid = true; break; }
+                float sLocal;
+                if (bf == kBfTestSignal) {
+                    sLocal = testSignal(s, d, dt, speedOfSound, is3D);
+                } else if (is3D) {
+                    float aDT2 = squ(aDT);
+                    float sq = std::sqrt(aDT2);
+                    float invX = 1.0f / std::min(sq, s.maxDistX);
+                    float invY = 1.0f / std::min(sq, s.maxDistY);
+                    sLocal = bf == kBfDelayAndSum ? sampleBeamform3D<float>(g, G, win, rf, s, k, aDT2, d, invX, invY, additionalOffset)
+                                                  : variant3D(bf, g, G, win, rf, s, k, aDT2, d, invX, invY, additionalOffset);
+                } else {
+                    float inv = 1 / std::min(aDT, s.maxDistX);
+                    sLocal = bf == kBfDelayAndSum ? sampleBeamform2D<float>(g, G, win, rf, s, k, aDT, d, inv, additionalOffset, nullptr)
+                                                  : variant2D(bf, g, G, win, rf, s, k, aDT, d, inv, additionalOffset);
+                }
+                if (interpolateTransmits) sInterp += static_cast<float>(s.txWeights[k]) * sLocal;
+                else sInterp += sLocal;
+            }
+            if (!invalid) out[static_cast<size_t>(r) * nRx + line] = clampToFloat(sInterp);
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------- raw delay
 // RawDelay::sampleDelay2D + rxDelayDTSPACEKernel, BF/RawDelay.cu:221-312 and :406-468.
 void rawDelayFrame(const sb_geometry* g, const float* rf, float* out, double fNumber, double c, int windowType,
@@ -551,6 +741,16 @@ int orc_das(const sb_geometry* g, const float* rf, float* out_f32, double* out_f
         dasFrame<float>(g, rf, out_f32, fNumber, c, windowType, windowParameter, interpolateTransmits,
                         additionalOffset, apod, nthreads);
     }
+    return 0;
+}
+
+// DAS with another sample beamformer (0 DelayAndSum, 1 DelayAndStdDev, 2 CoherenceFactorDelayAndSum,
+// 3 TestSignal: the order of RxBeamformerCuda::RxSampleBeamformer, BF/RxBeamformerCuda.h:31-36).
+int orc_das_bf(const sb_geometry* g, const float* rf, float* out, double fNumber, double c, int windowType,
+               float windowParameter, int interpolateTransmits, int32_t additionalOffset, int beamformer, int nthreads) {
+    if (!g || !rf || !out || beamformer < 0 || beamformer > 3) return -1;
+    dasFrameBf(g, rf, out, fNumber, c, windowType, windowParameter, interpolateTransmits, additionalOffset, beamformer,
+               nthreads <= 0 ? 1 : nthreads);
     return 0;
 }
 

@@ -42,6 +42,10 @@ def dtype_code(t: torch.Tensor) -> int:
         raise ValueError(f"unsupported dtype {t.dtype}") from None
 
 
+# RxBeamformerCuda::RxSampleBeamformer (Beamformer/RxBeamformerCuda.h:31-36)
+SAMPLE_BEAMFORMERS = {"DelayAndSum": 0, "DelayAndStdDev": 1, "CoherenceFactorDelayAndSum": 2, "TestSignal": 3}
+
+
 class RxBeamformer:
     """RxBeamformerCuda (Beamformer/RxBeamformerCuda.cu:24-663), DelayAndSum, 2D or 3D."""
 
@@ -63,14 +67,24 @@ class RxBeamformer:
 
     def beamform(self, rf: torch.Tensor, f_number=1.0, speed_of_sound_mm_s=None, window_type=1, window_parameter=0.0,
                  interpolate_transmits=False, additional_offset=0, out_dtype=torch.float32,
-                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
+                 out: Optional[torch.Tensor] = None, beamformer="DelayAndSum") -> torch.Tensor:
+        """RxBeamformerCuda::performRxBeamforming (Beamformer/RxBeamformerCuda.cu:540-662): [num_depths][num_rx].
+        beamformer: a name of BeamformingNode's "beamformerType" (DelayAndSum, DelayAndStdDev,
+        CoherenceFactorDelayAndSum, TestSignal) or its index."""
         g = self.geometry
         c = g.speed_of_sound_mm_s if speed_of_sound_mm_s is None else speed_of_sound_mm_s
+        bf = SAMPLE_BEAMFORMERS[beamformer] if isinstance(beamformer, str) else int(beamformer)
         if out is None:
             out = torch.empty((g.num_depths, g.num_rx), dtype=out_dtype, device=rf.device)
-        check("sb_das_run", self.lib.sb_das_run(self._plan, _ptr(rf), dtype_code(rf), _ptr(out), dtype_code(out),
-                                                float(f_number), float(c), int(window_type), float(window_parameter),
-                                                int(bool(interpolate_transmits)), int(additional_offset), _stream()))
+        if bf == 0:
+            check("sb_das_run", self.lib.sb_das_run(self._plan, _ptr(rf), dtype_code(rf), _ptr(out), dtype_code(out),
+                                                    float(f_number), float(c), int(window_type), float(window_parameter),
+                                                    int(bool(interpolate_transmits)), int(additional_offset), _stream()))
+        else:
+            check("sb_das_run_beamformer",
+                  self.lib.sb_das_run_beamformer(self._plan, bf, _ptr(rf), dtype_code(rf), _ptr(out), dtype_code(out),
+                                                 float(f_number), float(c), int(window_type), float(window_parameter),
+                                                 int(bool(interpolate_transmits)), int(additional_offset), _stream()))
         return out
 
     def raw_delay(self, rf: torch.Tensor, f_number=1.0, speed_of_sound_mm_s=None, window_type=1, window_parameter=0.0,

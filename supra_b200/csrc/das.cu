@@ -206,6 +206,195 @@ __global__ void __launch_bounds__(256) dasKernel(DasArgs a) {
     static_cast<OUT*>(a.out)[line + static_cast<size_t>(r) * a.nRx] = clampCast<OUT>(acc);
 }
 
+// ---------------------------------------------------------------------------------------------
+// The other sample beamformers of RxBeamformerCuda::performRxBeamforming (Beamformer/RxBeamformerCuda.cu:
+// 567-591), run by the same per-(scanline, depth) structure as dasKernel:
+//  - DelayAndStdDev (Beamformer/RxSampleBeamformerDelayAndStdDev.h): the DAS value s, then
+//    sqrt(sum_e (v_e - s)^2) / sum w * n with v_e = w_e * lerp_e (a second pass over the aperture);
+//  - CoherenceFactorDelayAndSum (...CoherenceFactorDelayAndSum.h): (sum u_e)^2 / sum u_e^2 / n * s
+//    with u_e = lerp_e unweighted, accumulated in the DAS pass itself (same elements, same delays);
+//  - TestSignal (...TestSignal.h): 1000 inside 2 mm cylinders every 6 mm at 30 mm depth, else 0.
+// In both reducers an element whose delay falls outside the record keeps the previous element's
+// value (the reference's `value` is not reset per element). Every operation is the reference's, in
+// its order, as separately rounded IEEE operations.
+template <typename RF, int BF>
+__device__ __forceinline__ float variant2D(const DasArgs& a, const LineDT& s, int k, const float* lut, float aDT,
+                                           float depth, float invMax) {
+    const float iD = s.initialDelay[k];
+    const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
+    const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, depth));
+    const float dy = __fmul_rn(s.dirY, depth);
+    const float dy2 = __fmul_rn(dy, dy);
+    float sample = 0.0f, weightAcum = 0.0f, value = 0.0f, cs = 0.0f, energy = 0.0f;
+    int numAdds = 0;
+    for (int pass = 0; pass < (BF == SB_BF_DELAY_AND_STDDEV ? 2 : 1); pass++) {
+        const float mean = pass == 0 ? 0.0f
+                                     : (numAdds > 0 ? __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds)) : 0.0f);
+        if (pass == 1) {
+            weightAcum = 0.0f;
+            numAdds = 0;
+            value = 0.0f;
+        }
+        for (int e = s.firstX[k]; e < s.lastX[k]; e++) {
+            const int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(static_cast<uint32_t>(e) % a.nCh);
+            if (ch < 0) continue;
+            const float xel = __ldg(a.xe + e);
+            const float dx = __fsub_rn(xel, s.x);
+            if (!(fabsf(dx) <= aDT)) continue;
+            const float w = lutGet(lut, __fmul_rn(dx, invMax));
+            weightAcum = __fadd_rn(weightAcum, w);
+            numAdds++;
+            const float ex = __fsub_rn(xel, xz);
+            const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2));
+            const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(dist, depth)), a.offset);
+            const int32_t delay = static_cast<int32_t>(floorf(delayf));
+            const float frac = __fsub_rn(delayf, static_cast<float>(delay));
+            const RF* p = tx + static_cast<size_t>(ch) * a.nS;
+            if (static_cast<uint32_t>(delay) < a.nS - 1) {
+                const float v0 = toFloat(p[delay]), v1 = toFloat(p[delay + 1]);
+                const float v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
+                if (pass == 0) sample = __fadd_rn(sample, __fmul_rn(w, v));
+                value = BF == SB_BF_DELAY_AND_STDDEV ? __fmul_rn(w, v) : v;
+            } else if (static_cast<uint32_t>(delay) < a.nS && frac == 0.0f) {
+                const float v0 = toFloat(p[delay]);
+                if (pass == 0) sample = __fadd_rn(sample, __fmul_rn(w, v0));
+                value = BF == SB_BF_DELAY_AND_STDDEV ? __fmul_rn(w, v0) : v0;
+            }
+            if (BF == SB_BF_COHERENCE_FACTOR_DAS) {
+                cs = __fadd_rn(cs, value);
+                energy = __fadd_rn(energy, __fmul_rn(value, value));
+            } else if (pass == 1) {
+                const float t = __fsub_rn(value, mean);
+                cs = __fadd_rn(cs, __fmul_rn(t, t));
+            }
+        }
+    }
+    if (numAdds == 0) return 0.0f;
+    if (BF == SB_BF_DELAY_AND_STDDEV) return __fmul_rn(__fdiv_rn(__fsqrt_rn(cs), weightAcum), static_cast<float>(numAdds));
+    const float das = __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds));
+    return __fmul_rn(__fdiv_rn(__fdiv_rn(__fmul_rn(cs, cs), energy), static_cast<float>(numAdds)), das);
+}
+
+template <typename RF, int BF>
+__device__ __forceinline__ float variant3D(const DasArgs& a, const LineDT& s, int k, const float* lut, float aDT2,
+                                           float depth, float invX, float invY) {
+    const float iD = s.initialDelay[k];
+    const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
+    const float px = __fadd_rn(s.x, __fmul_rn(s.dirX, depth));
+    const float pz = __fadd_rn(s.z, __fmul_rn(s.dirZ, depth));
+    const float ay = __fmul_rn(s.dirY, depth);
+    const float ay2 = __fmul_rn(ay, ay);
+    float sample = 0.0f, weightAcum = 0.0f, value = 0.0f, cs = 0.0f, energy = 0.0f;
+    int numAdds = 0;
+    for (int pass = 0; pass < (BF == SB_BF_DELAY_AND_STDDEV ? 2 : 1); pass++) {
+        const float mean = pass == 0 ? 0.0f
+                                     : (numAdds > 0 ? __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds)) : 0.0f);
+        if (pass == 1) {
+            weightAcum = 0.0f;
+            numAdds = 0;
+            value = 0.0f;
+        }
+        for (uint32_t ex = s.firstX[k]; ex < s.lastX[k]; ex++) {
+            for (uint32_t ey = s.firstY[k]; ey < s.lastY[k]; ey++) {
+                const uint32_t e = ex + ey * a.layoutX;
+                const int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(e % a.nCh);
+                if (ch < 0) continue;
+                const float xel = __ldg(a.xe + e), zel = __ldg(a.ye + e);
+                const float dx = __fsub_rn(xel, s.x), dz = __fsub_rn(zel, s.z);
+                if (!(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)) <= aDT2)) continue;
+                const float w = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(dx, invX)), lutGet(lut, __fmul_rn(dz, invY))));
+                weightAcum = __fadd_rn(weightAcum, w);
+                numAdds++;
+                const float qx = __fsub_rn(xel, px), qz = __fsub_rn(zel, pz);
+                const float q = __fadd_rn(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qz, qz)), ay2);
+                const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(__fsqrt_rn(q), depth)), a.offset);
+                const uint32_t delay = static_cast<uint32_t>(floorf(delayf));  // saturates at 0 like the reference
+                const float frac = __fsub_rn(delayf, static_cast<float>(delay));
+                const RF* p = tx + static_cast<size_t>(ch) * a.nS;
+                if (delay < a.nS - 1) {
+                    const float v0 = toFloat(p[delay]), v1 = toFloat(p[delay + 1]);
+                    const float v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
+                    if (pass == 0) sample = __fadd_rn(sample, __fmul_rn(w, v));
+                    value = BF == SB_BF_DELAY_AND_STDDEV ? __fmul_rn(w, v) : v;
+                } else if (delay < a.nS && frac == 0.0f) {
+                    const float v0 = toFloat(p[delay]);
+                    if (pass == 0) sample = __fadd_rn(sample, __fmul_rn(w, v0));
+                    value = BF == SB_BF_DELAY_AND_STDDEV ? __fmul_rn(w, v0) : v0;
+                }
+                if (BF == SB_BF_COHERENCE_FACTOR_DAS) {
+                    cs = __fadd_rn(cs, value);
+                    energy = __fadd_rn(energy, __fmul_rn(value, value));
+                } else if (pass == 1) {
+                    const float t = __fsub_rn(value, mean);
+                    cs = __fadd_rn(cs, __fmul_rn(t, t));
+                }
+            }
+        }
+    }
+    if (numAdds == 0) return 0.0f;
+    if (BF == SB_BF_DELAY_AND_STDDEV) return __fmul_rn(__fdiv_rn(__fsqrt_rn(cs), weightAcum), static_cast<float>(numAdds));
+    const float das = __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds));
+    return __fmul_rn(__fdiv_rn(__fdiv_rn(__fmul_rn(cs, cs), energy), static_cast<float>(numAdds)), das);
+}
+
+// RxSampleBeamformerTestSignal::sampleBeamform2D / 3D: the point back in mm (times dt times c), then
+// the distance to each cylinder axis in the plane normal to it.
+__device__ __forceinline__ float testSignal(const LineDT& s, float depth, float dt, float c, bool is3D) {
+    float px = __fadd_rn(s.x, __fmul_rn(s.dirX, depth));
+    float py = __fmul_rn(s.dirY, depth);
+    float pz = is3D ? __fadd_rn(s.z, __fmul_rn(s.dirZ, depth)) : __fmul_rn(s.dirZ, depth);
+    px = __fmul_rn(__fmul_rn(px, dt), c);
+    py = __fmul_rn(__fmul_rn(py, dt), c);
+    pz = __fmul_rn(__fmul_rn(pz, dt), c);
+    const float dy = __fsub_rn(py, 30.0f);
+    const float dy2 = __fmul_rn(dy, dy);
+    float sample = 0.0f;
+    for (int n = -3; n <= 3; n++) {  // cylinders along the elevation axis
+        const float dx = __fsub_rn(px, static_cast<float>(n) * 6.0f);
+        if (__fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), dy2), 0.0f)) <= 2.0f) sample = 1000.0f;
+    }
+    if (is3D) {
+        for (int n = -3; n <= 3; n++) {  // cylinders along x
+            const float dz = __fsub_rn(pz, static_cast<float>(n) * 6.0f);
+            if (__fsqrt_rn(__fadd_rn(__fadd_rn(0.0f, dy2), __fmul_rn(dz, dz))) <= 2.0f) sample = 1000.0f;
+        }
+    }
+    return sample;
+}
+
+template <typename RF, typename OUT, bool IS3D, int BF>
+__global__ void __launch_bounds__(256) dasVariantKernel(DasArgs a) {
+    __shared__ float lut[64];
+    if (threadIdx.x < 64) lut[threadIdx.x] = a.lut.v[threadIdx.x];
+    __syncthreads();
+    const uint32_t line = blockIdx.y;
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nD) return;
+    const LineDT s = a.lines[line];
+    const float d = __ldg(a.depth + r);
+    float aDT = apertureDT(d, a.dt, a.c, a.F);
+    float invX = 0.0f, invY = 0.0f;
+    if (IS3D) {
+        aDT = __fmul_rn(aDT, aDT);
+        const float sq = __fsqrt_rn(aDT);
+        invX = __fdiv_rn(1.0f, fminf(sq, s.maxDistX));
+        invY = __fdiv_rn(1.0f, fminf(sq, s.maxDistY));
+    } else {
+        invX = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+    }
+    float acc = 0.0f;
+    for (int k = 0; k < 4; k++) {
+        if (!a.interpTx && k != s.highest) continue;
+        if (!((s.activeMask >> k) & 1)) continue;
+        float v;
+        if (BF == SB_BF_TEST_SIGNAL) v = testSignal(s, d, a.dt, a.c, IS3D);
+        else if (IS3D) v = variant3D<RF, BF>(a, s, k, lut, aDT, d, invX, invY);
+        else v = variant2D<RF, BF>(a, s, k, lut, aDT, d, invX);
+        acc = a.interpTx ? __fadd_rn(acc, __fmul_rn(s.txWeight[k], v)) : __fadd_rn(acc, v);
+    }
+    static_cast<OUT*>(a.out)[line + static_cast<size_t>(r) * a.nRx] = clampCast<OUT>(acc);
+}
+
 // 3D delay-and-sum with a per-scanline element table in shared memory (highest-weight transmit).
 // The table keeps the reference's summation order (x outer, y inner, RxSampleBeamformerDelayAndSum.h:
 // 55-57), each element's position, offsets from the scanline and channel. Once the aperture covers
@@ -662,6 +851,45 @@ int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out,
     else SB_DAS_LAUNCH(float, int16_t);
 #undef SB_DAS_LAUNCH
     SB_CHECK_LAUNCH("dasKernel");
+    return SB_OK;
+}
+
+int sb_das_run_beamformer(const sb_das_plan* plan, int sample_beamformer, const void* rf, int rf_dtype, void* out,
+                          int out_dtype, double f_number, double speed_of_sound_mm_s, int window_type,
+                          float window_parameter, int interpolate_transmits, int32_t additional_offset, sb_stream stream) {
+    SB_REQUIRE(sample_beamformer >= SB_BF_DELAY_AND_SUM && sample_beamformer <= SB_BF_TEST_SIGNAL,
+               "sb_das_run_beamformer: sample beamformer %d not in [0, 3]", sample_beamformer);
+    if (sample_beamformer == SB_BF_DELAY_AND_SUM)
+        return sb_das_run(plan, rf, rf_dtype, out, out_dtype, f_number, speed_of_sound_mm_s, window_type,
+                          window_parameter, interpolate_transmits, additional_offset, stream);
+    SB_REQUIRE(plan && rf && out, "sb_das_run_beamformer: null argument");
+    SB_REQUIRE(rf_dtype == SB_INT16 || rf_dtype == SB_FLOAT32, "sb_das_run_beamformer: rf dtype %d unsupported", rf_dtype);
+    SB_REQUIRE(out_dtype == SB_FLOAT32 || out_dtype == SB_INT16, "sb_das_run_beamformer: out dtype %d unsupported", out_dtype);
+    sb_das_plan* p = const_cast<sb_das_plan*>(plan);
+    cudaStream_t st = S(stream);
+    DasArgs a;
+    int err = fillArgs(p, a, rf, out, f_number, speed_of_sound_mm_s, window_type, window_parameter,
+                       interpolate_transmits, additional_offset, st);
+    if (err != SB_OK) return err;
+    dim3 grid((p->numDepths + 255) / 256, p->numRx);
+#define SB_BF_LAUNCH(RFT, OUTT, BFV)                                                    \
+    do {                                                                                \
+        if (p->is3D) dasVariantKernel<RFT, OUTT, true, BFV><<<grid, 256, 0, st>>>(a);   \
+        else dasVariantKernel<RFT, OUTT, false, BFV><<<grid, 256, 0, st>>>(a);          \
+    } while (0)
+#define SB_BF_TYPES(BFV)                                                                \
+    do {                                                                                \
+        if (rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_BF_LAUNCH(int16_t, float, BFV); \
+        else if (rf_dtype == SB_INT16) SB_BF_LAUNCH(int16_t, int16_t, BFV);             \
+        else if (out_dtype == SB_FLOAT32) SB_BF_LAUNCH(float, float, BFV);              \
+        else SB_BF_LAUNCH(float, int16_t, BFV);                                         \
+    } while (0)
+    if (sample_beamformer == SB_BF_DELAY_AND_STDDEV) SB_BF_TYPES(SB_BF_DELAY_AND_STDDEV);
+    else if (sample_beamformer == SB_BF_COHERENCE_FACTOR_DAS) SB_BF_TYPES(SB_BF_COHERENCE_FACTOR_DAS);
+    else SB_BF_TYPES(SB_BF_TEST_SIGNAL);
+#undef SB_BF_TYPES
+#undef SB_BF_LAUNCH
+    SB_CHECK_LAUNCH("dasVariantKernel");
     return SB_OK;
 }
 

@@ -323,6 +323,11 @@ protected:
         m_windowParameter = c.getDouble("windowParameter");
         m_speedOfSoundMMperS = c.getDouble("speedOfSound") * 1000.0;
         m_beamformerType = c.get("beamformerType");
+        // BeamformingNode::updateImageProperties / configurationChanged (Beamformer/BeamformingNode.cpp:200-220)
+        m_beamformer = m_beamformerType == "DelayAndStdDev"               ? SB_BF_DELAY_AND_STDDEV
+                       : m_beamformerType == "CoherenceFactorDelayAndSum" ? SB_BF_COHERENCE_FACTOR_DAS
+                       : m_beamformerType == "TestSignal"                 ? SB_BF_TEST_SIGNAL
+                                                                          : SB_BF_DELAY_AND_SUM;
         m_interpolateTransmits = c.getBool("interpolateTransmits");
         m_additionalOffset = static_cast<int32_t>(c.getInt("additionalOffset"));
         m_outputType = c.getDataType("outputType");
@@ -332,7 +337,6 @@ protected:
         auto raw = std::static_pointer_cast<USRawData>(in);
         if (raw->properties && raw->properties->state != ImageProperties::State::Raw)
             return fail("input is not raw channel data");
-        if (m_beamformerType != "DelayAndSum") return fail("beamformer type " + m_beamformerType + " is not supported");
         if (raw->dtype != DataType::Int16 && raw->dtype != DataType::Float) return fail("input rawdata type not supported");
         sb_das_plan* plan = nullptr;
         int st = m_plans.get(raw->geometry, &plan);
@@ -340,9 +344,10 @@ protected:
         const sb_geometry& g = raw->geometry->g;
         auto out = deviceBuffer(static_cast<size_t>(g.num_depths) * g.num_rx * dtypeBytes(m_outputType), raw->stream);
         if (!out) return fail("device allocation failed");
-        st = sb_das_run(plan, raw->data.get(), static_cast<int>(raw->dtype), out.get(), static_cast<int>(m_outputType),
-                        m_fNumber, m_speedOfSoundMMperS, m_windowType, static_cast<float>(m_windowParameter),
-                        m_interpolateTransmits ? 1 : 0, m_additionalOffset, raw->stream);
+        st = sb_das_run_beamformer(plan, m_beamformer, raw->data.get(), static_cast<int>(raw->dtype), out.get(),
+                                   static_cast<int>(m_outputType), m_fNumber, m_speedOfSoundMMperS, m_windowType,
+                                   static_cast<float>(m_windowParameter), m_interpolateTransmits ? 1 : 0,
+                                   m_additionalOffset, raw->stream);
         if (st != SB_OK) return fail(statusMessage(st));
         auto img = std::make_shared<USImage>();
         img->size[0] = g.num_rx;
@@ -361,7 +366,7 @@ protected:
         p->specific["Beamformer.WindowType"] = std::to_string(m_windowType);
         p->specific["Beamformer.WindowParameter"] = fmtDouble(m_windowParameter);
         p->specific["Beamformer.RxSpeedOfSound"] = fmtDouble(m_speedOfSoundMMperS);
-        p->specific["Beamformer.BeamformerType"] = m_beamformerType;
+        p->specific["Beamformer.BeamformerType"] = std::to_string(m_beamformer);  // the enum, streamed
         p->specific["Beamformer.InterpolateTransmits"] = m_interpolateTransmits ? "1" : "0";
         img->properties = p;
         return img;
@@ -371,6 +376,7 @@ private:
     double m_fNumber = 1, m_windowParameter = 0, m_speedOfSoundMMperS = 1540e3;
     int m_windowType = 0;
     std::string m_beamformerType;
+    int m_beamformer = SB_BF_DELAY_AND_SUM;
     bool m_interpolateTransmits = false;
     int32_t m_additionalOffset = 0;
     DataType m_outputType = DataType::Float;

@@ -33,6 +33,12 @@ def small_matrix(num_samples=256):
                                  lines=(4, 4), aperture=(4, 4), focus_mm=15.0)
 
 
+def bf_geometries():
+    """Geometries of the sample-beamformer cases; the deep ones reach the test signal's 30 mm cylinders."""
+    return {"lin": small_linear(), "mat": small_matrix(), "lin_deep": small_linear(num_samples=2048),
+            "mat_deep": small_matrix(num_samples=1024)}
+
+
 def random_rf(geom, seed=0, dtype=np.int16, amp=3000):
     rng = np.random.Generator(np.random.PCG64(seed))
     x = rng.integers(-amp, amp + 1, size=(geom.num_tx, geom.num_channels, geom.num_samples))

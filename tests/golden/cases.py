@@ -7,3 +7,8 @@ DAS_CASES = [  # (geometry, f-number, window, window param, interpolate transmit
     ("lin", 1.0, 1, 0.0, 0, 0), ("lin", 0.7, 2, 0.1, 1, 3), ("lin", 2.0, 0, 0.0, 0, -2),
     ("mat", 1.0, 1, 0.0, 0, 0), ("mat", 1.5, 3, 0.5, 1, 1),
 ]
+DAS_BF_CASES = [  # (geometry, sample beamformer, f-number, window, window param, interpolate transmits, offset)
+    ("lin", 1, 1.0, 1, 0.0, 0, 0), ("lin", 2, 1.0, 1, 0.0, 0, 0), ("lin", 1, 0.7, 2, 0.1, 1, 3),
+    ("lin", 2, 2.0, 0, 0.0, 1, -2), ("mat", 1, 1.0, 1, 0.0, 0, 0), ("mat", 2, 1.5, 3, 0.5, 1, 1),
+    ("lin_deep", 3, 1.0, 1, 0.0, 0, 0), ("mat_deep", 3, 1.0, 1, 0.0, 1, 0), ("lin_deep", 1, 1.0, 1, 0.0, 0, 0),
+]

@@ -1,5 +1,6 @@
 """Regenerates tests/golden/ref_pins.npz from the reference's own code compiled in oracle/_ref
-(FirFilterFactory, WindowFunction, and the DAS per-sample reducers of RxSampleBeamformerDelayAndSum.h).
+(FirFilterFactory, WindowFunction, and the per-sample reducers of the four sample beamformers,
+RxSampleBeamformerDelayAndSum.h, ...DelayAndStdDev.h, ...CoherenceFactorDelayAndSum.h, ...TestSignal.h).
 
     make -C oracle ref && python tests/golden/make_golden.py
 
@@ -15,10 +16,10 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 sys.path.insert(0, os.path.dirname(HERE))
 sys.path.insert(0, HERE)
 
-from conftest import random_rf, small_linear, small_matrix  # noqa: E402
+from conftest import bf_geometries, random_rf, small_linear, small_matrix  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-from golden.cases import DAS_CASES, FIR_CASES, WIN_CASES  # noqa: E402
+from golden.cases import DAS_BF_CASES, DAS_CASES, FIR_CASES, WIN_CASES  # noqa: E402
 
 
 def main():
@@ -36,6 +37,12 @@ def main():
         rf = random_rf(g, seed=100 + i)  # regenerated from the seed by the test
         out[f"das_{i}"] = O.das(g, rf, F, window=w, window_param=wp, interp_tx=bool(itx), additional_offset=off,
                                 ref=True)
+    bgeoms = bf_geometries()
+    for i, (gname, bf, F, w, wp, itx, off) in enumerate(DAS_BF_CASES):
+        g = bgeoms[gname]
+        rf = random_rf(g, seed=200 + i)
+        out[f"dasbf_{i}"] = O.das_bf(g, rf, bf, F, window=w, window_param=wp, interp_tx=bool(itx),
+                                     additional_offset=off, ref=True)
     np.savez_compressed(os.path.join(HERE, "ref_pins.npz"), **out)
     print("wrote", os.path.join(HERE, "ref_pins.npz"))
 

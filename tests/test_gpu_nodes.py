@@ -42,10 +42,13 @@ def test_beamforming_node_equals_das(frame):
     ref16 = RxBeamformer(g).beamform(rf, 1.5, 1500e3, window_type=1, out_dtype=torch.int16)
     torch.cuda.synchronize()
     assert out16.dtype == torch.int16 and _eq(out16, ref16)
-    n.set("beamformerType", "CoherenceFactorDelayAndSum")
-    from supra_b200.abi import SupraError
-    with pytest.raises(SupraError):
-        n.process_raw(g, rf)
+    n.set("outputType", "float")
+    for name in ("CoherenceFactorDelayAndSum", "DelayAndStdDev", "TestSignal"):
+        n.set("beamformerType", name)
+        outv, _ = n.process_raw(g, rf)
+        refv = RxBeamformer(g).beamform(rf, 1.5, 1500e3, window_type=1, beamformer=name)
+        torch.cuda.synchronize()
+        assert _eq(outv, refv), name
 
 
 def test_envelope_log_scan_chain(frame):

@@ -5,7 +5,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import random_rf, small_linear, small_matrix
+from conftest import bf_geometries, random_rf, small_linear, small_matrix
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "ref_pins.npz")
 
@@ -51,6 +51,25 @@ def test_das_bit_exact_vs_reference(oracle, gold):
         ref[np.isnan(ref)] = -np.finfo(np.float32).max
         same = bits(got) == bits(ref)
         assert same.all(), f"DAS case {i}: {np.count_nonzero(~same)} differ"
+
+
+def test_sample_beamformers_bit_exact_vs_reference(oracle, gold):
+    """DelayAndStdDev, CoherenceFactorDelayAndSum and TestSignal (2D and 3D, highest-weight and
+    interpolated transmits) against the reference's own reducers."""
+    from golden.cases import DAS_BF_CASES as cases
+    geoms = bf_geometries()
+    for i, (gname, bf, F, w, wp, itx, off) in enumerate(cases):
+        g = geoms[gname]
+        rf = random_rf(g, seed=200 + i)
+        got = oracle.das_bf(g, rf, bf, F, window=w, window_param=wp, interp_tx=bool(itx), additional_offset=off)
+        ref = gold[f"dasbf_{i}"].copy()
+        ref[np.isnan(ref)] = -np.finfo(np.float32).max  # the GPU clampCast (see the DAS pin)
+        same = bits(got) == bits(ref)
+        assert same.all(), f"sample beamformer case {i}: {np.count_nonzero(~same)} differ"
+    # beamformer 0 is the delay-and-sum path
+    g = geoms["lin"]
+    rf = random_rf(g, seed=5)
+    assert np.array_equal(bits(oracle.das_bf(g, rf, 0)), bits(oracle.das(g, rf)))
 
 
 @pytest.mark.skipif(not os.path.isdir("/root/reference/src/SupraLib"), reason="reference sources not present")
