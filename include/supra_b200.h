@@ -144,6 +144,14 @@ int sb_das_run_beamformer(const sb_das_plan* plan, int sample_beamformer, const 
                           int out_dtype, double f_number, double speed_of_sound_mm_s, int window_type,
                           float window_parameter, int interpolate_transmits, int32_t additional_offset, sb_stream stream);
 
+/* TemporalFilter::filter (Beamformer/TemporalFilter.cu:48-110): out[i] = clampCast(sum_k w_k x_k[i] / sum_k w_k)
+ * over num_images device images of numel elements each (images[0] the oldest, the node's queue order),
+ * in float as the reference (weights given in double, converted to float; NULL = all 1, the node's
+ * weights). num_images in [1, 50]; in/out dtype SB_INT16 or SB_FLOAT32. images is a host array of
+ * device pointers. */
+int sb_temporal_filter_run(const void* const* images, uint32_t num_images, const double* weights, int in_dtype,
+                           void* out, int out_dtype, uint64_t numel, sb_stream stream);
+
 /* Allocation-free delay-and-sum, for callers that cannot allocate device memory: hosts that reserve
  * their whole device budget up front and hand out buffers from their own pool (as SUPRA's container
  * pool does), or real-time frame loops that cannot afford cudaMalloc/cudaFree (cudaFree synchronises
@@ -372,6 +380,13 @@ int sb_node_type_name(int index, char* name, size_t len);
 int sb_node_process_raw(sb_node* node, const sb_geometry* geometry, const void* data, int dtype, int delayed,
                         uint32_t num_tx, uint32_t num_channels, uint32_t num_samples, double depth_mm,
                         double image_resolution_mm, sb_stream stream, sb_record* out);
+/* Runs the node on a caller-owned device image (a USImage [size[2]][size[1]][size[0]], x fastest) in
+ * image state `state` (sb_record's codes); geometry (may be NULL) gives the scanline grid the scan
+ * converter needs. The data is borrowed: TemporalFilterNode keeps the pointers of its last numImages
+ * inputs and reads them again on its next calls, so they must stay valid while they are in its store. */
+int sb_node_process_image(sb_node* node, const sb_geometry* geometry, const void* data, int dtype, int state,
+                          const uint32_t size[3], double depth_mm, double image_resolution_mm, sb_stream stream,
+                          sb_record* out);
 /* Runs the node on the last output of `upstream`. */
 int sb_node_process_last(sb_node* node, sb_node* upstream, sb_record* out);
 

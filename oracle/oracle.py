@@ -141,6 +141,19 @@ def das_bf(geom, rf: np.ndarray, beamformer, f_number=1.0, c_mm_s=None, window=1
     return out.reshape(geom.num_depths, geom.num_rx)
 
 
+def temporal_filter(images, weights=None, out_dtype=np.float32) -> np.ndarray:
+    """TemporalFilter (float work type) over equally shaped images, oldest first."""
+    ims = [np.ascontiguousarray(im, dtype=np.float32).ravel() for im in images]
+    arr = (C.c_void_p * len(ims))(*[im.ctypes.data for im in ims])
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+    out = np.empty(ims[0].size, dtype=out_dtype)
+    code = {np.dtype(np.float32): 2, np.dtype(np.int16): 1}[np.dtype(out_dtype)]  # SB_FLOAT32, SB_INT16
+    st = lib().orc_temporal_filter(C.cast(arr, C.c_void_p), C.c_uint32(len(ims)), None if w is None else _vp(_p(w)),
+                                   C.c_uint64(ims[0].size), _vp(_p(out)), C.c_int(code))
+    assert st == 0
+    return out.reshape(np.shape(images[0]))
+
+
 def das_adjoint64(geom, rf: np.ndarray, apod, gout: np.ndarray, c_mm_s=None, f_number=1.0, window=1, window_param=0.0):
     """FP64 reference gradient of the apodised 2D DAS: (grad_rf, grad_apod, grad_c)."""
     g = geom.ctypes()

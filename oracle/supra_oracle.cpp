@@ -754,6 +754,25 @@ int orc_das_bf(const sb_geometry* g, const float* rf, float* out, double fNumber
     return 0;
 }
 
+// TemporalFilter::filter + temporalFilterKernel (BF/TemporalFilter.cu:22-46, WorkType float): per element
+// sum += w_k * x_k, sumWeights += w_k over the images in order, then sum / sumWeights, clampCast to
+// out_dtype (SB_FLOAT32 or SB_INT16; out holds that type). Images are given as float.
+int orc_temporal_filter(const float* const* images, uint32_t n, const double* weights, uint64_t numel, void* out,
+                        int out_dtype) {
+    if (!images || !out || n == 0) return -1;
+    for (uint64_t i = 0; i < numel; i++) {
+        float sum = 0.0f, sumWeights = 0.0f;
+        for (uint32_t k = 0; k < n; k++) {
+            float w = static_cast<float>(weights ? weights[k] : 1.0);
+            sum += w * images[k][i];
+            sumWeights += w;
+        }
+        sum /= sumWeights;
+        storeClamped(out, out_dtype, i, sum);
+    }
+    return 0;
+}
+
 // FP64 reference gradient of the apodised 2D DAS (extension without a reference counterpart): the
 // transpose of sampleBeamform2D<double> with apodisation (same discrete decisions: aperture, window
 // index, sample index), highest-weight transmit. For a pixel with upstream g, W_e = w_e a_e,

@@ -150,6 +150,7 @@ _SIGNATURES = {
     "sb_das_plan_destroy": (_int, [_vp]),
     "sb_das_run": (_int, [_vp, _vp, _int, _vp, _int, _f64, _f64, _int, _f32, _int, _i32, _vp]),
     "sb_das_run_beamformer": (_int, [_vp, _int, _vp, _int, _vp, _int, _f64, _f64, _int, _f32, _int, _i32, _vp]),
+    "sb_temporal_filter_run": (_int, [_vp, _u32, _vp, _int, _vp, _int, C.c_uint64, _vp]),
     "sb_das_run_static": (_int, [C.POINTER(sb_geometry), _vp, _int, _vp, _int, _f64, _f64, _int, _f32, _int, _i32,
                                  _vp]),
     "sb_rawdelay_run": (_int, [_vp, _vp, _int, _vp, _int, _f64, _f64, _int, _f32, _vp]),
@@ -192,6 +193,8 @@ _SIGNATURES = {
     "sb_node_process_raw": (_int, [_vp, C.POINTER(sb_geometry), _vp, _int, _int, _u32, _u32, _u32, _f64, _f64, _vp,
                                    C.POINTER(sb_record)]),
     "sb_node_process_last": (_int, [_vp, _vp, C.POINTER(sb_record)]),
+    "sb_node_process_image": (_int, [_vp, C.POINTER(sb_geometry), _vp, _int, _int, C.POINTER(_u32), _f64, _f64, _vp,
+                                     C.POINTER(sb_record)]),
     "sb_graph_create_xml": (_int, [C.c_char_p, C.POINTER(_vp)]),
     "sb_graph_destroy": (_int, [_vp]),
     "sb_graph_chain": (_int, [_vp, C.c_char_p, _sz]),

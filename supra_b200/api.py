@@ -297,6 +297,27 @@ class ScanConverter:
         return out
 
 
+def temporal_filter(images: Sequence[torch.Tensor], weights: Optional[Sequence[float]] = None,
+                    out_dtype=torch.float32, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """TemporalFilter::filter (Beamformer/TemporalFilter.cu:48-110): the weighted mean of equally shaped
+    images, images[0] the oldest; weights default to 1 (TemporalFilterNode's)."""
+    lib = load_library()
+    if not images:
+        raise ValueError("temporal_filter: no images")
+    shape, dt = images[0].shape, images[0].dtype
+    for im in images:
+        if im.shape != shape or im.dtype != dt or not im.is_contiguous():
+            raise ValueError("temporal_filter: images must be contiguous with one shape and dtype")
+    if out is None:
+        out = torch.empty(shape, dtype=out_dtype, device=images[0].device)
+    ptrs = (C.c_void_p * len(images))(*[im.data_ptr() for im in images])
+    w = None if weights is None else (C.c_double * len(images))(*[float(x) for x in weights])
+    check("sb_temporal_filter_run",
+          lib.sb_temporal_filter_run(C.cast(ptrs, C.c_void_p), len(images), None if w is None else C.cast(w, C.c_void_p),
+                                     dtype_code(images[0]), _ptr(out), dtype_code(out), images[0].numel(), _stream()))
+    return out
+
+
 def scan_tables_2d_host(scanlines: np.ndarray, layout_x: int, num_samples: int, depth_mm: float, resolution_mm: float):
     """Host-only 2D table build of the product (no GPU needed)."""
     lib = load_library()

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <deque>
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -721,6 +722,67 @@ private:
     DataType m_outputType = DataType::Float;
 };
 
+// ----------------------------------------------------------------- TemporalFilterNode
+// TemporalFilterNode (Beamformer/TemporalFilterNode.cpp:36-168): keeps the last numImages images of one
+// size and data type (a change of either empties the store) and outputs their mean, weights 1, oldest
+// first. "outputType" offers float and uint16 as the reference's dictionary does; the reference's filter
+// exists for int16 and float outputs only, so uint16 is refused ("Image output type not supported").
+class TemporalFilterNode : public AbstractNode {
+public:
+    explicit TemporalFilterNode(const std::string& id) : AbstractNode(id) {
+        auto& d = m_valueRangeDictionary;
+        d.setRange("numImages", "uint32_t", 1, 50, "3", "Number of Images");
+        d.setChoices("outputType", "DataType", {"float", "uint16"}, "float", "Output type");
+        finishConstruction();
+    }
+    const char* getType() const override { return "TemporalFilterNode"; }
+
+protected:
+    void configurationChanged() override {
+        m_numImages = static_cast<uint32_t>(m_configurationDictionary.getInt("numImages"));
+        m_outputType = m_configurationDictionary.getDataType("outputType");
+    }
+    std::shared_ptr<RecordObject> processLocked(const std::shared_ptr<RecordObject>& in) override {
+        if (in->getType() != RecordType::Image) return fail("input is not USImage");
+        auto im = std::static_pointer_cast<USImage>(in);
+        if (im->dtype != DataType::Int16 && im->dtype != DataType::Float) return fail("Image input type not supported");
+        if (!std::equal(im->size, im->size + 3, m_size) || im->dtype != m_dtype) {
+            std::copy(im->size, im->size + 3, m_size);
+            m_dtype = im->dtype;
+            m_stored.clear();
+        }
+        m_stored.push_back(im->data);
+        while (m_stored.size() > m_numImages) m_stored.pop_front();
+        if (m_outputType != DataType::Float && m_outputType != DataType::Int16)
+            return fail("Image output type not supported");
+        const size_t n = static_cast<size_t>(im->size[0]) * im->size[1] * std::max<uint32_t>(im->size[2], 1);
+        auto out = deviceBuffer(n * dtypeBytes(m_outputType), im->stream);
+        if (!out) return fail("device allocation failed");
+        std::vector<const void*> images;
+        for (const auto& d : m_stored) images.push_back(d.get());
+        const int st = sb_temporal_filter_run(images.data(), static_cast<uint32_t>(images.size()), nullptr,
+                                              static_cast<int>(m_dtype), out.get(), static_cast<int>(m_outputType), n,
+                                              im->stream);
+        if (st != SB_OK) return fail(statusMessage(st));
+        auto o = std::make_shared<USImage>();
+        std::copy(im->size, im->size + 3, o->size);
+        o->dtype = m_outputType;
+        o->data = out;
+        o->stream = im->stream;
+        auto p = derivedProperties(*im, im->properties ? im->properties->state : ImageProperties::State::RF);
+        p->specific["TemporalFilter.NumImages"] = std::to_string(m_numImages);
+        o->properties = p;
+        return o;
+    }
+
+private:
+    uint32_t m_numImages = 3;
+    DataType m_outputType = DataType::Float;
+    uint32_t m_size[3] = {0, 0, 0};
+    DataType m_dtype = DataType::Float;
+    std::deque<std::shared_ptr<void>> m_stored;  // the images' buffers, oldest first
+};
+
 // ------------------------------------------------------------------ ScanConverterNode
 class ScanConverterNode : public AbstractNode {
 public:
@@ -802,6 +864,7 @@ const std::vector<std::pair<std::string, Creator>>& creators() {
         {"IQDemodulatorNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new IQDemodulatorNode(id)); }},
         {"LogCompressorNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new LogCompressorNode(id)); }},
         {"ScanConverterNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new ScanConverterNode(id)); }},
+        {"TemporalFilterNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new TemporalFilterNode(id)); }},
     };
     return c;
 }
@@ -1126,6 +1189,32 @@ std::shared_ptr<RecordObject> recordFromRaw(std::shared_ptr<const Geometry>& cac
     return r;
 }
 
+// A caller-owned device image as a USImage record (state as in sb_record; geometry optional).
+std::shared_ptr<RecordObject> recordFromImage(std::shared_ptr<const Geometry>& cache, const sb_geometry* geometry,
+                                              const void* data, int dtype, int state, const uint32_t size[3],
+                                              double depth_mm, double image_resolution_mm, sb_stream stream) {
+    auto im = std::make_shared<USImage>();
+    im->data = std::shared_ptr<void>(const_cast<void*>(data), [](void*) {});  // caller-owned
+    im->dtype = static_cast<DataType>(dtype);
+    std::copy(size, size + 3, im->size);
+    if (im->size[2] == 0) im->size[2] = 1;
+    im->stream = stream;
+    auto p = std::make_shared<ImageProperties>();
+    p->state = static_cast<ImageProperties::State>(state);
+    if (geometry) {
+        p->geometry = geometryFor(cache, *geometry);
+        p->layoutX = geometry->rx_layout[0];
+        p->layoutY = geometry->rx_layout[1];
+        if (!(depth_mm > 0) && geometry->num_depths) depth_mm = geometry->depths_mm[geometry->num_depths - 1];
+    }
+    p->numScanlines = size[0];
+    p->numSamples = size[1];
+    p->depthMM = depth_mm > 0 ? depth_mm : 0.0;
+    p->imageResolutionMM = image_resolution_mm > 0 ? image_resolution_mm : 0.1;
+    im->properties = p;
+    return im;
+}
+
 void describe(const std::shared_ptr<RecordObject>& rec, sb_record* out) {
     std::memset(out, 0, sizeof(*out));
     if (!rec) return;
@@ -1224,6 +1313,18 @@ int sb_node_process_raw(sb_node* node, const sb_geometry* geometry, const void* 
     if (!node || !geometry || !data || !out) return nodeFail("sb_node_process_raw: null argument");
     auto rec = recordFromRaw(node->geometry, geometry, data, dtype, delayed, num_tx, num_channels, num_samples,
                              depth_mm, image_resolution_mm, stream);
+    node->last = node->node->process(rec);
+    if (!node->last) return nodeFail(node->node->lastError(), SB_ERR_UNSUPPORTED);
+    describe(node->last, out);
+    return SB_OK;
+}
+
+int sb_node_process_image(sb_node* node, const sb_geometry* geometry, const void* data, int dtype, int state,
+                          const uint32_t size[3], double depth_mm, double image_resolution_mm, sb_stream stream,
+                          sb_record* out) {
+    if (!node || !data || !size || !out) return nodeFail("sb_node_process_image: null argument");
+    if (state < 0 || state > 5) return nodeFail("sb_node_process_image: state not in [0, 5]", SB_ERR_INVALID_ARG);
+    auto rec = recordFromImage(node->geometry, geometry, data, dtype, state, size, depth_mm, image_resolution_mm, stream);
     node->last = node->node->process(rec);
     if (!node->last) return nodeFail(node->node->lastError(), SB_ERR_UNSUPPORTED);
     describe(node->last, out);

@@ -13,6 +13,7 @@ clone them to keep them.
 """
 from __future__ import annotations
 
+import collections
 import ctypes as C
 from typing import Dict, List, Optional
 
@@ -66,6 +67,7 @@ class Node:
         check("sb_node_create", self.lib.sb_node_create(node_type.encode(), node_id.encode(), C.byref(self._h)))
         self.type, self.id = node_type, node_id
         self._geometry_keep = None
+        self._inputs = collections.deque(maxlen=50)
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value:
@@ -105,6 +107,25 @@ class Node:
                                                                   float(geometry.depth_mm), float(image_resolution_mm),
                                                                   _stream(), C.byref(rec)))
         return _record_tensor(rec, data.device), STATES[rec.state]
+
+    def process_image(self, image: torch.Tensor, state: str = "rf", geometry=None, depth_mm: float = 0.0,
+                      image_resolution_mm: float = 0.1):
+        """Runs the node on a device image [(depth,) samples, scanlines] in image state `state`. The last
+        50 inputs are kept referenced here, since the C entry point borrows them (TemporalFilterNode
+        reads its stored images again on later calls)."""
+        if not image.is_contiguous() or image.dim() not in (2, 3):
+            raise ValueError("process_image: a contiguous 2D or 3D image")
+        size = (C.c_uint32 * 3)(image.shape[-1], image.shape[-2], image.shape[0] if image.dim() == 3 else 1)
+        g = None if geometry is None else geometry.ctypes()
+        if g is not None:
+            self._geometry_keep = g
+        self._inputs.append(image)
+        rec = sb_record()
+        check("sb_node_process_image",
+              self.lib.sb_node_process_image(self._h, None if g is None else C.byref(g), _ptr(image), dtype_code(image),
+                                             STATES.index(state), size, float(depth_mm), float(image_resolution_mm),
+                                             _stream(), C.byref(rec)))
+        return _record_tensor(rec, image.device), STATES[rec.state]
 
     def process_after(self, upstream: "Node", device="cuda"):
         rec = sb_record()

@@ -21,6 +21,7 @@ NODES = {
     "IQDemodulatorNode": "IQDemodulatorNode.cpp",
     "LogCompressorNode": "LogCompressorNode.cpp",
     "ScanConverterNode": "ScanConverterNode.cpp",
+    "TemporalFilterNode": "TemporalFilterNode.cpp",
 }
 DTYPES = {"TypeFloat": "float", "TypeInt16": "int16", "TypeUint8": "uint8", "TypeUint16": "uint16"}
 CALL = re.compile(r'm_valueRangeDictionary\.set<\s*(\w+)\s*>\((.*)\);')

@@ -79,6 +79,7 @@ CONFIG = """<?xml version="1.0"?>
         <param name="windowParameter" type="double">0.5</param>
         <param name="speedOfSound" type="double">1500</param>
       </node>
+      <node type="TimeGainCompensationNode" id="TGC"/>
       <node type="TemporalFilterNode" id="FILT"/>
       <node type="HilbertFirEnvelopeNode" id="ENV">
         <param name="filterLength" type="uint32_t">64</param>
@@ -96,7 +97,8 @@ CONFIG = """<?xml version="1.0"?>
   </devices>
   <connections>
     <connection><from id="SRC" port="0"/><to id="BEAM" port="0"/></connection>
-    <connection><from id="BEAM" port="0"/><to id="FILT" port="0"/></connection>
+    <connection><from id="BEAM" port="0"/><to id="TGC" port="0"/></connection>
+    <connection><from id="TGC" port="0"/><to id="FILT" port="0"/></connection>
     <connection><from id="FILT" port="0"/><to id="ENV" port="0"/></connection>
     <connection><from id="ENV" port="0"/><to id="LOGC" port="0"/></connection>
     <connection><from id="LOGC" port="0"/><to id="SCAN" port="0"/></connection>
@@ -109,7 +111,9 @@ CONFIG = """<?xml version="1.0"?>
 def test_graph_from_xml():
     from supra_b200.nodes import Graph
     g = Graph(CONFIG)
-    assert g.chain() == ["BEAM", "ENV", "LOGC", "SCAN"]  # TemporalFilterNode is outside the receive path
+    # TimeGainCompensationNode (post-processing) is not built: bypassed
+    assert g.chain() == ["BEAM", "FILT", "ENV", "LOGC", "SCAN"]
+    assert g.get("FILT", "numImages") == "3"
     assert g.get("BEAM", "windowType") == "Hamming"
     assert float(g.get("BEAM", "speedOfSound")) == 1500.0
     assert g.get("ENV", "filterLength") == "64"
