@@ -152,6 +152,36 @@ int sb_das_run_beamformer(const sb_das_plan* plan, int sample_beamformer, const 
 int sb_temporal_filter_run(const void* const* images, uint32_t num_images, const double* weights, int in_dtype,
                            void* out, int out_dtype, uint64_t numel, sb_stream stream);
 
+/* ---- Recorded raw data (SUPRA's mock format) ------------------------------------------------------
+ * Metadata: RxBeamformerParameters::readMetaDataForMock / writeMetaDataForMock
+ * (Beamformer/RxBeamformerParameters.cpp:93-450), ".mock" (ASCII) or ".json" by suffix, parsed with the
+ * reference's number types (float fields as float, the JSON depths derived from depth and rxNumDepths).
+ * Frames: UltrasoundInterfaceRawDataMock (SupraLib/InputOutput/UltrasoundInterfaceRawDataMock.cpp:47-204),
+ * int16 [num_tx][num_channels][num_samples] frames back to back in each data file. */
+typedef struct sb_mock_meta sb_mock_meta;
+typedef struct sb_mock_reader sb_mock_reader;
+
+int sb_mock_meta_read(const char* filename, sb_mock_meta** meta);
+int sb_mock_meta_destroy(sb_mock_meta* meta);
+/* The geometry of the metadata (pointers into `meta`, valid until it is destroyed; no channel map). */
+int sb_mock_meta_geometry(const sb_mock_meta* meta, sb_geometry* geometry, double* depth_mm,
+                          double* speed_of_sound_mm_s);
+/* writeMetaDataForMock: the JSON metadata of a geometry (element positions, scanlines, sizes, depth). */
+int sb_mock_write_json(const char* filename, const sb_geometry* geometry, double depth_mm, double speed_of_sound_mm_s);
+/* A replay of the frame files (comma-separated names, as the node parameter "mockDataFilename"): frames
+ * in file order, file after file, wrapping; stream_sequence_once ends after the last frame of the last
+ * file; single_image repeats the first frame. A reader thread fills page-locked buffers ahead. */
+int sb_mock_reader_create(const sb_mock_meta* meta, const char* data_filenames, int single_image,
+                          int stream_sequence_once, sb_mock_reader** reader);
+/* Frame bytes, number of files and frames per file (sequence_lengths holds num_sequences entries). */
+int sb_mock_reader_info(const sb_mock_reader* reader, uint64_t* frame_bytes, uint32_t* num_sequences,
+                        uint64_t* sequence_lengths);
+/* Copies the next frame into device_frame (frame_bytes, device memory) on `stream` (asynchronous:
+ * one cudaMemcpyAsync from a page-locked buffer). *last_frame = 1 for the final frame of a
+ * stream-once replay; later calls fail. */
+int sb_mock_reader_next(sb_mock_reader* reader, void* device_frame, sb_stream stream, int* last_frame);
+int sb_mock_reader_destroy(sb_mock_reader* reader);
+
 /* Allocation-free delay-and-sum, for callers that cannot allocate device memory: hosts that reserve
  * their whole device budget up front and hand out buffers from their own pool (as SUPRA's container
  * pool does), or real-time frame loops that cannot afford cudaMalloc/cudaFree (cudaFree synchronises
@@ -400,6 +430,12 @@ int sb_graph_node_get_param(const sb_graph* graph, const char* node_id, const ch
 int sb_graph_process_raw(sb_graph* graph, const sb_geometry* geometry, const void* data, int dtype, uint32_t num_tx,
                          uint32_t num_channels, uint32_t num_samples, double depth_mm, double image_resolution_mm,
                          sb_stream stream, sb_record* out);
+/* For a configuration whose input is UltrasoundInterfaceRawDataMock: the first call opens its
+ * mockMetaDataFilename and mockDataFilename (singleImage, streamSequenceOnce as configured); each
+ * call copies the next recorded frame to the device and pushes it through the chain. *last_frame = 1
+ * on the final frame of a stream-once replay. */
+int sb_graph_process_next(sb_graph* graph, double image_resolution_mm, sb_stream stream, int* last_frame,
+                          sb_record* out);
 
 #ifdef __cplusplus
 }

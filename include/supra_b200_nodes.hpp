@@ -173,10 +173,18 @@ public:
     const std::vector<std::string>& skippedNodes() const { return m_skipped; }
     // Pushes `in` from the first node after the input through the chain; returns the last output.
     std::shared_ptr<RecordObject> process(const std::shared_ptr<RecordObject>& in, std::string* error);
+    const std::string& inputType() const { return m_inputType; }
+    // a parameter of the first input ("" if absent)
+    std::string inputParam(const std::string& name) const {
+        auto it = m_inputParams.find(name);
+        return it == m_inputParams.end() ? std::string() : it->second;
+    }
 
 private:
     std::map<std::string, std::unique_ptr<AbstractNode>> m_nodes;
     std::vector<std::string> m_chain, m_skipped;
+    std::string m_inputType;                            // type of the first <input>
+    std::map<std::string, std::string> m_inputParams;  // its <param> values
 };
 
 }  // namespace supra_b200

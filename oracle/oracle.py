@@ -154,6 +154,31 @@ def temporal_filter(images, weights=None, out_dtype=np.float32) -> np.ndarray:
     return out.reshape(np.shape(images[0]))
 
 
+def ref_mock_write(filename: str, geom, ascii_format: bool = False) -> None:
+    """The reference's mock metadata for a geometry: writeMetaDataForMock (JSON) or, for the ASCII
+    layout, the reference's scanline stream operator (oracle/_ref)."""
+    g = geom.ctypes()
+    fn = ref_lib().ref_mock_write_ascii if ascii_format else ref_lib().ref_mock_write_json
+    assert fn(filename.encode(), C.byref(g), C.c_double(geom.depth_mm), C.c_double(geom.speed_of_sound_mm_s)) == 0
+
+
+def ref_mock_read(filename: str, max_lines=4096, max_depths=65536, max_elems=65536) -> dict:
+    """readMetaDataForMock of the reference (oracle/_ref): sizes, values and arrays."""
+    from supra_b200.abi import SCANLINE_DTYPE
+    sizes = np.zeros(9, np.uint64)
+    vals = np.zeros(3, np.float64)
+    lines = np.zeros(max_lines, SCANLINE_DTYPE)
+    depths = np.zeros(max_depths, np.float32)
+    xs = np.zeros(max_elems, np.float32)
+    ys = np.zeros(max_elems, np.float32)
+    st = ref_lib().ref_mock_read(filename.encode(), _vp(_p(sizes)), _vp(_p(vals)), _vp(_p(lines)), _vp(_p(depths)),
+                                 _vp(_p(xs)), _vp(_p(ys)), C.c_uint64(max_lines), C.c_uint64(max_depths),
+                                 C.c_uint64(max_elems))
+    assert st == 0, "reference reader failed"
+    nE, nD, nL = int(sizes[0]), int(sizes[8]), int(sizes[6] * sizes[7])
+    return {"sizes": sizes, "vals": vals, "lines": lines[:nL], "depths": depths[:nD], "xs": xs[:nE], "ys": ys[:nE]}
+
+
 def das_adjoint64(geom, rf: np.ndarray, apod, gout: np.ndarray, c_mm_s=None, f_number=1.0, window=1, window_param=0.0):
     """FP64 reference gradient of the apodised 2D DAS: (grad_rf, grad_apod, grad_c)."""
     g = geom.ctypes()

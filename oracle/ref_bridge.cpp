@@ -11,7 +11,9 @@
 //   - the per-sample reducers sampleBeamform2D / sampleBeamform3D of the four sample beamformers
 //     (DelayAndSum, DelayAndStdDev, CoherenceFactorDelayAndSum, TestSignal), called exactly as the
 //     kernels rxBeamformingDTSPACEKernel / rxBeamformingDTSPACE3DKernel call them
-//     (RxBeamformerCuda.cu:238-323 and :119-228, one (line, depth) at a time).
+//     (RxBeamformerCuda.cu:238-323 and :119-228, one (line, depth) at a time),
+//   - the mock metadata reader RxBeamformerParameters::readMetaDataForMock and the JSON writer
+//     writeMetaDataForMock (Beamformer/RxBeamformerParameters.cpp:93-450, with the vendored jsoncpp).
 // ================================================================================================
 #include <math.h>    // brings the float overloads of abs() into the global namespace
 #include <stdlib.h>
@@ -35,6 +37,12 @@ template <typename T> constexpr inline T squ(const T& x) { return x * x; }
 #include "RxSampleBeamformerDelayAndStdDev.h"
 #include "RxSampleBeamformerCoherenceFactorDelayAndSum.h"
 #include "RxSampleBeamformerTestSignal.h"
+#include "RxBeamformerParameters.h"
+#include "USRawData.h"
+
+#include <cstring>
+#include <fstream>
+#include <iomanip>
 
 #include "supra_b200.h"
 
@@ -161,6 +169,86 @@ int ref_das(const sb_geometry* g, const float* rf, float* out, double fNumber, d
             int windowType, float windowParameter, int interpolateTransmits, int32_t additionalOffset) {
     return refDas<RxSampleBeamformerDelayAndSum>(g, rf, out, fNumber, speedOfSoundMMperS, windowType, windowParameter,
                                                  interpolateTransmits, additionalOffset);
+}
+
+// The reference's JSON mock metadata for a geometry (writeMetaDataForMock).
+int ref_mock_write_json(const char* filename, const sb_geometry* g, double depth, double speedOfSoundMMperS) {
+    std::vector<ScanlineRxParameters3D> lines(g->num_rx);
+    std::memcpy(lines.data(), g->scanlines, g->num_rx * sizeof(sb_scanline_rx));
+    std::vector<float> depths(g->depths_mm, g->depths_mm + g->num_depths);
+    std::vector<float> xs(g->element_x_mm, g->element_x_mm + g->num_elements);
+    std::vector<float> ys(g->element_y_mm, g->element_y_mm + g->num_elements);
+    auto params = std::make_shared<RxBeamformerParameters>(g->num_rx, vec2s{g->rx_layout[0], g->rx_layout[1]},
+                                                           speedOfSoundMMperS, depths, lines, xs, ys, g->num_depths);
+    auto props = std::make_shared<USImageProperties>(vec2s{g->num_tx, 1}, g->num_depths, USImageProperties::ImageType::BMode,
+                                                     USImageProperties::ImageState::Raw,
+                                                     USImageProperties::TransducerType::Linear, depth);
+    auto raw = std::make_shared<USRawData>(g->num_tx, g->num_elements, vec2s{g->element_layout[0], g->element_layout[1]},
+                                           g->num_channels, g->num_samples, g->sampling_frequency_hz, nullptr, params,
+                                           props, 0, 0);
+    params->writeMetaDataForMock(filename, raw);
+    return 0;
+}
+
+// An ASCII mock file in the layout readMetaDataForMockAscii reads, scanlines written with the
+// reference's operator<< (SupraLib/USImageProperties.cpp:38-59).
+int ref_mock_write_ascii(const char* filename, const sb_geometry* g, double depth, double speedOfSoundMMperS) {
+    std::ofstream f(filename);
+    f << "rawDataMockMetadata v 1\n";
+    f << g->num_elements << " " << g->element_layout[0] << " " << g->element_layout[1] << " " << g->num_channels << " "
+      << g->num_samples << " " << g->num_tx << " " << g->rx_layout[0] << " " << g->rx_layout[1] << " "
+      << std::setprecision(17) << depth << " " << g->sampling_frequency_hz << " " << g->num_depths << " "
+      << speedOfSoundMMperS << "\n";
+    for (uint32_t i = 0; i < g->num_rx; i++) {
+        ScanlineRxParameters3D p;
+        std::memcpy(&p, &g->scanlines[i], sizeof(p));
+        f << p << "\n";
+    }
+    f << std::setprecision(9);
+    for (uint32_t i = 0; i < g->num_depths; i++) f << g->depths_mm[i] << " ";
+    f << "\n";
+    for (uint32_t i = 0; i < g->num_elements; i++) f << g->element_x_mm[i] << " ";
+    f << "\n";
+    for (uint32_t i = 0; i < g->num_elements; i++) f << g->element_y_mm[i] << " ";
+    f << "\n";
+    return f.good() ? 0 : -1;
+}
+
+// readMetaDataForMock of the reference: sizes[9] = numElements, elementLayout x/y, numReceivedChannels,
+// numSamples, numTxScanlines, scanlineLayout x/y, rxNumDepths; vals[3] = depth, samplingFrequency,
+// speedOfSoundMMperS; arrays filled up to their capacities. Returns -1 on a reader exception.
+int ref_mock_read(const char* filename, uint64_t* sizes, double* vals, sb_scanline_rx* lines, float* depths, float* xs,
+                  float* ys, uint64_t capLines, uint64_t capDepths, uint64_t capElems) {
+    std::shared_ptr<USRawData> raw;
+    try {
+        raw = RxBeamformerParameters::readMetaDataForMock(filename);
+    } catch (...) {
+        return -1;
+    }
+    auto p = raw->getRxBeamformerParameters();
+    sizes[0] = raw->getNumElements();
+    sizes[1] = raw->getElementLayout().x;
+    sizes[2] = raw->getElementLayout().y;
+    sizes[3] = raw->getNumReceivedChannels();
+    sizes[4] = raw->getNumSamples();
+    sizes[5] = raw->getNumScanlines();
+    sizes[6] = p->getRxScanlineLayout().x;
+    sizes[7] = p->getRxScanlineLayout().y;
+    sizes[8] = p->getRxNumDepths();
+    vals[0] = raw->getImageProperties()->getDepth();
+    vals[1] = raw->getSamplingFrequency();
+    vals[2] = p->getSpeedOfSoundMMperS();
+    const auto& L = p->getRxScanlines();
+    for (size_t i = 0; i < L.size() && i < capLines; i++) std::memcpy(&lines[i], &L[i], sizeof(sb_scanline_rx));
+    const auto& D = p->getRxDepths();
+    for (size_t i = 0; i < D.size() && i < capDepths; i++) depths[i] = D[i];
+    const auto& X = p->getRxElementXs();
+    const auto& Y = p->getRxElementYs();
+    for (size_t i = 0; i < X.size() && i < capElems; i++) {
+        xs[i] = X[i];
+        ys[i] = Y[i];
+    }
+    return 0;
 }
 
 // beamformer: the order of RxBeamformerCuda::RxSampleBeamformer (RxBeamformerCuda.h:31-36).

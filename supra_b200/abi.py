@@ -193,6 +193,15 @@ _SIGNATURES = {
     "sb_node_process_raw": (_int, [_vp, C.POINTER(sb_geometry), _vp, _int, _int, _u32, _u32, _u32, _f64, _f64, _vp,
                                    C.POINTER(sb_record)]),
     "sb_node_process_last": (_int, [_vp, _vp, C.POINTER(sb_record)]),
+    "sb_graph_process_next": (_int, [_vp, _f64, _vp, C.POINTER(_int), C.POINTER(sb_record)]),
+    "sb_mock_meta_read": (_int, [C.c_char_p, C.POINTER(_vp)]),
+    "sb_mock_meta_destroy": (_int, [_vp]),
+    "sb_mock_meta_geometry": (_int, [_vp, C.POINTER(sb_geometry), C.POINTER(_f64), C.POINTER(_f64)]),
+    "sb_mock_write_json": (_int, [C.c_char_p, C.POINTER(sb_geometry), _f64, _f64]),
+    "sb_mock_reader_create": (_int, [_vp, C.c_char_p, _int, _int, C.POINTER(_vp)]),
+    "sb_mock_reader_info": (_int, [_vp, C.POINTER(C.c_uint64), C.POINTER(_u32), C.POINTER(C.c_uint64)]),
+    "sb_mock_reader_next": (_int, [_vp, _vp, _vp, C.POINTER(_int)]),
+    "sb_mock_reader_destroy": (_int, [_vp]),
     "sb_node_process_image": (_int, [_vp, C.POINTER(sb_geometry), _vp, _int, _int, C.POINTER(_u32), _f64, _f64, _vp,
                                      C.POINTER(sb_record)]),
     "sb_graph_create_xml": (_int, [C.c_char_p, C.POINTER(_vp)]),

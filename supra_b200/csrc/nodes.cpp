@@ -1056,7 +1056,14 @@ std::unique_ptr<Graph> Graph::fromXml(const std::string& xml, std::string* error
     const XmlNode* devices = root->first("devices");
     if (devices) {
         if (const XmlNode* ins = devices->first("inputs"))
-            for (const XmlNode* i : ins->all("input")) inputs.push_back(i->attrs.count("id") ? i->attrs.at("id") : "");
+            for (const XmlNode* i : ins->all("input")) {
+                inputs.push_back(i->attrs.count("id") ? i->attrs.at("id") : "");
+                if (inputs.size() == 1) {  // the first input's type and parameters (a recorded-data input is replayed)
+                    g->m_inputType = i->attrs.count("type") ? i->attrs.at("type") : "";
+                    for (const XmlNode* p : i->all("param"))
+                        if (p->attrs.count("name")) g->m_inputParams[p->attrs.at("name")] = trim(p->text);
+                }
+            }
         if (const XmlNode* nodes = devices->first("nodes")) {
             for (const XmlNode* n : nodes->all("node")) {
                 const std::string type = n->attrs.count("type") ? n->attrs.at("type") : "";
@@ -1130,6 +1137,16 @@ struct sb_graph {
     std::unique_ptr<Graph> graph;
     std::shared_ptr<RecordObject> last;
     std::shared_ptr<const Geometry> geometry;
+    // replay of a recorded-data input (UltrasoundInterfaceRawDataMock)
+    sb_mock_meta* meta = nullptr;
+    sb_mock_reader* reader = nullptr;
+    void* frame = nullptr;  // device frame buffer, reused frame after frame on the caller's stream
+    ~sb_graph() {
+        last.reset();
+        sb_mock_reader_destroy(reader);
+        sb_mock_meta_destroy(meta);
+        if (frame) cudaFree(frame);  // cudaFree waits for the work that may still read it
+    }
 };
 
 namespace {
@@ -1382,6 +1399,50 @@ int sb_graph_process_raw(sb_graph* graph, const sb_geometry* geometry, const voi
     graph->last = graph->graph->process(rec, &err);
     if (!graph->last) return nodeFail("sb_graph_process_raw: " + err, SB_ERR_UNSUPPORTED);
     describe(graph->last, out);
+    return SB_OK;
+}
+
+int sb_graph_process_next(sb_graph* graph, double image_resolution_mm, sb_stream stream, int* last_frame,
+                          sb_record* out) {
+    if (!graph || !out) return nodeFail("sb_graph_process_next: null argument");
+    if (last_frame) *last_frame = 0;
+    Graph& G = *graph->graph;
+    if (G.inputType() != "UltrasoundInterfaceRawDataMock")
+        return nodeFail("sb_graph_process_next: the configuration's input is " +
+                        (G.inputType().empty() ? std::string("missing") : G.inputType()) +
+                        ", not UltrasoundInterfaceRawDataMock");
+    if (!graph->reader) {
+        // UltrasoundInterfaceRawDataMock::initializeDevice (SupraLib/InputOutput/UltrasoundInterfaceRawDataMock.cpp:47-92)
+        auto flag = [&](const char* k) {
+            const std::string v = G.inputParam(k);
+            return v == "1" || v == "true";
+        };
+        int st = sb_mock_meta_read(G.inputParam("mockMetaDataFilename").c_str(), &graph->meta);
+        if (st != SB_OK) return st;
+        st = sb_mock_reader_create(graph->meta, G.inputParam("mockDataFilename").c_str(), flag("singleImage") ? 1 : 0,
+                                   flag("streamSequenceOnce") ? 1 : 0, &graph->reader);
+        if (st != SB_OK) return st;
+        uint64_t bytes = 0;
+        sb_mock_reader_info(graph->reader, &bytes, nullptr, nullptr);
+        const cudaError_t e = cudaMalloc(&graph->frame, bytes);
+        if (e != cudaSuccess) {
+            graph->frame = nullptr;
+            return nodeFail(std::string("sb_graph_process_next: frame buffer: ") + cudaGetErrorString(e), SB_ERR_NO_MEMORY);
+        }
+    }
+    int last = 0;
+    int st = sb_mock_reader_next(graph->reader, graph->frame, stream, &last);
+    if (st != SB_OK) return st;
+    sb_geometry g;
+    double depth = 0.0, c = 0.0;
+    sb_mock_meta_geometry(graph->meta, &g, &depth, &c);
+    auto rec = recordFromRaw(graph->geometry, &g, graph->frame, SB_INT16, 0, g.num_tx, g.num_channels, g.num_samples,
+                             depth, image_resolution_mm, stream);
+    std::string err;
+    graph->last = G.process(rec, &err);
+    if (!graph->last) return nodeFail("sb_graph_process_next: " + err, SB_ERR_UNSUPPORTED);
+    describe(graph->last, out);
+    if (last_frame) *last_frame = last;
     return SB_OK;
 }
 

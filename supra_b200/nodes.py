@@ -156,6 +156,15 @@ class Graph:
                                                                           buf, 256))
         return buf.value.decode()
 
+    def process_next(self, image_resolution_mm: float = 0.1, device="cuda"):
+        """Next frame of the configuration's UltrasoundInterfaceRawDataMock input through the chain:
+        (output tensor, state, last_frame)."""
+        rec = sb_record()
+        last = C.c_int(0)
+        check("sb_graph_process_next", self.lib.sb_graph_process_next(self._h, float(image_resolution_mm), _stream(),
+                                                                      C.byref(last), C.byref(rec)))
+        return _record_tensor(rec, device), STATES[rec.state], bool(last.value)
+
     def process_raw(self, geometry, rf: torch.Tensor, image_resolution_mm: float = 0.1):
         g = geometry.ctypes()
         self._geometry_keep = g
