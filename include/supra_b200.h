@@ -304,6 +304,17 @@ int sb_mv_run(const void* raw_delayed, int in_dtype, void* out, int out_dtype, u
               double subarray_scaling_power, int compute_means, float loading_scale, float fp64_threshold,
               sb_mv_stats* stats_host, sb_stream stream);
 
+/* Replaces RxBeamformerMVpcg::performRxBeamforming (Beamformer/RxBeamformerMVpcg.cu:622-800): the same
+ * covariance, smoothing (over +-temporal_smoothing samples clipped only at the record ends: no
+ * 2000-sample blocks), loading and weighting as sb_mv_run, with R a = 1 solved by Jacobi-preconditioned
+ * conjugate gradients from a = 1 (residual recomputed every iteration) for max_iterations_override
+ * iterations (0: subarray size) or until |r| <= convergence_threshold (BeamformingMVpcgNode passes
+ * 10^convergenceThresholdExponent). Real data only (SB_FLOAT32 / SB_INT16 in and out). */
+int sb_mv_pcg_run(const void* raw_delayed, int in_dtype, void* out, int out_dtype, uint32_t num_scanlines,
+                  uint32_t num_channels, uint32_t num_samples, uint32_t subarray_size, uint32_t temporal_smoothing,
+                  uint32_t max_iterations_override, double convergence_threshold, double subarray_scaling_power,
+                  int compute_means, float loading_scale, sb_stream stream);
+
 /* ---------------------------------------------------------------- batched, graph-captured DAS + IQ */
 
 typedef struct sb_batch_plan sb_batch_plan;

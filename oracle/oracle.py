@@ -286,6 +286,22 @@ def scan_apply(x: np.ndarray, lx: int, ly: int, tables: dict, out_dtype=np.uint8
     return out.reshape(size[2], size[1], size[0])
 
 
+def mv_pcg(raw: np.ndarray, L: int, T: int, max_iterations=0, threshold=1e-4, scaling_power=1.5, loading_scale=1.0,
+           precision=32, threads=None) -> np.ndarray:
+    """RxBeamformerMVpcg on real raw [nRx][nCh][nS] float32 (PCG in float for precision 32, double for
+    64); returns [nS][nRx]."""
+    nRx, nCh, nS = raw.shape
+    r = np.ascontiguousarray(raw, np.float32)
+    dt = np.float64 if precision == 64 else np.float32
+    out = np.zeros(nS * nRx, dt)
+    o32, o64 = (None, _vp(_p(out))) if precision == 64 else (_vp(_p(out)), None)
+    st = lib().orc_mv_pcg(_vp(_p(r)), o32, o64, C.c_uint32(nRx), C.c_uint32(nCh), C.c_uint32(nS), C.c_uint32(L),
+                          C.c_uint32(T), C.c_double(scaling_power), C.c_float(loading_scale), C.c_uint32(max_iterations),
+                          C.c_double(threshold), C.c_int(precision), C.c_int(threads or nthreads()))
+    assert st == 0
+    return out.reshape(nS, nRx)
+
+
 def mv(raw: np.ndarray, L: int, T: int, scaling_power=1.5, loading_scale=1.0, precision=32, block=2000,
        threads=None) -> np.ndarray:
     """raw [nRx][nCh][nS] float32 (real) or complex64; returns [nS][nRx]."""

@@ -328,9 +328,60 @@ int orc_scan_apply(const float* in, uint32_t lx, uint32_t ly, uint32_t numSample
 // the reference reads them at depth - 2000 from out-of-range buffers, quirk Q4).
 // precision 32: covariance and weighting in float, solve in double. 64: everything double.
 // Complex data (iscomplex = 1, interleaved): R = sum x x^H, y = sum_v conj(a_v) xbar_v / (Re sum a ...).
-int orc_mv(const float* raw, int iscomplex, float* outF, double* outD, uint32_t nRx, uint32_t nCh, uint32_t nS,
-           uint32_t L, uint32_t T, double scalingPower, float loadingScale, int precision, uint32_t blockSize,
-           int nthreads) {
+}  // extern "C"
+
+// solveBlockwisePCGJacobi (BF/RxBeamformerMVpcg.cu:450-546) in working precision W on the leading
+// sz x sz block of R (row-major, pitch L), right-hand side 1; the solution goes to a[0..sz).
+template <typename W>
+void pcgSolve(const std::vector<std::complex<double>>& R, uint32_t L, uint32_t sz, uint32_t maxIt, double thr,
+              std::vector<std::complex<double>>& a) {
+    std::vector<W> x(sz, W(1)), r(sz), d(sz), q(sz), t(sz), sv(sz), A(static_cast<size_t>(sz) * sz);
+    for (uint32_t i = 0; i < sz; i++)
+        for (uint32_t j = 0; j < sz; j++) A[i * sz + j] = static_cast<W>(R[i * L + j].real());
+    auto matvec = [&](const std::vector<W>& v, std::vector<W>& o) {
+        for (uint32_t i = 0; i < sz; i++) {
+            W acc = 0;
+            for (uint32_t j = 0; j < sz; j++) acc += A[i * sz + j] * v[j];
+            o[i] = acc;
+        }
+    };
+    auto dot = [&](const std::vector<W>& u, const std::vector<W>& w) {
+        W acc = 0;
+        for (uint32_t i = 0; i < sz; i++) acc += u[i] * w[i];
+        return acc;
+    };
+    matvec(x, t);
+    for (uint32_t i = 0; i < sz; i++) {
+        r[i] = W(-1) * t[i] + W(1);
+        d[i] = r[i] / A[i * sz + i];
+    }
+    W deltaNew = dot(r, d);
+    W residualNorm = W(2) * static_cast<W>(thr);
+    for (uint32_t it = 0; it < maxIt && static_cast<double>(deltaNew) > 1e-30 && residualNorm > static_cast<W>(thr); it++) {
+        matvec(d, q);
+        const W alpha = deltaNew / dot(d, q);
+        for (uint32_t i = 0; i < sz; i++) x[i] = alpha * d[i] + x[i];
+        matvec(x, t);
+        for (uint32_t i = 0; i < sz; i++) r[i] = W(-1) * t[i] + W(1);
+        residualNorm = std::sqrt(dot(r, r));
+        for (uint32_t i = 0; i < sz; i++) sv[i] = r[i] / A[i * sz + i];
+        const W deltaOld = deltaNew;
+        deltaNew = dot(r, sv);
+        const W beta = deltaNew / deltaOld;
+        for (uint32_t i = 0; i < sz; i++) d[i] = beta * d[i] + sv[i];
+    }
+    for (uint32_t i = 0; i < sz; i++) a[i] = std::complex<double>(static_cast<double>(x[i]), 0.0);
+}
+
+extern "C" {
+
+// solver 0: Cholesky (RxBeamformerMV). solver 1: RxBeamformerMVpcg's Jacobi-PCG (BF/RxBeamformerMVpcg.cu:
+// 450-546): on the sz x sz loaded system R a = 1 from a = 1, residual r = b - R a recomputed every
+// iteration (reinitialisation frequency 1), stop after maxIt iterations, when r.s <= 1e-30 or when
+// |r| <= pcgThr; sums in order, in float (precision 32) or double (64). Real data only.
+static int mvImpl(const float* raw, int iscomplex, float* outF, double* outD, uint32_t nRx, uint32_t nCh, uint32_t nS,
+                  uint32_t L, uint32_t T, double scalingPower, float loadingScale, int precision, uint32_t blockSize,
+                  int nthreads, int solver, uint32_t maxIt, double pcgThr) {
     if (L == 0) L = nCh / 2;
     if (L > nCh || L == 0) return -1;
     if (blockSize == 0) blockSize = 2000;
@@ -420,7 +471,38 @@ int orc_mv(const float* raw, int iscomplex, float* outF, double* outD, uint32_t 
                 for (uint32_t i = sz; i < L; i++) R[i * L + i] = cd(loading, 0);
             }
             cd y(0, 0);
-            if (trace > 0 && std::isfinite(trace)) {
+            if (solver == 1 && trace > 0 && std::isfinite(trace)) {
+                std::vector<cd> a(L, cd(0, 0));
+                if (precision == 32) pcgSolve<float>(R, L, sz, maxIt, pcgThr, a);
+                else pcgSolve<double>(R, L, sz, maxIt, pcgThr, a);
+                int nActive = 0;
+                for (uint32_t k = 0; k < numSub; k++) nActive += masks[s * numSub + k] != 0;
+                if (precision == 32) {
+                    float ws = 0.0f;
+                    for (uint32_t v = 0; v < sz; v++) ws += static_cast<float>(a[v].real()) * 1.0f;
+                    ws = 1.0f / (ws * std::pow(static_cast<float>(nActive), static_cast<float>(scalingPower)));
+                    float bs = 0.0f;
+                    for (uint32_t v = 0; v < sz; v++) {
+                        float sm = 0.0f;
+                        for (uint32_t k = 0; k < numSub; k++)
+                            if (masks[s * numSub + k]) sm += static_cast<float>(X(s, offs[s * numSub + k] + v).real());
+                        bs += sm * static_cast<float>(a[v].real()) * ws;
+                    }
+                    y = cd(bs, 0);
+                } else {
+                    double asum = 0;
+                    for (uint32_t v = 0; v < sz; v++) asum += a[v].real();
+                    double ws = 1.0 / (asum * std::pow(static_cast<double>(nActive), scalingPower));
+                    double bs = 0;
+                    for (uint32_t v = 0; v < sz; v++) {
+                        double sm = 0;
+                        for (uint32_t k = 0; k < numSub; k++)
+                            if (masks[s * numSub + k]) sm += X(s, offs[s * numSub + k] + v).real();
+                        bs += sm * a[v].real() * ws;
+                    }
+                    y = cd(bs, 0);
+                }
+            } else if (solver == 0 && trace > 0 && std::isfinite(trace)) {
                 // Cholesky R = G G^H (double), a = R^-1 1
                 std::vector<cd> G(static_cast<size_t>(L) * L, cd(0, 0));
                 bool ok = true;
@@ -489,6 +571,23 @@ int orc_mv(const float* raw, int iscomplex, float* outF, double* outD, uint32_t 
         }
     }
     return 0;
+}
+
+int orc_mv(const float* raw, int iscomplex, float* outF, double* outD, uint32_t nRx, uint32_t nCh, uint32_t nS,
+           uint32_t L, uint32_t T, double scalingPower, float loadingScale, int precision, uint32_t blockSize,
+           int nthreads) {
+    return mvImpl(raw, iscomplex, outF, outD, nRx, nCh, nS, L, T, scalingPower, loadingScale, precision, blockSize,
+                  nthreads, 0, 0, 0.0);
+}
+
+// RxBeamformerMVpcg::performRxBeamforming (BF/RxBeamformerMVpcg.cu:622-800): real data, no sample
+// blocks; maxIt 0 means the subarray size (:649).
+int orc_mv_pcg(const float* raw, float* outF, double* outD, uint32_t nRx, uint32_t nCh, uint32_t nS, uint32_t L,
+               uint32_t T, double scalingPower, float loadingScale, uint32_t maxIt, double thr, int precision,
+               int nthreads) {
+    const uint32_t Ls = L == 0 ? nCh / 2 : L;
+    return mvImpl(raw, 0, outF, outD, nRx, nCh, nS, L, T, scalingPower, loadingScale, precision, nS, nthreads, 1,
+                  maxIt == 0 ? Ls : maxIt, thr);
 }
 
 }  // extern "C"

@@ -171,6 +171,7 @@ _SIGNATURES = {
     "sb_env_log_scan_run": (_int, [_vp, _vp, _vp, _vp, _int, _f64, _f64, _f64, _vp]),
     "sb_mv_run": (_int, [_vp, _int, _vp, _int, _u32, _u32, _u32, _u32, _u32, _f64, _int, _f32, _f32,
                          C.POINTER(sb_mv_stats), _vp]),
+    "sb_mv_pcg_run": (_int, [_vp, _int, _vp, _int, _u32, _u32, _u32, _u32, _u32, _u32, _f64, _f64, _int, _f32, _vp]),
     "sb_batch_plan_create": (_int, [_vp, _u32, C.POINTER(sb_batch_params), C.POINTER(_vp)]),
     "sb_batch_plan_destroy": (_int, [_vp]),
     "sb_batch_run": (_int, [_vp, _int, _vp]),

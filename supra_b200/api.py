@@ -369,6 +369,23 @@ def mv_beamform(raw_delayed: torch.Tensor, subarray_size=0, temporal_smoothing=3
     return out, stats
 
 
+def mv_beamform_pcg(raw_delayed: torch.Tensor, subarray_size=0, temporal_smoothing=3, max_iterations_override=0,
+                    convergence_threshold=1e-4, subarray_scaling_power=1.5, compute_means=False, loading_scale=1.0,
+                    out_dtype=torch.float32) -> torch.Tensor:
+    """RxBeamformerMVpcg::performRxBeamforming (Beamformer/RxBeamformerMVpcg.cu:622-800): minimum variance
+    with the weights from Jacobi-PCG. raw_delayed [num_rx][num_channels][num_depths] float32 or int16 ->
+    [num_depths][num_rx]."""
+    lib = load_library()
+    nRx, nCh, nS = raw_delayed.shape
+    out = torch.empty((nS, nRx), dtype=out_dtype, device=raw_delayed.device)
+    check("sb_mv_pcg_run", lib.sb_mv_pcg_run(_ptr(raw_delayed), dtype_code(raw_delayed), _ptr(out), dtype_code(out), nRx,
+                                             nCh, nS, int(subarray_size), int(temporal_smoothing),
+                                             int(max_iterations_override), float(convergence_threshold),
+                                             float(subarray_scaling_power), int(bool(compute_means)),
+                                             float(loading_scale), _stream()))
+    return out
+
+
 class BatchedDasIq:
     """Persistent, graph-captured batched DAS + complex IQ over frames of uneven probes.
 

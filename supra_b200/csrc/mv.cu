@@ -135,7 +135,11 @@ struct MvArgs {
     void* out;
     uint32_t nRx, nCh, nS, L, T;
     uint32_t ringSlots, ringPitch, runsPerLine, runsPerBlock, numItems;
+    uint32_t blockLen;  // temporal windows are clipped to blocks of this many samples
     float power, loadScale, thr;
+    int pcg;            // solve by Jacobi-PCG (RxBeamformerMVpcg) instead of Cholesky
+    int pcgMaxIt;
+    float pcgThr;
     uint32_t* queue;
     MvCounters* counters;
 };
@@ -402,6 +406,88 @@ __device__ __forceinline__ MvOut<T> solveRegs(GE* Gs, int GP, int L, int sz, T l
     return res;
 }
 
+// RxBeamformerMVpcg (Beamformer/RxBeamformerMVpcg.cu:450-546, 548-620) on the sz x sz loaded system
+// R a = 1, real data: Jacobi-preconditioned conjugate gradients from x = 1 with the residual
+// recomputed from x every iteration (reinitialisation frequency 1), stopping after maxIt iterations,
+// when r.s <= 1e-30 or when |r| <= thr; then y = sum_v xbar_v a_v / (sum_v a_v * K^p). Row i of R
+// sits in registers of lane i % 32 (q = i / 32); R v broadcasts v_j from its lane.
+template <int NR, class GE>
+__device__ __forceinline__ MvOut<float> solvePcgRegs(const GE* Gs, int GP, int sz, float loading, int lane,
+                                                     const V<float> (&xbar)[NR], float power, int K, int maxIt, float thr) {
+    float A[NR][32 * NR], dg[NR];
+    bool valid[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) {
+        const int i = lane + 32 * q;
+        valid[q] = i < sz;
+#pragma unroll
+        for (int j = 0; j < 32 * NR; j++) {
+            float v = 0.0f;
+            if (valid[q] && j < sz) v = Gs[i * GP + j].re + (i == j ? loading : 0.0f);
+            A[q][j] = v;
+        }
+        dg[q] = valid[q] ? Gs[i * GP + i].re + loading : 1.0f;
+    }
+    auto matvec = [&](const float (&v)[NR], float (&o)[NR]) {
+#pragma unroll
+        for (int q = 0; q < NR; q++) o[q] = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 32 * NR; j++) {
+            if (j >= sz) break;  // warp-uniform
+            const float vj = __shfl_sync(kFull, v[j >> 5], j & 31);
+#pragma unroll
+            for (int q = 0; q < NR; q++) o[q] = fmaf(A[q][j], vj, o[q]);
+        }
+    };
+    auto dot = [&](const float (&u)[NR], const float (&w)[NR]) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int q = 0; q < NR; q++) acc = fmaf(u[q], w[q], acc);
+        return warpSum(acc);
+    };
+    float x[NR], r[NR], d[NR], t[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) x[q] = valid[q] ? 1.0f : 0.0f;
+    matvec(x, t);
+#pragma unroll
+    for (int q = 0; q < NR; q++) {
+        r[q] = valid[q] ? fmaf(-1.0f, t[q], 1.0f) : 0.0f;
+        d[q] = r[q] / dg[q];
+    }
+    float deltaNew = dot(r, d);
+    float residualNorm = 2.0f * thr;
+    for (int it = 0; it < maxIt && static_cast<double>(deltaNew) > 1e-30 && residualNorm > thr; it++) {
+        matvec(d, t);  // q = A d
+        const float alpha = deltaNew / dot(d, t);
+#pragma unroll
+        for (int q = 0; q < NR; q++) x[q] = fmaf(alpha, d[q], x[q]);
+        matvec(x, t);  // r = b - A x
+#pragma unroll
+        for (int q = 0; q < NR; q++) r[q] = valid[q] ? fmaf(-1.0f, t[q], 1.0f) : 0.0f;
+        residualNorm = sqrtf(dot(r, r));
+        float sv[NR];
+#pragma unroll
+        for (int q = 0; q < NR; q++) sv[q] = r[q] / dg[q];
+        const float deltaOld = deltaNew;
+        deltaNew = dot(r, sv);
+        const float beta = deltaNew / deltaOld;
+#pragma unroll
+        for (int q = 0; q < NR; q++) d[q] = fmaf(beta, d[q], sv[q]);
+    }
+    float asum = 0.0f, y = 0.0f;
+#pragma unroll
+    for (int q = 0; q < NR; q++) asum += x[q];
+    asum = warpSum(asum);
+    const float ws = 1.0f / (asum * powf(static_cast<float>(K), power));
+#pragma unroll
+    for (int q = 0; q < NR; q++) y += xbar[q].re * x[q] * ws;
+    MvOut<float> res;
+    res.ok = true;
+    res.y = V<float>{warpSum(y), 0.0f};
+    res.cond = 0.0f;
+    return res;
+}
+
 // Same factorisation and substitutions in FP64 with the rows kept in shared memory (used only for
 // the queued systems).
 template <bool C, int NR>
@@ -615,8 +701,8 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
     if (item >= a.numItems) return;
     const uint32_t line = item / a.runsPerLine, run = item % a.runsPerLine;
     const uint32_t blk = run / a.runsPerBlock, j = run % a.runsPerBlock;
-    const uint32_t b0 = blk * kMvBlock;
-    const uint32_t bEnd = min(a.nS, b0 + kMvBlock);  // exclusive
+    const uint32_t b0 = blk * a.blockLen;
+    const uint32_t bEnd = min(a.nS, b0 + a.blockLen);  // exclusive
     const uint32_t sA = b0 + j * kMvRun;
     if (sA >= bEnd) return;
     const uint32_t sB = min(sA + kMvRun, bEnd);
@@ -748,7 +834,13 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
         }
         V<float> y = vz<C, float>();
         bool write = true;
-        if (tr > 0.0f && isfinite(tr)) {
+        if (!C && a.pcg) {
+            if constexpr (!C) {
+                if (tr > 0.0f && isfinite(tr))
+                    y = solvePcgRegs<NR, Elem<C>>(Gs, L_::GP, ms.sz, loading, lane, xbar, a.power, ms.K, a.pcgMaxIt,
+                                                  a.pcgThr).y;
+            }
+        } else if (tr > 0.0f && isfinite(tr)) {
             const MvOut<float> r =
                 solveRegs<C, NR, float, Elem<C>>(Gs, L_::GP, L, ms.sz, loading, lane, xbar, a.power, ms.K);
             const float cond = r.ok ? r.cond : INFINITY;
@@ -796,8 +888,8 @@ __global__ void __launch_bounds__(128) mvFp64Kernel(MvArgs a, uint32_t window) {
     for (unsigned int qi = blockIdx.x * warpsPerCta + warp; qi < nq; qi += gridDim.x * warpsPerCta) {
         const uint32_t id = a.queue[qi];
         const uint32_t line = id / a.nS, s = id % a.nS;
-        const uint32_t b0 = (s / kMvBlock) * kMvBlock;
-        const uint32_t bEnd = min(a.nS, b0 + kMvBlock);
+        const uint32_t b0 = (s / a.blockLen) * a.blockLen;
+        const uint32_t bEnd = min(a.nS, b0 + a.blockLen);
         const uint32_t t0 = static_cast<uint32_t>(max(static_cast<int>(b0), static_cast<int>(s) - static_cast<int>(a.T)));
         const uint32_t t1 = min(bEnd - 1, s + a.T);
         const In* xl = static_cast<const In*>(a.in) + static_cast<size_t>(line) * a.nCh * a.nS;
@@ -896,10 +988,14 @@ template <bool C, class In, class Out> int dispatchNR(MvArgs& a, cudaStream_t st
 
 using namespace sb;
 
-extern "C" int sb_mv_run(const void* raw_delayed, int in_dtype, void* out, int out_dtype, uint32_t num_scanlines,
-                         uint32_t num_channels, uint32_t num_samples, uint32_t subarray_size, uint32_t temporal_smoothing,
-                         double subarray_scaling_power, int compute_means, float loading_scale, float fp64_threshold,
-                         sb_mv_stats* stats_host, sb_stream stream) {
+namespace {
+
+// Shared body of sb_mv_run and sb_mv_pcg_run: blockLen clips the temporal windows, pcgMaxIt > 0
+// selects the PCG solve.
+int mvRun(const void* raw_delayed, int in_dtype, void* out, int out_dtype, uint32_t num_scanlines,
+          uint32_t num_channels, uint32_t num_samples, uint32_t subarray_size, uint32_t temporal_smoothing,
+          double subarray_scaling_power, int compute_means, float loading_scale, float fp64_threshold,
+          sb_mv_stats* stats_host, sb_stream stream, uint32_t blockLen, int pcgMaxIt, float pcgThr) {
     SB_REQUIRE(raw_delayed && out, "sb_mv_run: null pointer");
     SB_REQUIRE(num_scanlines > 0 && num_channels > 0 && num_samples > 0, "sb_mv_run: empty input");
     if (compute_means)
@@ -928,13 +1024,17 @@ extern "C" int sb_mv_run(const void* raw_delayed, int in_dtype, void* out, int o
     a.ringSlots = 2 * temporal_smoothing + 2;
     // channel reads reach index nCh - 1 + L - 1 (apertures narrower than L); padding is zero
     a.ringPitch = (num_channels + (L <= 32 ? 32 : 64) + 31) / 32 * 32;
-    a.runsPerBlock = (kMvBlock + kMvRun - 1) / kMvRun;
-    const uint32_t nBlocks = (num_samples + kMvBlock - 1) / kMvBlock;
+    a.blockLen = blockLen;
+    a.runsPerBlock = (blockLen + kMvRun - 1) / kMvRun;
+    const uint32_t nBlocks = (num_samples + blockLen - 1) / blockLen;
     a.runsPerLine = nBlocks * a.runsPerBlock;
     a.numItems = num_scanlines * a.runsPerLine;
     a.power = static_cast<float>(subarray_scaling_power);
     a.loadScale = loading_scale;
     a.thr = fp64_threshold;
+    a.pcg = pcgMaxIt > 0 ? 1 : 0;
+    a.pcgMaxIt = pcgMaxIt;
+    a.pcgThr = pcgThr;
 
     // scratch: counters, and the FP64 queue when the re-solve is enabled
     const size_t qBytes = fp64_threshold > 0.0f ? static_cast<size_t>(num_scanlines) * num_samples * sizeof(uint32_t) : 0;
@@ -966,4 +1066,31 @@ extern "C" int sb_mv_run(const void* raw_delayed, int in_dtype, void* out, int o
     }
     cudaFreeAsync(scratch, st);
     return rc;
+}
+
+}  // namespace
+
+extern "C" int sb_mv_run(const void* raw_delayed, int in_dtype, void* out, int out_dtype, uint32_t num_scanlines,
+                         uint32_t num_channels, uint32_t num_samples, uint32_t subarray_size, uint32_t temporal_smoothing,
+                         double subarray_scaling_power, int compute_means, float loading_scale, float fp64_threshold,
+                         sb_mv_stats* stats_host, sb_stream stream) {
+    return mvRun(raw_delayed, in_dtype, out, out_dtype, num_scanlines, num_channels, num_samples, subarray_size,
+                 temporal_smoothing, subarray_scaling_power, compute_means, loading_scale, fp64_threshold, stats_host,
+                 stream, kMvBlock, 0, 0.0f);
+}
+
+extern "C" int sb_mv_pcg_run(const void* raw_delayed, int in_dtype, void* out, int out_dtype, uint32_t num_scanlines,
+                             uint32_t num_channels, uint32_t num_samples, uint32_t subarray_size,
+                             uint32_t temporal_smoothing, uint32_t max_iterations_override, double convergence_threshold,
+                             double subarray_scaling_power, int compute_means, float loading_scale, sb_stream stream) {
+    SB_REQUIRE(in_dtype != SB_COMPLEX64, "sb_mv_pcg_run: the PCG solve takes real data (float32 or int16)");
+    SB_REQUIRE(convergence_threshold >= 0.0, "sb_mv_pcg_run: negative convergence threshold");
+    const uint32_t L = subarray_size == 0 ? num_channels / 2 : subarray_size;
+    // RxBeamformerMVpcg.cu:649: maxIterations = subArraySize unless overridden
+    const uint32_t maxIt = max_iterations_override == 0 ? L : max_iterations_override;
+    SB_REQUIRE(maxIt >= 1 && maxIt <= 100000, "sb_mv_pcg_run: iteration count %u out of range", maxIt);
+    // no sample blocks: the PCG reference smooths over +-T clipped only at the record ends
+    return mvRun(raw_delayed, in_dtype, out, out_dtype, num_scanlines, num_channels, num_samples, subarray_size,
+                 temporal_smoothing, subarray_scaling_power, compute_means, loading_scale, 0.0f, nullptr, stream,
+                 std::max<uint32_t>(num_samples, 1), static_cast<int>(maxIt), static_cast<float>(convergence_threshold));
 }

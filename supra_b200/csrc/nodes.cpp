@@ -504,8 +504,8 @@ protected:
         img->data = out;
         img->stream = raw->stream;
         auto p = derivedProperties(*raw, ImageProperties::State::RF);
-        p->specific["Beamformer.subArraySize"] = std::to_string(m_subArraySize);
-        p->specific["Beamformer.temporalSmoothing"] = std::to_string(m_temporalSmoothing);
+        p->specific["BeamformingMVNode.subArraySize"] = std::to_string(m_subArraySize);
+        p->specific["BeamformingMVNode.temporalSmoothing"] = std::to_string(m_temporalSmoothing);
         img->properties = p;
         return img;
     }
@@ -514,6 +514,70 @@ private:
     uint32_t m_subArraySize = 0, m_temporalSmoothing = 3;
     DataType m_outputType = DataType::Float;
     double m_scalingPower = 1.5, m_loading = 1.0, m_fp64Threshold = 1e6;
+    bool m_computeMeans = false;
+};
+
+// ---------------------------------------------------------------- BeamformingMVpcgNode
+// BeamformingMVpcgNode (Beamformer/BeamformingMVpcgNode.cpp:41-190): minimum variance on raw-delayed
+// data with the weights from Jacobi-PCG; the convergence threshold is 10^convergenceThresholdExponent.
+class BeamformingMVpcgNode : public AbstractNode {
+public:
+    explicit BeamformingMVpcgNode(const std::string& id) : AbstractNode(id) {
+        auto& d = m_valueRangeDictionary;
+        d.setRange("subArraySize", "uint32_t", 0, 64, "0", "Sub-array size");
+        d.setRange("temporalSmoothing", "uint32_t", 0, 10, "3", "temporal smoothing");
+        d.setChoices("outputType", "DataType", {"float", "uint16"}, "float", "Output type");
+        d.setRange("maxIterationsOverride", "uint32_t", 0, 10000, "0", "Max iterations override (if != 0)");
+        d.setRange("convergenceThresholdExponent", "double", -100.0, 0.0, "-4", "Convergence threshold exponent");
+        d.setRange("subArrayScalingPower", "double", 0.5, 3.0, "1.5", "Subarray count scaling power");
+        d.setChoices("computeMeans", "bool", {"false", "true"}, "false", "compute signal means");
+        finishConstruction();
+    }
+    const char* getType() const override { return "BeamformingMVpcgNode"; }
+
+protected:
+    void configurationChanged() override {
+        const auto& c = m_configurationDictionary;
+        m_subArraySize = static_cast<uint32_t>(c.getInt("subArraySize"));
+        m_temporalSmoothing = static_cast<uint32_t>(c.getInt("temporalSmoothing"));
+        m_outputType = c.getDataType("outputType");
+        m_maxIterationsOverride = static_cast<uint32_t>(c.getInt("maxIterationsOverride"));
+        m_convergenceThreshold = std::pow(10.0, c.getDouble("convergenceThresholdExponent"));
+        m_scalingPower = c.getDouble("subArrayScalingPower");
+        m_computeMeans = c.getBool("computeMeans");
+    }
+    std::shared_ptr<RecordObject> processLocked(const std::shared_ptr<RecordObject>& in) override {
+        if (in->getType() != RecordType::RawData) return fail("input is not USRawData");
+        auto raw = std::static_pointer_cast<USRawData>(in);
+        if (!raw->properties || raw->properties->state != ImageProperties::State::RawDelayed)
+            return fail("Cannot beamform undelayed RawData. Apply RawDelayNode first");
+        if (raw->dtype != DataType::Int16 && raw->dtype != DataType::Float) return fail("input rawdata type is not supported");
+        // the reference's output switch handles float and int16 only (BeamformingMVpcgNode.cpp:124-140)
+        if (m_outputType != DataType::Float) return fail("output image type not supported");
+        const uint32_t nRx = raw->numTx, nCh = raw->numChannels, nS = raw->numSamples;
+        auto out = deviceBuffer(static_cast<size_t>(nS) * nRx * sizeof(float), raw->stream);
+        if (!out) return fail("device allocation failed");
+        const int st = sb_mv_pcg_run(raw->data.get(), static_cast<int>(raw->dtype), out.get(), SB_FLOAT32, nRx, nCh, nS,
+                                     m_subArraySize, m_temporalSmoothing, m_maxIterationsOverride, m_convergenceThreshold,
+                                     m_scalingPower, m_computeMeans ? 1 : 0, 1.0f, raw->stream);
+        if (st != SB_OK) return fail(statusMessage(st));
+        auto img = std::make_shared<USImage>();
+        img->size[0] = nRx;
+        img->size[1] = nS;
+        img->dtype = DataType::Float;
+        img->data = out;
+        img->stream = raw->stream;
+        auto p = derivedProperties(*raw, ImageProperties::State::RF);
+        p->specific["BeamformingMVNode.subArraySize"] = std::to_string(m_subArraySize);
+        p->specific["BeamformingMVNode.temporalSmoothing"] = std::to_string(m_temporalSmoothing);
+        img->properties = p;
+        return img;
+    }
+
+private:
+    uint32_t m_subArraySize = 0, m_temporalSmoothing = 3, m_maxIterationsOverride = 0;
+    DataType m_outputType = DataType::Float;
+    double m_convergenceThreshold = 1e-4, m_scalingPower = 1.5;
     bool m_computeMeans = false;
 };
 
@@ -860,6 +924,7 @@ const std::vector<std::pair<std::string, Creator>>& creators() {
         {"BeamformingNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new BeamformingNode(id)); }},
         {"RawDelayNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new RawDelayNode(id)); }},
         {"BeamformingMVNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new BeamformingMVNode(id)); }},
+        {"BeamformingMVpcgNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new BeamformingMVpcgNode(id)); }},
         {"HilbertFirEnvelopeNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new HilbertFirEnvelopeNode(id)); }},
         {"IQDemodulatorNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new IQDemodulatorNode(id)); }},
         {"LogCompressorNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new LogCompressorNode(id)); }},

@@ -17,6 +17,7 @@ NODES = {
     "BeamformingNode": "BeamformingNode.cpp",
     "RawDelayNode": "RawDelayNode.cpp",
     "BeamformingMVNode": "BeamformingMVNode.cpp",
+    "BeamformingMVpcgNode": "BeamformingMVpcgNode.cpp",
     "HilbertFirEnvelopeNode": "HilbertFirEnvelopeNode.cpp",
     "IQDemodulatorNode": "IQDemodulatorNode.cpp",
     "LogCompressorNode": "LogCompressorNode.cpp",

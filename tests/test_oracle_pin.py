@@ -129,3 +129,16 @@ def test_oracle_mv_reference_vs_fp64(oracle):
     a = oracle.mv(raw, 8, 2, precision=32)
     b = oracle.mv(raw, 8, 2, precision=64)
     assert np.max(np.abs(a - b)) <= 1e-3 * np.max(np.abs(b))
+
+
+def test_oracle_mv_pcg_converges_to_direct_solve(oracle):
+    """The PCG restatement (RxBeamformerMVpcg) with enough iterations and a tight threshold gives the
+    direct solve (Cholesky) of the same systems; with the reference's defaults it is close to it."""
+    rng = np.random.Generator(np.random.PCG64(0))
+    raw = rng.standard_normal((3, 16, 64)).astype(np.float32)
+    raw[:, :3, :10] = 0
+    direct = oracle.mv(raw, 8, 2, precision=64, block=64)  # one block: the PCG reference has none
+    pcg = oracle.mv_pcg(raw, 8, 2, max_iterations=64, threshold=1e-9, precision=64)
+    assert np.max(np.abs(pcg - direct)) <= 1e-7 * np.max(np.abs(direct))
+    default = oracle.mv_pcg(raw, 8, 2, precision=32)
+    assert np.max(np.abs(default - direct)) <= 1e-3 * np.max(np.abs(direct))
