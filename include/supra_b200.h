@@ -144,6 +144,17 @@ int sb_das_run_beamformer(const sb_das_plan* plan, int sample_beamformer, const 
                           int out_dtype, double f_number, double speed_of_sound_mm_s, int window_type,
                           float window_parameter, int interpolate_transmits, int32_t additional_offset, sb_stream stream);
 
+/* HilbertEnvelope::computeHilbertEnvelope (Beamformer/HilbertEnvelope.cu:127-207): the envelope of the
+ * analytic signal along each scanline, |x + i H x| with H the circular discrete Hilbert transform of
+ * the whole line (the reference's FFT, positive-frequency doubling and inverse FFT), for any number of
+ * samples. The plan holds the transform's kernel for num_samples; images are [num_samples][num_scanlines]
+ * (SB_INT16 or SB_FLOAT32 in and out; the reference's decimation parameter is not applied, as there). */
+typedef struct sb_analytic_plan sb_analytic_plan;
+int sb_analytic_plan_create(uint32_t num_samples, sb_analytic_plan** plan);
+int sb_analytic_plan_destroy(sb_analytic_plan* plan);
+int sb_analytic_env_run(const sb_analytic_plan* plan, const void* in, int in_dtype, void* out, int out_dtype,
+                        uint32_t num_scanlines, sb_stream stream);
+
 /* TemporalFilter::filter (Beamformer/TemporalFilter.cu:48-110): out[i] = clampCast(sum_k w_k x_k[i] / sum_k w_k)
  * over num_images device images of numel elements each (images[0] the oldest, the node's queue order),
  * in float as the reference (weights given in double, converted to float; NULL = all 1, the node's

@@ -159,8 +159,8 @@ private:
 
 // InterfaceFactory::createNode analogue (SupraLib/InterfaceFactory.cpp:212-251) for the receive-path
 // types: BeamformingNode, RawDelayNode, BeamformingMVNode, HilbertFirEnvelopeNode,
-// IQDemodulatorNode, LogCompressorNode, ScanConverterNode, TemporalFilterNode, BeamformingMVpcgNode. nullptr
-// for other types.
+// IQDemodulatorNode, LogCompressorNode, ScanConverterNode, TemporalFilterNode, BeamformingMVpcgNode,
+// HilbertEnvelopeNode. nullptr for other types.
 std::unique_ptr<AbstractNode> createNode(const std::string& type, const std::string& nodeID);
 std::vector<std::string> nodeTypes();
 

@@ -179,6 +179,25 @@ def ref_mock_read(filename: str, max_lines=4096, max_depths=65536, max_elems=655
     return {"sizes": sizes, "vals": vals, "lines": lines[:nL], "depths": depths[:nD], "xs": xs[:nE], "ys": ys[:nE]}
 
 
+def analytic_env(img: np.ndarray) -> np.ndarray:
+    """HilbertEnvelope (BF/HilbertEnvelope.cu:27-207) in FP64: per scanline (columns of [N][nRx]) the
+    FFT, the spectrum mask of maskSpectrum (DC x1; bins 1..N/2-1 x2 and N/2 x1 for even N, bins
+    1..(N-1)/2 x2 for odd N; the rest 0), the inverse FFT (numpy's is normalised: the reference's
+    unnormalised inverse divided by N) and the magnitude."""
+    x = np.asarray(img, np.float64)
+    N = x.shape[0]
+    m = np.zeros(N)
+    m[0] = 1.0
+    if N % 2 == 0:
+        m[1:N // 2] = 2.0
+        if N > 1:
+            m[N // 2] = 1.0
+    else:
+        m[1:(N + 1) // 2] = 2.0
+    z = np.fft.ifft(np.fft.fft(x, axis=0) * m[:, None], axis=0)
+    return np.abs(z)
+
+
 def das_adjoint64(geom, rf: np.ndarray, apod, gout: np.ndarray, c_mm_s=None, f_number=1.0, window=1, window_param=0.0):
     """FP64 reference gradient of the apodised 2D DAS: (grad_rf, grad_apod, grad_c)."""
     g = geom.ctypes()

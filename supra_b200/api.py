@@ -173,6 +173,31 @@ class HilbertFirEnvelope:
         return out
 
 
+class HilbertEnvelope:
+    """HilbertEnvelope (Beamformer/HilbertEnvelope.cu:27-207): the envelope of the analytic signal of each
+    scanline over its whole length (the reference computes it by FFT; here by the exact circular Hilbert
+    transform), for images [num_samples][num_scanlines]."""
+
+    def __init__(self, num_samples: int):
+        self.lib = load_library()
+        self.num_samples = int(num_samples)
+        self._plan = C.c_void_p()
+        check("sb_analytic_plan_create", self.lib.sb_analytic_plan_create(self.num_samples, C.byref(self._plan)))
+
+    def __del__(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            self.lib.sb_analytic_plan_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    def envelope(self, img: torch.Tensor, out_dtype=torch.float32) -> torch.Tensor:
+        if img.dim() != 2 or img.shape[0] != self.num_samples or not img.is_contiguous():
+            raise ValueError("HilbertEnvelope: a contiguous [num_samples][num_scanlines] image")
+        out = torch.empty(img.shape, dtype=out_dtype, device=img.device)
+        check("sb_analytic_env_run", self.lib.sb_analytic_env_run(self._plan, _ptr(img), dtype_code(img), _ptr(out),
+                                                                  dtype_code(out), img.shape[1], _stream()))
+        return out
+
+
 class LogCompressor:
     """LogCompressor::compress (Beamformer/LogCompressor.cu:44-66)."""
 

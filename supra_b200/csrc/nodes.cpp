@@ -581,6 +581,63 @@ private:
     bool m_computeMeans = false;
 };
 
+// ------------------------------------------------------------------ HilbertEnvelopeNode
+// HilbertEnvelopeNode (Beamformer/HilbertEnvelopeNode.cpp:38-156): the analytic-signal envelope of each
+// scanline over its whole length; "decimation" is kept as a parameter and property but, as in the
+// reference (HilbertEnvelope::decimatedSignalLength), not applied.
+class HilbertEnvelopeNode : public AbstractNode {
+public:
+    explicit HilbertEnvelopeNode(const std::string& id) : AbstractNode(id) {
+        auto& d = m_valueRangeDictionary;
+        d.setRange("decimation", "uint32_t", 1, 100, "8", "Decimation");
+        d.setChoices("outputType", "DataType", {"float", "int16"}, "float", "Output type");
+        finishConstruction();
+    }
+    ~HilbertEnvelopeNode() override { sb_analytic_plan_destroy(m_plan); }
+    const char* getType() const override { return "HilbertEnvelopeNode"; }
+
+protected:
+    void configurationChanged() override {
+        m_decimation = static_cast<uint32_t>(m_configurationDictionary.getInt("decimation"));
+        m_outputType = m_configurationDictionary.getDataType("outputType");
+    }
+    std::shared_ptr<RecordObject> processLocked(const std::shared_ptr<RecordObject>& in) override {
+        if (in->getType() != RecordType::Image) return fail("input is not USImage");
+        auto im = std::static_pointer_cast<USImage>(in);
+        if (im->dtype != DataType::Int16 && im->dtype != DataType::Float) return fail("Input image type not supported.");
+        const uint32_t nL = im->size[0], nS = im->size[1];
+        if (!m_plan || m_planSamples != nS) {
+            sb_analytic_plan_destroy(m_plan);
+            m_plan = nullptr;
+            const int st = sb_analytic_plan_create(nS, &m_plan);
+            if (st != SB_OK) return fail(statusMessage(st));
+            m_planSamples = nS;
+        }
+        auto out = deviceBuffer(static_cast<size_t>(nL) * nS * dtypeBytes(m_outputType), im->stream);
+        if (!out) return fail("device allocation failed");
+        const int st = sb_analytic_env_run(m_plan, im->data.get(), static_cast<int>(im->dtype), out.get(),
+                                           static_cast<int>(m_outputType), nL, im->stream);
+        if (st != SB_OK) return fail(statusMessage(st));
+        auto o = std::make_shared<USImage>();
+        o->size[0] = nL;
+        o->size[1] = nS;
+        o->size[2] = 1;
+        o->dtype = m_outputType;
+        o->data = out;
+        o->stream = im->stream;
+        auto p = derivedProperties(*im, ImageProperties::State::EnvDetected);
+        p->numSamples = nS;
+        p->specific["Hilbert.Decimation"] = std::to_string(m_decimation);
+        o->properties = p;
+        return o;
+    }
+
+private:
+    uint32_t m_decimation = 8, m_planSamples = 0;
+    DataType m_outputType = DataType::Float;
+    sb_analytic_plan* m_plan = nullptr;
+};
+
 // ------------------------------------------------------------ HilbertFirEnvelopeNode
 class HilbertFirEnvelopeNode : public AbstractNode {
 public:
@@ -926,6 +983,7 @@ const std::vector<std::pair<std::string, Creator>>& creators() {
         {"BeamformingMVNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new BeamformingMVNode(id)); }},
         {"BeamformingMVpcgNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new BeamformingMVpcgNode(id)); }},
         {"HilbertFirEnvelopeNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new HilbertFirEnvelopeNode(id)); }},
+        {"HilbertEnvelopeNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new HilbertEnvelopeNode(id)); }},
         {"IQDemodulatorNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new IQDemodulatorNode(id)); }},
         {"LogCompressorNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new LogCompressorNode(id)); }},
         {"ScanConverterNode", [](const std::string& id) { return std::unique_ptr<AbstractNode>(new ScanConverterNode(id)); }},

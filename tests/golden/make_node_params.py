@@ -19,6 +19,7 @@ NODES = {
     "BeamformingMVNode": "BeamformingMVNode.cpp",
     "BeamformingMVpcgNode": "BeamformingMVpcgNode.cpp",
     "HilbertFirEnvelopeNode": "HilbertFirEnvelopeNode.cpp",
+    "HilbertEnvelopeNode": "HilbertEnvelopeNode.cpp",
     "IQDemodulatorNode": "IQDemodulatorNode.cpp",
     "LogCompressorNode": "LogCompressorNode.cpp",
     "ScanConverterNode": "ScanConverterNode.cpp",

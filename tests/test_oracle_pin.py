@@ -142,3 +142,23 @@ def test_oracle_mv_pcg_converges_to_direct_solve(oracle):
     assert np.max(np.abs(pcg - direct)) <= 1e-7 * np.max(np.abs(direct))
     default = oracle.mv_pcg(raw, 8, 2, precision=32)
     assert np.max(np.abs(default - direct)) <= 1e-3 * np.max(np.abs(direct))
+
+
+def test_oracle_analytic_envelope(oracle):
+    """HilbertEnvelope's FFT envelope: a periodic tone's envelope is its amplitude, and it equals
+    sqrt(x^2 + (k (*) x)^2) with the circular Hilbert kernel k[n] = (2/N) sum_{j=1..J} sin(2 pi j n / N)
+    in the closed form the library's plan uses, for even and odd lengths."""
+    for N in (64, 63, 1000, 7):
+        n = np.arange(N)
+        x = 3.0 * np.cos(2 * np.pi * 5 * n / N + 0.3)
+        env = oracle.analytic_env(x[:, None])[:, 0]
+        if N > 11:
+            assert np.max(np.abs(env - 3.0)) < 1e-9
+        J = N // 2 - 1 if N % 2 == 0 else (N - 1) // 2
+        t = 2 * np.pi * n[1:] / N
+        k = np.zeros(N)
+        k[1:] = 2.0 / N * np.sin(J * t / 2) * np.sin((J + 1) * t / 2) / np.sin(t / 2)
+        rng = np.random.Generator(np.random.PCG64(N))
+        y = rng.standard_normal((N, 3))
+        h = np.stack([[np.sum(k[(i - np.arange(N)) % N] * y[:, c]) for i in range(N)] for c in range(3)], axis=1)
+        assert np.max(np.abs(np.sqrt(y * y + h * h) - oracle.analytic_env(y))) < 1e-9
