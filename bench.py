@@ -193,6 +193,26 @@ def extras(wl, plans):
     res["mv_c3"] = {"px_per_s": x3.shape[0] * x3.shape[2] / ms * 1e3, "frames_per_s": 1e3 / ms, "ms": ms,
                     "fp64_systems": int(st.fp64_systems), "max_condition_estimate": float(st.max_condition_estimate)}
     del x3
+    # the other sample beamformers on the c0 frame (per-frame kernels, reference float semantics)
+    for name in ("DelayAndStdDev", "CoherenceFactorDelayAndSum"):
+        ms = _event_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0, beamformer=name), 10)
+        res["das_" + name] = {"px_per_s": g0.num_rx * g0.num_depths / ms * 1e3, "ms": ms}
+    # MV with the PCG solve on the c0 frame's raw-delayed data (real, 128 lines x 64 channels x 2048)
+    from supra_b200.api import HilbertEnvelope, mv_beamform_pcg, temporal_filter
+    raw0 = bf0.raw_delay(rf0, 1.0, window_type=1)
+    raw0[~(raw0.abs() < 1e30)] = 0.0
+    ms = _event_ms(lambda: mv_beamform_pcg(raw0, 32, 5), 3, warm=1)
+    res["mv_pcg_c0"] = {"px_per_s": raw0.shape[0] * raw0.shape[2] / ms * 1e3, "ms": ms, "L": 32, "T": 5}
+    del raw0
+    # analytic-signal envelope (HilbertEnvelope) of the c0 image: 2 N^2 flops per scanline
+    env = HilbertEnvelope(g0.num_depths)
+    ms = _event_ms(lambda: env.envelope(o0), 10)
+    res["analytic_env_c0"] = {"ms": ms, "tflops": 2.0 * g0.num_depths ** 2 * g0.num_rx / ms / 1e9}
+    # temporal filter over 3 float images of 4096 x 4096 (192 MB in + 64 MB out, above the 126 MB L2)
+    ims = [torch.randn((4096, 4096), device="cuda") for _ in range(3)]
+    ms = _event_ms(lambda: temporal_filter(ims), 10)
+    res["temporal_filter"] = {"ms": ms, "gb_per_s": 4 * 4096 * 4096 * 4 / ms / 1e6, "images": 3}
+    del ims
     # c4: differentiable DAS, 16 frames: adjoint (all three gradients) vs forward
     g4, rf4 = W.c4_batch()
     bf4 = RxBeamformer(g4)
