@@ -164,6 +164,25 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         g.off = static_cast<uint32_t>(e.ch) + idx;  // e.ch holds the row offset
         return g;
     };
+    if constexpr (K >= 8) {
+        // wide packs: one element's gathers in flight while the next element's geometry is computed
+        // (two sample registers per frame instead of four, so 8 frames fit the register budget)
+        G g = geom(j0);
+        for (int j = j0; j < j1; j++) {
+            int16_t a[K], b[K];
+#pragma unroll
+            for (int f = 0; f < K; f++) {
+                a[f] = __ldg(tb[f] + g.off);
+                b[f] = __ldg(tb[f] + g.off + 1);
+            }
+            const G gn = j + 1 < j1 ? geom(j + 1) : g;
+#pragma unroll
+            for (int f = 0; f < K; f++)
+                acc.v[f] = fmaf(g.wB, s16ToFloat(b[f]), fmaf(g.wA, static_cast<float>(a[f]), acc.v[f]));
+            g = gn;
+        }
+        return;
+    }
     int16_t a0[K], b0[K], a1[K], b1[K];
     G g0 = geom(j0);
     G g1 = j0 + 1 < j1 ? geom(j0 + 1) : g0;
