@@ -11,6 +11,12 @@
 // needs slide by one per input sample, so each step is one shared-memory float4 of x, one k and 16
 // FMAs. Sums are blocked per 32-sample chunk (chunk sum added to the total) to keep the FP32 error of
 // the N-term sums small. The output is clampCast(sqrt(x^2 + h^2)).
+// Long lines leave too few tiles to fill the GPU (2048 x 128: 256 CTAs of 2 warps), so the input
+// range of each output tile is split over the 8 CTAs of a thread-block cluster (CTA r sums chunks
+// r, r + 8, ...); rank 0 adds the 8 partial tiles from distributed shared memory in rank order (a
+// deterministic reduction, no scratch memory) and writes the envelope.
+#include <cooperative_groups.h>
+
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -28,20 +34,21 @@ namespace {
 constexpr int kAT = 32;   // samples and scanlines per CTA tile, and samples per staged chunk
 constexpr int kAThreads = 64;
 
-template <typename IN, typename OUT>
-__global__ void __launch_bounds__(kAThreads) analyticEnvKernel(const IN* __restrict__ in, OUT* __restrict__ out,
-                                                               const float* __restrict__ kern, int N, int nL) {
-    __shared__ __align__(16) float xs[kAT][kAT];  // [m - m0][line - l0]
-    __shared__ float ks[2 * kAT];                 // k[(n0 - m0 + d) mod N], d = -(kAT - 1) .. kAT - 1
+constexpr int kASplit = 8;  // CTAs per cluster sharing one output tile
+
+// The 4 x 4 partial sums of this thread over the chunks m0 = first, first + step, ... (x tiles staged
+// in xs, kernel values in ks).
+template <typename IN>
+__device__ __forceinline__ void analyticPartial(const IN* __restrict__ in, const float* __restrict__ kern, int N, int nL,
+                                                int n0, int l0, int first, int step, float (&xs)[kAT][kAT],
+                                                float (&ks)[2 * kAT], float (&tot)[4][4]) {
     const int tid = threadIdx.x;
-    const int ty = tid / 8, tx = tid % 8;  // sample group (4 samples), line group (4 lines)
-    const int n0 = blockIdx.y * kAT, l0 = blockIdx.x * kAT;
-    float tot[4][4], acc[4][4];
+    const int ty = tid / 8, tx = tid % 8;
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) tot[i][j] = 0.0f;
-    for (int m0 = 0; m0 < N; m0 += kAT) {
+    for (int m0 = first; m0 < N; m0 += step) {
         __syncthreads();  // the previous chunk's reads are done
         for (int e = tid; e < kAT * kAT; e += kAThreads) {
             const int mm = e / kAT, ll = e % kAT;
@@ -49,12 +56,13 @@ __global__ void __launch_bounds__(kAThreads) analyticEnvKernel(const IN* __restr
             xs[mm][ll] = (m < N && l < nL) ? toFloat(in[static_cast<size_t>(m) * nL + l]) : 0.0f;
         }
         for (int e = tid; e < 2 * kAT - 1; e += kAThreads) {
-            int d = n0 - m0 + e - (kAT - 1);  // in (-N, N)
+            int d = n0 - m0 + e - (kAT - 1);  // in (-2N, N)
             d %= N;
             if (d < 0) d += N;
             ks[e] = __ldg(kern + d);
         }
         __syncthreads();
+        float acc[4][4];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -85,6 +93,12 @@ __global__ void __launch_bounds__(kAThreads) analyticEnvKernel(const IN* __restr
 #pragma unroll
             for (int j = 0; j < 4; j++) tot[i][j] += acc[i][j];
     }
+}
+
+template <typename IN, typename OUT>
+__device__ __forceinline__ void analyticStore(const IN* __restrict__ in, OUT* __restrict__ out, int N, int nL, int n0,
+                                              int l0, const float (&h)[4][4]) {
+    const int ty = threadIdx.x / 8, tx = threadIdx.x % 8;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const int n = n0 + ty * 4 + i;
@@ -95,9 +109,57 @@ __global__ void __launch_bounds__(kAThreads) analyticEnvKernel(const IN* __restr
             if (l >= nL) continue;
             const size_t o = static_cast<size_t>(n) * nL + l;
             const float x = toFloat(in[o]);
-            out[o] = clampCast<OUT>(sqrtf(fmaf(x, x, tot[i][j] * tot[i][j])));
+            out[o] = clampCast<OUT>(sqrtf(fmaf(x, x, h[i][j] * h[i][j])));
         }
     }
+}
+
+// Cluster of kASplit CTAs along z per output tile.
+template <typename IN, typename OUT>
+__global__ void __cluster_dims__(1, 1, kASplit) __launch_bounds__(kAThreads)
+    analyticEnvClusterKernel(const IN* __restrict__ in, OUT* __restrict__ out, const float* __restrict__ kern, int N,
+                             int nL) {
+    namespace cg = cooperative_groups;
+    __shared__ __align__(16) float xs[kAT][kAT];
+    __shared__ float ks[2 * kAT];
+    __shared__ float part[kAThreads][16];  // this CTA's partial tile, per thread
+    cg::cluster_group cluster = cg::this_cluster();
+    const unsigned rank = cluster.block_rank();
+    const int n0 = blockIdx.y * kAT, l0 = blockIdx.x * kAT;
+    float tot[4][4];
+    analyticPartial<IN>(in, kern, N, nL, n0, l0, static_cast<int>(rank) * kAT, kASplit * kAT, xs, ks, tot);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) part[threadIdx.x][i * 4 + j] = tot[i][j];
+    cluster.sync();  // every partial tile is in its CTA's shared memory
+    if (rank == 0) {
+        float h[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) h[i][j] = tot[i][j];
+        for (unsigned r = 1; r < kASplit; r++) {
+            const float* rp = cluster.map_shared_rank(&part[threadIdx.x][0], r);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) h[i][j] += rp[i * 4 + j];
+        }
+        analyticStore<IN, OUT>(in, out, N, nL, n0, l0, h);
+    }
+    cluster.sync();  // the other CTAs keep their shared memory until rank 0 has read it
+}
+
+template <typename IN, typename OUT>
+__global__ void __launch_bounds__(kAThreads) analyticEnvKernel(const IN* __restrict__ in, OUT* __restrict__ out,
+                                                               const float* __restrict__ kern, int N, int nL) {
+    __shared__ __align__(16) float xs[kAT][kAT];
+    __shared__ float ks[2 * kAT];
+    const int n0 = blockIdx.y * kAT, l0 = blockIdx.x * kAT;
+    float tot[4][4];
+    analyticPartial<IN>(in, kern, N, nL, n0, l0, 0, kAT, xs, ks, tot);
+    analyticStore<IN, OUT>(in, out, N, nL, n0, l0, tot);
 }
 
 }  // namespace
@@ -154,8 +216,19 @@ int sb_analytic_env_run(const sb_analytic_plan* p, const void* in, int in_dtype,
     dim3 grid((nL + kAT - 1) / kAT, (N + kAT - 1) / kAT);
     SB_REQUIRE(grid.y <= 65535u, "sb_analytic_env_run: %d samples exceed the grid", N);
     cudaStream_t st = S(stream);
-#define SB_AN(IT, OT) \
-    analyticEnvKernel<IT, OT><<<grid, kAThreads, 0, st>>>(static_cast<const IT*>(in), static_cast<OT*>(out), p->dK, N, nL)
+    // split the input range over a cluster when the tiles alone leave the GPU mostly idle and each
+    // CTA still gets at least two chunks
+    const bool split = static_cast<long>(grid.x) * grid.y < 8L * smCount() && N >= 2 * kASplit * kAT;
+    dim3 gridSplit(grid.x, grid.y, kASplit);
+#define SB_AN(IT, OT)                                                                                                  \
+    do {                                                                                                               \
+        if (split)                                                                                                     \
+            analyticEnvClusterKernel<IT, OT><<<gridSplit, kAThreads, 0, st>>>(static_cast<const IT*>(in),              \
+                                                                               static_cast<OT*>(out), p->dK, N, nL);  \
+        else                                                                                                           \
+            analyticEnvKernel<IT, OT><<<grid, kAThreads, 0, st>>>(static_cast<const IT*>(in), static_cast<OT*>(out),   \
+                                                                  p->dK, N, nL);                                       \
+    } while (0)
     if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_AN(int16_t, float);
     else if (in_dtype == SB_INT16) SB_AN(int16_t, int16_t);
     else if (out_dtype == SB_FLOAT32) SB_AN(float, float);
