@@ -242,6 +242,10 @@ def profile_case(case: str):
     elif case == "mv":
         x = torch.randn((16, 128, 2048), dtype=torch.complex64, device="cuda")
         mv_beamform(x, 32, 5, 1.5, False, 0.01, 1e6)
+    elif case == "pcg":
+        x = torch.randn((16, 64, 2048), device="cuda") * 1000.0
+        from supra_b200.api import mv_beamform_pcg
+        mv_beamform_pcg(x, 32, 5)
     elif case == "das3d":
         from supra_b200 import workloads as W
         g2 = W.c2_geometry()
@@ -268,7 +272,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements (c0, c2, c3, c4)")
     ap.add_argument("--frames", type=int, default=64, help="frames per launch (64 = the named workload)")
-    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d"],
+    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg"],
                     help="run one small case for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:

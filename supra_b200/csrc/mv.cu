@@ -414,30 +414,50 @@ __device__ __forceinline__ MvOut<T> solveRegs(GE* Gs, int GP, int L, int sz, T l
 template <int NR, class GE>
 __device__ __forceinline__ MvOut<float> solvePcgRegs(const GE* Gs, int GP, int sz, float loading, int lane,
                                                      const V<float> (&xbar)[NR], float power, int K, int maxIt, float thr) {
-    float A[NR][32 * NR], dg[NR];
+    // R stays in the shared-memory tile (rows of pitch GP, read as aligned pairs); the covariance
+    // accumulators of the sliding window are live across the solve, so R is not copied to registers
+    float dg[NR];
     bool valid[NR];
 #pragma unroll
     for (int q = 0; q < NR; q++) {
         const int i = lane + 32 * q;
         valid[q] = i < sz;
-#pragma unroll
-        for (int j = 0; j < 32 * NR; j++) {
-            float v = 0.0f;
-            if (valid[q] && j < sz) v = Gs[i * GP + j].re + (i == j ? loading : 0.0f);
-            A[q][j] = v;
-        }
         dg[q] = valid[q] ? Gs[i * GP + i].re + loading : 1.0f;
     }
+    // o = R v on the sz x sz block. The loop runs over whole groups of four columns (a warp-uniform
+    // trip count, no per-column branch): the vectors are zero on rows >= sz, so the columns past sz
+    // (finite window sums of the tile) contribute nothing. Four independent accumulators per row.
+    auto pick = [&](const float (&v)[NR], int qq) {
+        float r = v[0];
+#pragma unroll
+        for (int k = 1; k < NR; k++) r = qq == k ? v[k] : r;
+        return r;
+    };
+    const int jmax = (sz + 3) & ~3;
     auto matvec = [&](const float (&v)[NR], float (&o)[NR]) {
+        float p4[NR][4];
 #pragma unroll
-        for (int q = 0; q < NR; q++) o[q] = 0.0f;
+        for (int q = 0; q < NR; q++)
 #pragma unroll
-        for (int j = 0; j < 32 * NR; j++) {
-            if (j >= sz) break;  // warp-uniform
-            const float vj = __shfl_sync(kFull, v[j >> 5], j & 31);
+            for (int c = 0; c < 4; c++) p4[q][c] = 0.0f;
+        for (int j = 0; j < jmax; j += 4) {
+            float vj[4];
 #pragma unroll
-            for (int q = 0; q < NR; q++) o[q] = fmaf(A[q][j], vj, o[q]);
+            for (int c = 0; c < 4; c++) vj[c] = __shfl_sync(kFull, pick(v, (j + c) >> 5), (j + c) & 31);
+#pragma unroll
+            for (int q = 0; q < NR; q++) {
+                const GE* row = &Gs[(valid[q] ? lane + 32 * q : 0) * GP + j];
+                const float2 a0 = *reinterpret_cast<const float2*>(row);
+                const float2 a1 = *reinterpret_cast<const float2*>(row + 2);
+                p4[q][0] = fmaf(a0.x, vj[0], p4[q][0]);
+                p4[q][1] = fmaf(a0.y, vj[1], p4[q][1]);
+                p4[q][2] = fmaf(a1.x, vj[2], p4[q][2]);
+                p4[q][3] = fmaf(a1.y, vj[3], p4[q][3]);
+            }
         }
+#pragma unroll
+        for (int q = 0; q < NR; q++)
+            o[q] = valid[q] ? fmaf(loading, v[q], (p4[q][0] + p4[q][1]) + (p4[q][2] + p4[q][3])) : 0.0f;
     };
     auto dot = [&](const float (&u)[NR], const float (&w)[NR]) {
         float acc = 0.0f;
@@ -464,12 +484,23 @@ __device__ __forceinline__ MvOut<float> solvePcgRegs(const GE* Gs, int GP, int s
         matvec(x, t);  // r = b - A x
 #pragma unroll
         for (int q = 0; q < NR; q++) r[q] = valid[q] ? fmaf(-1.0f, t[q], 1.0f) : 0.0f;
-        residualNorm = sqrtf(dot(r, r));
         float sv[NR];
+        float rr = 0.0f, rs = 0.0f;
 #pragma unroll
-        for (int q = 0; q < NR; q++) sv[q] = r[q] / dg[q];
+        for (int q = 0; q < NR; q++) {
+            sv[q] = r[q] / dg[q];
+            rr = fmaf(r[q], r[q], rr);
+            rs = fmaf(r[q], sv[q], rs);
+        }
+        // the two reductions interleaved (independent shuffle chains)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            rr += __shfl_xor_sync(kFull, rr, o);
+            rs += __shfl_xor_sync(kFull, rs, o);
+        }
+        residualNorm = sqrtf(rr);
         const float deltaOld = deltaNew;
-        deltaNew = dot(r, sv);
+        deltaNew = rs;
         const float beta = deltaNew / deltaOld;
 #pragma unroll
         for (int q = 0; q < NR; q++) d[q] = fmaf(beta, d[q], sv[q]);
@@ -722,6 +753,12 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
         const uint32_t sl = i / (a.ringPitch - a.nCh), ch = a.nCh + i % (a.ringPitch - a.nCh);
         ring[static_cast<size_t>(sl) * a.ringPitch + ch].re = 0.0f;
         if constexpr (C) ring[static_cast<size_t>(sl) * a.ringPitch + ch].im = 0.0f;
+    }
+    // the transposed window sums fill rows and columns < L of Gs; the rest stays 0 (the PCG products
+    // run over whole groups of four columns)
+    for (uint32_t i = lane; i < static_cast<uint32_t>(32 * NR) * L_::GP; i += 32) {
+        Gs[i].re = 0.0f;
+        if constexpr (C) Gs[i].im = 0.0f;
     }
     auto slotOf = [&](uint32_t t) -> Elem<C>* { return ring + static_cast<size_t>(t % R) * a.ringPitch; };
     auto complete = [&](uint32_t t) {
