@@ -161,6 +161,13 @@ def extras(wl, plans):
     from supra_b200.api import RxBeamformer, iq_complex, mv_beamform
     from supra_b200 import workloads as W
     res = {}
+    hbm, peak_kind = peaks()
+    # FP32 FMA peak of the SIMT pipes at the measured maximum SM clock (148 SMs x 128 lanes x 2 flop)
+    fp32_tflops = 148 * 128 * 2 * 1.965e9 / 1e12
+
+    def hbm_row(nbytes, ms):
+        gbs = nbytes / ms / 1e6
+        return {"gb_per_s": gbs, "hbm_frac": gbs / hbm, "peak": f"{hbm:.1f} GB/s {peak_kind}", "bytes": nbytes}
     # plain per-frame GPU path on the same 64 frames: per-frame DAS kernel + IQ kernel, one frame at a time
     outs = [torch.empty((wl.geometries[p].num_depths, wl.geometries[p].num_rx), device="cuda") for p in wl.frame_probe]
 
@@ -177,14 +184,16 @@ def extras(wl, plans):
     bf0 = RxBeamformer(g0)
     o0 = torch.empty((g0.num_depths, g0.num_rx), device="cuda")
     ms = _event_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0), 20)
-    res["das_c0"] = {"px_per_s": g0.num_rx * g0.num_depths / ms * 1e3, "frames_per_s": 1e3 / ms, "ms": ms}
+    res["das_c0"] = {"px_per_s": g0.num_rx * g0.num_depths / ms * 1e3, "frames_per_s": 1e3 / ms, "ms": ms,
+                     **hbm_row(rf0.numel() * 2 + o0.numel() * 4, ms)}
     # c2: 3D volume, 32 x 32 lines x 1024 depths from 1024 transmits x 256 channels x 1024 samples
     g2 = W.c2_geometry()
     rf2 = W.c2_volume(g2)
     bf2 = RxBeamformer(g2)
     o2 = torch.empty((g2.num_depths, g2.num_rx), device="cuda")
     ms = _event_ms(lambda: bf2.beamform(rf2, 1.0, window_type=1, out=o2), 3, warm=1)
-    res["das3d_c2"] = {"vox_per_s": g2.num_rx * g2.num_depths / ms * 1e3, "volumes_per_s": 1e3 / ms, "ms": ms}
+    res["das3d_c2"] = {"vox_per_s": g2.num_rx * g2.num_depths / ms * 1e3, "volumes_per_s": 1e3 / ms, "ms": ms,
+                       **hbm_row(rf2.numel() * 2 + o2.numel() * 4, ms)}
     del rf2
     # c3: complex MV, 128 x 2048 systems of 32 x 32, FP64 re-solve above 1e6
     g3, x3 = W.c3_raw_delayed()
@@ -196,7 +205,8 @@ def extras(wl, plans):
     # the other sample beamformers on the c0 frame (per-frame kernels, reference float semantics)
     for name in ("DelayAndStdDev", "CoherenceFactorDelayAndSum"):
         ms = _event_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0, beamformer=name), 10)
-        res["das_" + name] = {"px_per_s": g0.num_rx * g0.num_depths / ms * 1e3, "ms": ms}
+        res["das_" + name] = {"px_per_s": g0.num_rx * g0.num_depths / ms * 1e3, "ms": ms,
+                              **hbm_row(rf0.numel() * 2 + o0.numel() * 4, ms)}
     # MV with the PCG solve on the c0 frame's raw-delayed data (real, 128 lines x 64 channels x 2048)
     from supra_b200.api import HilbertEnvelope, mv_beamform_pcg, temporal_filter
     raw0 = bf0.raw_delay(rf0, 1.0, window_type=1)
@@ -207,11 +217,13 @@ def extras(wl, plans):
     # analytic-signal envelope (HilbertEnvelope) of the c0 image: 2 N^2 flops per scanline
     env = HilbertEnvelope(g0.num_depths)
     ms = _event_ms(lambda: env.envelope(o0), 10)
-    res["analytic_env_c0"] = {"ms": ms, "tflops": 2.0 * g0.num_depths ** 2 * g0.num_rx / ms / 1e9}
+    tf = 2.0 * g0.num_depths ** 2 * g0.num_rx / ms / 1e9
+    res["analytic_env_c0"] = {"ms": ms, "tflops": tf, "fp32_frac": tf / fp32_tflops,
+                              "peak": f"{fp32_tflops:.1f} TFLOP/s nominal FP32 FMA"}
     # temporal filter over 3 float images of 4096 x 4096 (192 MB in + 64 MB out, above the 126 MB L2)
     ims = [torch.randn((4096, 4096), device="cuda") for _ in range(3)]
     ms = _event_ms(lambda: temporal_filter(ims), 10)
-    res["temporal_filter"] = {"ms": ms, "gb_per_s": 4 * 4096 * 4096 * 4 / ms / 1e6, "images": 3}
+    res["temporal_filter"] = {"ms": ms, "images": 3, **hbm_row(4 * 4096 * 4096 * 4, ms)}
     del ims
     # c4: differentiable DAS, 16 frames: adjoint (all three gradients) vs forward
     g4, rf4 = W.c4_batch()

@@ -98,13 +98,14 @@ using namespace sb;
 
 extern "C" int sb_temporal_filter_run(const void* const* images, uint32_t num_images, const double* weights, int in_dtype,
                                       void* out, int out_dtype, uint64_t numel, sb_stream stream) {
-    SB_REQUIRE(images && out, "sb_temporal_filter_run: null argument");
+    SB_REQUIRE(images, "sb_temporal_filter_run: null image array");
     SB_REQUIRE(num_images >= 1 && num_images <= static_cast<uint32_t>(kMaxTemporalImages),
                "sb_temporal_filter_run: num_images %u not in [1, %d]", num_images, kMaxTemporalImages);
     SB_REQUIRE(in_dtype == SB_INT16 || in_dtype == SB_FLOAT32, "sb_temporal_filter_run: input dtype %d unsupported", in_dtype);
     SB_REQUIRE(out_dtype == SB_INT16 || out_dtype == SB_FLOAT32, "sb_temporal_filter_run: output dtype %d unsupported",
                out_dtype);
-    if (numel == 0) return SB_OK;
+    if (numel == 0) return SB_OK;  // empty images (their data pointers may be null)
+    SB_REQUIRE(out, "sb_temporal_filter_run: null output");
     TemporalArgs a;
     bool aligned = (reinterpret_cast<uintptr_t>(out) % 16) == 0;
     for (uint32_t k = 0; k < num_images; k++) {
