@@ -140,14 +140,17 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         uint32_t off;
         float wA, wB;
     };
-    auto geom = [&](int j) -> G {
+    // geometry of element j; `count` adds its window weight to wsum (false for the clamped look-ahead
+    // past the range, which repeats the last element so that every address stays valid without a branch)
+    auto geom = [&](int j, bool count) -> G {
         const ElemRec e = el[j];
         float w;
         if (DEEP) {
             w = e.wDeep;
         } else {
             w = lutIndexWeight(lut, __fmul_rn(e.dx, invMax));
-            wsum = __fadd_rn(wsum, w);
+            const float ws = __fadd_rn(wsum, w);
+            wsum = count ? ws : wsum;
         }
         const float ex = __fsub_rn(e.xel, xz);
         float t = __fadd_rn(s.iD, __fadd_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2)), d));
@@ -167,7 +170,7 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
     if constexpr (K >= 8) {
         // wide packs: one element's gathers in flight while the next element's geometry is computed
         // (two sample registers per frame instead of four, so 8 frames fit the register budget)
-        G g = geom(j0);
+        G g = geom(j0, true);
         for (int j = j0; j < j1; j++) {
             int16_t a[K], b[K];
 #pragma unroll
@@ -175,7 +178,7 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
                 a[f] = __ldg(tb[f] + g.off);
                 b[f] = __ldg(tb[f] + g.off + 1);
             }
-            const G gn = j + 1 < j1 ? geom(j + 1) : g;
+            const G gn = geom(min(j + 1, j1 - 1), j + 1 < j1);
 #pragma unroll
             for (int f = 0; f < K; f++)
                 acc.v[f] = fmaf(g.wB, s16ToFloat(b[f]), fmaf(g.wA, static_cast<float>(a[f]), acc.v[f]));
@@ -184,8 +187,8 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         return;
     }
     int16_t a0[K], b0[K], a1[K], b1[K];
-    G g0 = geom(j0);
-    G g1 = j0 + 1 < j1 ? geom(j0 + 1) : g0;
+    G g0 = geom(j0, true);
+    G g1 = geom(min(j0 + 1, j1 - 1), j0 + 1 < j1);
     // all slots load valid addresses (empty pack slots alias frame 0, the step past the last element
     // repeats it), so the loads carry no predicate
 #pragma unroll
@@ -199,7 +202,7 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
             a1[f] = __ldg(tb[f] + g1.off);
             b1[f] = __ldg(tb[f] + g1.off + 1);
         }
-        const G g2 = j + 2 < j1 ? geom(j + 2) : g1;
+        const G g2 = geom(min(j + 2, j1 - 1), j + 2 < j1);
 #pragma unroll
         for (int f = 0; f < K; f++) {
             acc.v[f] = fmaf(g0.wB, s16ToFloat(b0[f]), fmaf(g0.wA, static_cast<float>(a0[f]), acc.v[f]));
