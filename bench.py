@@ -307,6 +307,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     from supra_b200.api import BatchedDasIq, RxBeamformer, check_device_errors
+    from supra_b200.replicas import job_rate
     from supra_b200.workloads import c1_workload
 
     wl = c1_workload(num_frames=args.frames, device="cuda", seed0=1000 + 100 * rank)
@@ -337,12 +338,8 @@ def main():
     check_device_errors()
     per = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     total_ms = evs[0].elapsed_time(evs[-1])
-    t = torch.tensor([total_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
     px = wl.beamformed_px
-    value = px * args.steps * world / (total_ms / 1e3)
+    value, total_ms = job_rate(px, args.steps, total_ms, device="cuda")
     kern_ms = statistics.mean(per)
     alg_bytes = wl.rf_bytes + wl.iq_bytes(4)
     hbm, peak_kind = peaks()
@@ -372,10 +369,7 @@ def main():
         e2e_step()
     b.record(stream)
     torch.cuda.synchronize()
-    e_ms = torch.tensor([a.elapsed_time(b)], device="cuda")
-    if world > 1:
-        dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
-    e2e_value = px * args.e2e_steps * world / (float(e_ms.item()) / 1e3)
+    e2e_value, _ = job_rate(px, args.e2e_steps, a.elapsed_time(b), device="cuda")
 
     extra = None
     if world == 1 and not args.no_extras:
