@@ -370,6 +370,11 @@ int sb_batch_autotune(sb_batch_plan* plan, const char* cache_path, int32_t* ctas
 /* Device-side failure flag shared by the kernels with bounded waits: returns SB_ERR_TIMEOUT if any
  * wait gave up since the last call (and clears the flag when reset != 0). Synchronises the device. */
 int sb_check_device_errors(int reset);
+/* Self-test of that failure path (no reference counterpart): a kernel waits on an mbarrier that nothing
+ * arrives at (arrive = 0) with a limit of `polls` polls, gives up, raises the flag and returns; with
+ * arrive = 1 the wait completes. *completed (may be NULL) receives 1 if the wait completed. No fault:
+ * the context stays usable. Synchronises `stream`. */
+int sb_selftest_bounded_wait(uint32_t polls, int arrive, int* completed, sb_stream stream);
 
 /* ---------------------------------------------------------------- adjoint DAS */
 
