@@ -19,6 +19,8 @@ from supra_b200.abi import sb_geometry, SB_FLOAT32, SB_INT16, SB_UINT8
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libsupra_ref.so")
+# the reference's own CUDA kernels built without fast-math or FMA contraction (make -C oracle refgpu)
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libsupra_ref_gpu.so")
 
 _vp = C.c_void_p
 _lib = None
@@ -30,6 +32,7 @@ def build(ref: bool = True) -> None:
     subprocess.check_call(["make", "-s", "-C", HERE, "all"])
     if ref and os.path.isdir("/root/reference/src/SupraLib"):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+        subprocess.check_call(["make", "-s", "-C", HERE, "refgpu"])
 
 
 def lib() -> C.CDLL:
@@ -196,6 +199,71 @@ def analytic_env(img: np.ndarray) -> np.ndarray:
         m[1:(N + 1) // 2] = 2.0
     z = np.fft.ifft(np.fft.fft(x, axis=0) * m[:, None], axis=0)
     return np.abs(z)
+
+
+# ------------------------------------------------------------------ reference GPU kernels
+_refg = None
+
+
+def refgpu_lib() -> Optional[C.CDLL]:
+    """The reference's CUDA kernels (oracle/_ref/libsupra_ref_gpu.so), None when not built."""
+    global _refg
+    if _refg is None and os.path.exists(REF_GPU_LIB):
+        _refg = C.CDLL(REF_GPU_LIB)
+    return _refg
+
+
+def refg_das(geom, rf: np.ndarray, beamformer=0, f_number=1.0, c_mm_s=None, window=1, window_param=0.0,
+             interp_tx=False, additional_offset=0) -> np.ndarray:
+    """RxBeamformerCuda::performRxBeamforming of the reference on the GPU: [num_depths][num_rx]."""
+    g = geom.ctypes()
+    x = np.ascontiguousarray(rf, np.int16)
+    out = np.zeros(geom.num_depths * geom.num_rx, np.float32)
+    c = geom.speed_of_sound_mm_s if c_mm_s is None else c_mm_s
+    assert refgpu_lib().refg_das(C.byref(g), _vp(_p(x)), _vp(_p(out)), C.c_double(f_number), C.c_double(c),
+                                 C.c_int(window), C.c_float(window_param), C.c_int(int(interp_tx)),
+                                 C.c_int32(additional_offset), C.c_int(beamformer), C.c_double(geom.depth_mm)) == 0
+    return out.reshape(geom.num_depths, geom.num_rx)
+
+
+def refg_rawdelay(geom, rf: np.ndarray, f_number=1.0, window=1, window_param=0.0) -> np.ndarray:
+    g = geom.ctypes()
+    x = np.ascontiguousarray(rf, np.int16)
+    out = np.zeros(geom.num_rx * geom.num_channels * geom.num_depths, np.float32)
+    assert refgpu_lib().refg_rawdelay(C.byref(g), _vp(_p(x)), _vp(_p(out)), C.c_double(f_number),
+                                      C.c_double(geom.speed_of_sound_mm_s), C.c_int(window), C.c_float(window_param),
+                                      C.c_double(geom.depth_mm)) == 0
+    return out.reshape(geom.num_rx, geom.num_channels, geom.num_depths)
+
+
+def refg_hilbert(img: np.ndarray, filter_length: int) -> np.ndarray:
+    x = np.ascontiguousarray(img, np.float32)
+    out = np.zeros_like(x)
+    assert refgpu_lib().refg_hilbert(_vp(_p(x)), _vp(_p(out)), C.c_uint32(x.shape[1]), C.c_uint32(x.shape[0]),
+                                     C.c_uint32(filter_length)) == 0
+    return out
+
+
+def refg_logcompress(img: np.ndarray, dynamic_range: float, gain: float, in_max: float, uint8=False) -> np.ndarray:
+    x = np.ascontiguousarray(img, np.float32)
+    out = np.zeros(x.shape, np.uint8 if uint8 else np.float32)
+    assert refgpu_lib().refg_logcompress(_vp(_p(x)), _vp(_p(out)), C.c_uint32(x.shape[1]), C.c_uint32(x.shape[0]),
+                                         C.c_double(dynamic_range), C.c_double(gain), C.c_double(in_max),
+                                         C.c_int(int(uint8))) == 0
+    return out
+
+
+def refg_iq(img: np.ndarray, fs: float, reference_frequency: float, cutoff: float, lowpass_length: int,
+            bandpass_length: int, decimation: int, frequencies, bandwidths, weights) -> np.ndarray:
+    x = np.ascontiguousarray(img, np.float32)
+    nS, nRx = x.shape
+    f, b, w = (np.ascontiguousarray(v, np.float64) for v in (frequencies, bandwidths, weights))
+    out = np.zeros((nS // decimation if decimation > 1 else nS) * nRx, np.float32)  # decimatedSignalLength
+    assert refgpu_lib().refg_iq(_vp(_p(x)), _vp(_p(out)), C.c_uint32(nRx), C.c_uint32(nS), C.c_double(fs),
+                                C.c_double(reference_frequency), C.c_double(cutoff), C.c_uint32(lowpass_length),
+                                C.c_uint32(bandpass_length), C.c_uint32(decimation), C.c_uint32(len(f)), _vp(_p(f)),
+                                _vp(_p(b)), _vp(_p(w))) == 0
+    return out.reshape(-1, nRx)
 
 
 def das_adjoint64(geom, rf: np.ndarray, apod, gout: np.ndarray, c_mm_s=None, f_number=1.0, window=1, window_param=0.0):
