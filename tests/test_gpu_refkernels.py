@@ -91,3 +91,25 @@ def test_iq_magnitude_matches_reference_kernel(ref, rf_image, dec, filters):
     got = IQDemodulator(40e6, 2.5e6, 51, 33, refs, bws, ws).demodulate_magnitude(rf_image, dec).cpu().numpy()
     assert got.shape == want.shape
     assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want))
+
+
+def test_c1_batched_path_matches_reference_kernel(ref):
+    """The headline path: one frame of each c1 probe (P64, P128, P192) through the batched pack kernel,
+    its RF against the reference's own DAS kernel on the same frames (within 1e-6 of the peak: the pack
+    kernel contracts the per-frame sums into FMAs; the +-FLT_MAX of empty apertures equal)."""
+    from supra_b200.api import BatchedDasIq, RxBeamformer
+    from supra_b200.workloads import c1_workload
+    wl = c1_workload(num_frames=3, device="cuda")
+    plans = [RxBeamformer(g) for g in wl.geometries]
+    b = BatchedDasIq([(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)], 1.0, 1540e3, 1, 0.0, 5e6, 2.5e6, 32, 4,
+                     ctas_per_sm=8, depth_tile=128, frames_per_pack=4)
+    b.enable_rf_outputs()
+    b.run(use_graph=False)
+    torch.cuda.synchronize()
+    for k, p in enumerate(wl.frame_probe):
+        g = wl.geometries[p]
+        want = ref.refg_das(g, wl.rf[k].cpu().numpy(), 0, 1.0, c_mm_s=1540e3, window=1)
+        got = b.rf_outputs[k].cpu().numpy()
+        big = np.abs(want) > 1e30
+        assert np.array_equal(got[big], want[big])
+        assert np.max(np.abs(got[~big] - want[~big])) <= 1e-6 * np.max(np.abs(want[~big])), f"probe {p}"
