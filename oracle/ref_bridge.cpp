@@ -104,7 +104,10 @@ int refDas(const sb_geometry* g, const float* rf, float* out, double fNumber, do
     LocationType F = static_cast<LocationType>(fNumber);
     bool is3D = g->rx_layout[0] > 1 && g->rx_layout[1] > 1;
     vec2T<uint32_t> elementLayout{g->element_layout[0], g->element_layout[1]};
-    for (uint32_t scanlineIdx = 0; scanlineIdx < g->num_rx; scanlineIdx++) {
+    // scanlines are independent (as the kernel's threads are): spread over the host cores
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t sl = 0; sl < static_cast<int64_t>(g->num_rx); sl++) {
+        const uint32_t scanlineIdx = static_cast<uint32_t>(sl);
         for (uint32_t r = 0; r < g->num_depths; r++) {
             LocationType d = ds[r];
             ScanlineRxParameters3D scanline = lines[scanlineIdx];
