@@ -400,7 +400,7 @@ int launchBatch(sb_batch_plan* p, int nt, int ctas, int fp, int staged, cudaStre
             if (fp == 4) return launchStagedPack<4, 1>(a, grid, st);
             return ctas == 2 ? launchStagedPack<2, 2>(a, grid, st) : launchStagedPack<2, 1>(a, grid, st);
         }
-#define SB_PACK_LAUNCH(FPV, NTV, MB) batchPackKernel<FPV, NTV, MB><<<grid, NTV, 0, st>>>(a)
+#define SB_PACK_LAUNCH(FPV, NTV, MB) batchPackKernel<FPV, NTV, MB, 0><<<grid, NTV, 0, st>>>(a)
         if (nt != 128 && nt != 256) return fail(SB_ERR_INVALID_ARG, "sb_batch: pack kernel block %d not in {128, 256}", nt);
         // register budget: `ctas` resident CTAs of nt threads per SM
         const int mb = std::max(1, std::min(ctas, 2048 / nt));

@@ -54,6 +54,7 @@ struct PackArgs {
     int taps, half, dec;
     WindowLut lut;
     float lp[kIqMaxTaps + 1];
+    PackDev single;  // MODE 1: the one frame (no pack table)
 };
 
 __device__ __forceinline__ int floorDiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
@@ -65,7 +66,7 @@ struct PackAcc {
 
 // Sum of one depth over the element table for the first K frames of the pack (the reference's
 // sampleBeamform2D per frame, with the per-element geometry shared).
-template <int FP, int K, bool DEEP, bool USE_OFFSET>
+template <int FP, int K, bool DEEP, bool USE_OFFSET, bool EXACT>
 __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float* lut, const PackDev& P, const LineK& s,
                                           const int16_t* const (&tb)[FP], int nf, float d, float aDT, float invMax,
                                           float& wsum, int& cnt, PackAcc<FP>& acc) {
@@ -96,6 +97,24 @@ __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float*
         // last sample with zero fraction -> lerp(nS - 2, nS - 1) with weights (0, 1) = RF[nS - 1];
         // no sample -> weight 0 on an in-range index.
         const bool interior = static_cast<uint32_t>(delay) < nS - 1;
+        if constexpr (EXACT) {
+            // the reference's arithmetic: sample += w * ((1 - f) * x[i] + f * x[i + 1]); the last sample
+            // with zero fraction as (i = nS - 2, f = 1), which gives w * x[nS - 1] exactly; no sample as w = 0
+            const bool lastOne = !interior && static_cast<uint32_t>(delay) < nS && frac == 0.0f;
+            const uint32_t idx = interior ? static_cast<uint32_t>(delay) : (lastOne ? nS - 2 : 0u);
+            const float wE = (interior || lastOne) ? w : 0.0f;
+            const float fE = interior ? frac : (lastOne ? 1.0f : 0.0f);
+            const uint32_t off = static_cast<uint32_t>(e.ch) + idx;
+#pragma unroll
+            for (int f = 0; f < K; f++) {
+                const int16_t* p = tb[f] + off;
+                const float v0 = static_cast<float>(__ldg(p));
+                const float v1 = s16ToFloat(__ldg(p + 1));
+                acc.v[f] = __fadd_rn(acc.v[f],
+                                     __fmul_rn(wE, __fadd_rn(__fmul_rn(__fsub_rn(1.0f, fE), v0), __fmul_rn(fE, v1))));
+            }
+            continue;
+        }
         uint32_t idx;
         float wA, wB;
         if (__all_sync(__activemask(), interior)) {  // vote among the lanes present here (the loop and the depth range diverge)
@@ -127,7 +146,7 @@ __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float*
 // of elements inside the aperture (contiguous when the table is ordered by x) and each weight is the
 // window-LUT entry of dx / min(aDT, maxElementDistance), summed into wsum in element order (the
 // reference's order).
-template <int FP, int K, bool USE_OFFSET, bool DEEP>
+template <int FP, int K, bool USE_OFFSET, bool DEEP, bool EXACT>
 __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, int j1, const float* lut, const PackDev& P,
                                                    const LineK& s, const int16_t* const (&tb)[FP], float d,
                                                    float invMax, float& wsum, PackAcc<FP>& acc) {
@@ -162,8 +181,13 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         const bool lastOne = !interior && static_cast<uint32_t>(delay) < nS && frac == 0.0f;
         G g;
         const uint32_t idx = interior ? static_cast<uint32_t>(delay) : (lastOne ? nS - 2 : 0u);
-        g.wB = interior ? __fmul_rn(w, frac) : (lastOne ? w : 0.0f);
-        g.wA = interior ? __fmul_rn(w, __fsub_rn(1.0f, frac)) : 0.0f;
+        if constexpr (EXACT) {  // (weight, fraction) for the reference's arithmetic, see packDepth
+            g.wA = (interior || lastOne) ? w : 0.0f;
+            g.wB = interior ? frac : (lastOne ? 1.0f : 0.0f);
+        } else {
+            g.wB = interior ? __fmul_rn(w, frac) : (lastOne ? w : 0.0f);
+            g.wA = interior ? __fmul_rn(w, __fsub_rn(1.0f, frac)) : 0.0f;
+        }
         g.off = static_cast<uint32_t>(e.ch) + idx;  // e.ch holds the row offset
         return g;
     };
@@ -205,7 +229,12 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         const G g2 = geom(min(j + 2, j1 - 1), j + 2 < j1);
 #pragma unroll
         for (int f = 0; f < K; f++) {
-            acc.v[f] = fmaf(g0.wB, s16ToFloat(b0[f]), fmaf(g0.wA, static_cast<float>(a0[f]), acc.v[f]));
+            if constexpr (EXACT)
+                acc.v[f] = __fadd_rn(acc.v[f], __fmul_rn(g0.wA, __fadd_rn(__fmul_rn(__fsub_rn(1.0f, g0.wB),
+                                                                                    static_cast<float>(a0[f])),
+                                                                          __fmul_rn(g0.wB, s16ToFloat(b0[f])))));
+            else
+                acc.v[f] = fmaf(g0.wB, s16ToFloat(b0[f]), fmaf(g0.wA, static_cast<float>(a0[f]), acc.v[f]));
             a0[f] = a1[f];
             b0[f] = b1[f];
         }
@@ -235,7 +264,7 @@ __device__ __forceinline__ void apertureRange(const ElemRec* el, int n, float aD
 // One beamformed depth for the first K frames of the pack: the deep path (every element active
 // with its precomputed weight), the aperture range of an x-ordered table, or the element-by-element
 // aperture test; then the reference's normalisation (sum / weight sum * count) and clamped cast.
-template <int FP, int K>
+template <int FP, int K, bool EXACT>
 __device__ __forceinline__ void packRow(const ElemRec* el, int n, const float* lut, const PackDev& P, const LineK& s,
                                         const int16_t* const (&tb)[FP], int nf, float d, int deepOk, int sortedX,
                                         float sumDeep, int cntDeep, PackAcc<FP>& acc) {
@@ -244,21 +273,21 @@ __device__ __forceinline__ void packRow(const ElemRec* el, int n, const float* l
     float wsum = 0.0f;
     int cnt = 0;
     if (deepOk && aDT >= s.maxDistX && n > 0) {
-        if (useOffset) packDepthPipelined<FP, K, true, true>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
-        else packDepthPipelined<FP, K, false, true>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
+        if (useOffset) packDepthPipelined<FP, K, true, true, EXACT>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
+        else packDepthPipelined<FP, K, false, true, EXACT>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
         wsum = sumDeep;
         cnt = cntDeep;
     } else if (sortedX) {
         const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
         int j0, j1;
         apertureRange(el, n, aDT, j0, j1);
-        if (useOffset) packDepthPipelined<FP, K, true, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
-        else packDepthPipelined<FP, K, false, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
+        if (useOffset) packDepthPipelined<FP, K, true, false, EXACT>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
+        else packDepthPipelined<FP, K, false, false, EXACT>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
         cnt = j1 - j0;
     } else {
         const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
-        if (useOffset) packDepth<FP, K, false, true>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
-        else packDepth<FP, K, false, false>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
+        if (useOffset) packDepth<FP, K, false, true, EXACT>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
+        else packDepth<FP, K, false, false, EXACT>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
     }
 #pragma unroll
     for (int f = 0; f < K; f++) {
@@ -267,12 +296,17 @@ __device__ __forceinline__ void packRow(const ElemRec* el, int n, const float* l
     }
 }
 
-template <int FP, int NT, int MINB>
+// MODE 0: batched DAS + complex IQ over frame packs (RF contracted into FMAs). MODE 1: one frame,
+// DAS only, bit-identical to the reference's arithmetic (sb_das_run's single-frame path): items carry
+// no low-pass halo and the RF is written straight to the output image.
+template <int FP, int NT, int MINB, int MODE>
 __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
+    constexpr bool EXACT = MODE == 1;
     __shared__ ElemRec el[kMaxApertureElems];
     __shared__ float lut[64];
     constexpr int kHalf = FP >= 4 ? FP / 2 : 1;
-    __shared__ float seg[FP][kPackRows];  // the item's beamformed depths (segment + low-pass halo)
+    // the item's beamformed depths (segment + low-pass halo), for the IQ epilogue of MODE 0
+    __shared__ float seg[MODE == 0 ? FP : 1][MODE == 0 ? kPackRows : 1];
     __shared__ uint32_t itemIdx;
     __shared__ int nEl, cntDeep, deepOk, sortedX;
     __shared__ float sumDeep;
@@ -285,7 +319,7 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         const uint32_t it = itemIdx;
         if (it >= a.nItems) return;
         const PackItem pi = a.items[it];
-        const PackDev& P = a.packs[pi.pack];
+        const PackDev& P = MODE == 1 ? a.single : a.packs[pi.pack];
         const LineK s = reduceLine(P.lines[pi.line]);
         const int nf = P.nf;
         // element table (as setupLine, all threads)
@@ -301,12 +335,36 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
                 r.xel = xel;
                 r.dx = __fsub_rn(xel, s.x);
                 r.wDeep = lutIndexWeight(lut, __fmul_rn(r.dx, invDeep));
-                r.ch = ch;
+                // without a channel map no element drops out: the row offset is final here
+                r.ch = P.e2c ? ch : ch * static_cast<int>(P.nS);
                 el[j] = r;
             }
         }
+        if (!P.e2c) {
+            // table in element order as filled: order and deep-aperture tests in parallel, the
+            // weight sum in element order by one thread
+            int sortedMine = 1, okMine = 1;
+            __syncthreads();
+            if (valid)
+                for (int j = tid; j < n0; j += NT) {
+                    if (j > 0 && !(el[j].dx >= el[j - 1].dx)) sortedMine = 0;
+                    if (!(fabsf(el[j].dx) <= s.maxDistX)) okMine = 0;
+                }
+            const int sortedAll = __syncthreads_and(sortedMine);
+            const int okAll = __syncthreads_and(okMine);
+            if (tid == 0) {
+                float sum = 0.0f;
+                const int m = valid ? n0 : 0;
+                for (int j = 0; j < m; j++) sum = __fadd_rn(sum, el[j].wDeep);
+                nEl = m;
+                sumDeep = sum;
+                cntDeep = m;
+                deepOk = okAll;
+                sortedX = sortedAll;
+            }
+        }
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && P.e2c) {
             int m = 0, ok = 1, sorted = 1;
             float sum = 0.0f;
             if (valid) {
@@ -333,8 +391,8 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         for (int f = 0; f < FP; f++)
             tb[f] = P.rf[f < nf ? f : 0] + static_cast<size_t>(s.txIdx) * P.nCh * P.nS;
         const int nD = static_cast<int>(P.nD);
-        const int rStart = max(0, static_cast<int>(pi.seg0) - a.half);
-        const int rEnd = min(nD, static_cast<int>(pi.seg1) + a.half + 1);
+        const int rStart = MODE == 1 ? static_cast<int>(pi.seg0) : max(0, static_cast<int>(pi.seg0) - a.half);
+        const int rEnd = MODE == 1 ? min(nD, static_cast<int>(pi.seg1)) : min(nD, static_cast<int>(pi.seg1) + a.half + 1);
         const int so0 = static_cast<int>(pi.seg0) / a.dec;
         const int so1 = min(static_cast<int>(pi.seg1) / a.dec, nD / a.dec);
         const int nBlocks = (rEnd - rStart + NT - 1) / NT;
@@ -347,9 +405,13 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             for (int f = 0; f < FP; f++) acc.v[f] = 0.0f;
             if (r < rEnd && valid) {
                 const float d = __ldg(P.depth + r);
-                if (kw == FP) packRow<FP, FP>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
-                else if (kw == kHalf) packRow<FP, kHalf>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
-                else packRow<FP, 1>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
+                if (kw == FP) packRow<FP, FP, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
+                else if (kw == kHalf) packRow<FP, kHalf, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
+                else packRow<FP, 1, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
+            }
+            if (MODE == 1) {
+                if (r < rEnd) P.rfOut[0][pi.line + static_cast<size_t>(r) * P.nRx] = acc.v[0];
+                continue;
             }
             if (r < rEnd) {
 #pragma unroll
@@ -360,6 +422,7 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
                 }
             }
         }
+        if (MODE == 1) continue;  // the next item's first barrier orders the table's reuse
         // one barrier per item: the segment's RF is complete; its IQ outputs [so0, so1) for every frame
         __syncthreads();
         const int cntOut = max(0, so1 - so0) * nf;

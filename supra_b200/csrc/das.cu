@@ -6,10 +6,13 @@
 // sample index — are evaluated with the same IEEE float operations in the same order (explicit
 // _rn intrinsics, so nothing is contracted into FMAs), which keeps them bit-identical to the CPU
 // restatement of the reference.
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
+#include "batch_pack.cuh"
 #include "das.cuh"
 #include "das_core.cuh"
 #include "design.h"
@@ -676,6 +679,65 @@ FrameDesc frameOf(const sb_das_plan* p, const DasArgs& a) {
     return f;
 }
 
+// Single-frame path (2D, int16 channel data, float image, highest-weight transmit): the frame-pack
+// kernel with one frame, in the reference's exact arithmetic (MODE 1). Items are (scanline, 128-depth
+// segment), deepest segments first (they hold the most aperture elements), so a single frame still
+// spreads over every SM.
+constexpr int kSinglePackRows = 128;
+constexpr int kSinglePackThreads = 128;
+
+int launchSinglePack(sb_das_plan* p, const DasArgs& a, cudaStream_t st) {
+    if (!p->packItems) {
+        std::vector<PackItem> items;
+        const uint32_t nSeg = (p->numDepths + kSinglePackRows - 1) / kSinglePackRows;
+        for (uint32_t k = nSeg; k-- > 0;)
+            for (uint32_t l = 0; l < p->numRx; l++)
+                items.push_back({0u, l, k * kSinglePackRows, std::min(p->numDepths, (k + 1) * kSinglePackRows)});
+        void* di = nullptr;
+        uint32_t* dc = nullptr;
+        cudaError_t e = cudaMalloc(&di, items.size() * sizeof(PackItem));
+        if (e == cudaSuccess) e = cudaMalloc(&dc, sizeof(uint32_t));
+        if (e == cudaSuccess) e = cudaMemcpy(di, items.data(), items.size() * sizeof(PackItem), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(di);
+            cudaFree(dc);
+            return cudaFail(e, "sb_das_run: work items");
+        }
+        p->packItems = di;
+        p->packCounter = dc;
+        p->packItemCount = static_cast<uint32_t>(items.size());
+    }
+    PackArgs pa;
+    std::memset(&pa, 0, sizeof(pa));
+    pa.items = static_cast<const PackItem*>(p->packItems);
+    pa.nItems = p->packItemCount;
+    pa.counter = p->packCounter;
+    pa.dec = 1;
+    pa.lut = a.lut;
+    PackDev& d = pa.single;
+    d.lines = a.lines;
+    d.xe = a.xe;
+    d.depth = a.depth;
+    d.e2c = a.e2c;
+    d.nCh = a.nCh;
+    d.nS = a.nS;
+    d.nRx = a.nRx;
+    d.nD = a.nD;
+    d.c = a.c;
+    d.dt = a.dt;
+    d.F = a.F;
+    d.offset = a.offset;
+    d.nf = 1;
+    d.rf[0] = static_cast<const int16_t*>(a.rf);
+    d.rfOut[0] = static_cast<float*>(a.out);
+    SB_CUDA(cudaMemsetAsync(p->packCounter, 0, sizeof(uint32_t), st));
+    const unsigned grid = static_cast<unsigned>(
+        std::min<size_t>(static_cast<size_t>(smCount()) * 8, (p->packItemCount + 1)));
+    batchPackKernel<1, kSinglePackThreads, 8, 1><<<grid, kSinglePackThreads, 0, st>>>(pa);
+    SB_CHECK_LAUNCH("batchPackKernel");
+    return SB_OK;
+}
+
 int launchStaged(const sb_das_plan* p, const DasArgs& a, int rfDt, int outDt, cudaStream_t st) {
     const size_t rfSize = rfDt == SB_INT16 ? 2 : 4;
     const uint32_t maxW = stagedMaxW(p->numChannels, rfSize);
@@ -812,6 +874,8 @@ int sb_das_plan_destroy(sb_das_plan* p) {
     cudaFree(p->dDepth);
     cudaFree(p->dLines);
     cudaFree(p->adjScratch);
+    cudaFree(p->packItems);
+    cudaFree(p->packCounter);
     delete p->hLines;
     delete p->hXeMM;
     delete p->hDepthMM;
@@ -835,6 +899,10 @@ int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out,
     const bool staged = !p->is3D && !interpolate_transmits && p->maxApertureX <= kMaxApertureElems &&
                         (p->numSamples * rfSize) % 16 == 0 && (reinterpret_cast<uintptr_t>(rf) % 16) == 0 &&
                         stagedMaxW(p->numChannels, rfSize) >= 64;
+    // the frame-pack kernel with one frame (exact arithmetic) where its conditions hold
+    if (!p->is3D && !interpolate_transmits && rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32 &&
+        p->maxApertureX <= kMaxApertureElems && p->numSamples >= 2)
+        return launchSinglePack(p, a, st);
     if (staged) return launchStaged(p, a, rf_dtype, out_dtype, st);
     dim3 grid((p->numDepths + 255) / 256, p->numRx);
     const bool table3D = p->is3D && !interpolate_transmits &&

@@ -53,6 +53,11 @@ struct sb_das_plan {
     // with the plan so that repeated calls allocate nothing
     void* adjScratch = nullptr;
     size_t adjScratchBytes = 0;
+    // work items (scanline, depth segment) of the single-frame pack path of sb_das_run and its work
+    // counter, built on the first call
+    void* packItems = nullptr;
+    uint32_t packItemCount = 0;
+    uint32_t* packCounter = nullptr;
 };
 
 namespace sb {
