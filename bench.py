@@ -153,6 +153,31 @@ def run_reference(args, rank):
     }), flush=True)
 
 
+def _graph_ms(fn, n, warm=2):
+    """Device time of fn (a sequence of library launches) captured once in a CUDA graph and replayed n
+    times, so the host's launch overhead stays out of the measurement."""
+    import torch
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(warm):
+            fn()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        fn()
+    g.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(n):
+        g.replay()
+    b.record()
+    torch.cuda.synchronize()
+    del g
+    return a.elapsed_time(b) / n
+
+
 def _event_ms(fn, n, warm=2):
     import torch
     for _ in range(warm):
@@ -187,15 +212,16 @@ def extras(wl, plans):
         for k, p in enumerate(wl.frame_probe):
             plans[p].beamform(wl.rf[k], 1.0, window_type=1, out=outs[k])
             iq_complex(outs[k], 40e6, 5e6, 2.5e6, 32, 4)
-    ms = _event_ms(per_frame, 3)
+    ms = _graph_ms(per_frame, 3)
     res["per_frame_path"] = {"px_per_s": wl.beamformed_px / ms * 1e3, "frames_per_s": len(wl.rf) / ms * 1e3,
-                             "ms_per_batch": ms, "what": "same 64 frames, per-frame DAS + IQ launches"}
+                             "ms_per_batch": ms,
+                             "what": "same 64 frames, per-frame DAS + IQ launches (device time, graph-captured)"}
     # c0: one 128-line x 2048-depth frame through the per-frame DAS path
     from supra_b200 import synth
     g0, rf0 = synth.c0_frame(0, device="cuda")
     bf0 = RxBeamformer(g0)
     o0 = torch.empty((g0.num_depths, g0.num_rx), device="cuda")
-    ms = _event_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0), 20)
+    ms = _graph_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0), 20)
     res["das_c0"] = {"px_per_s": g0.num_rx * g0.num_depths / ms * 1e3, "frames_per_s": 1e3 / ms, "ms": ms,
                      **hbm_row(rf0.numel() * 2 + o0.numel() * 4, ms)}
     # c2: 3D volume, 32 x 32 lines x 1024 depths from 1024 transmits x 256 channels x 1024 samples
@@ -209,21 +235,21 @@ def extras(wl, plans):
     del rf2
     # c3: complex MV, 128 x 2048 systems of 32 x 32, FP64 re-solve above 1e6
     g3, x3 = W.c3_raw_delayed()
-    ms = _event_ms(lambda: mv_beamform(x3, W.C3_L, W.C3_T, 1.5, False, W.C3_LOADING, 1e6, with_stats=False), 3, warm=1)
+    ms = _event_ms(lambda: mv_beamform(x3, W.C3_L, W.C3_T, 1.5, False, W.C3_LOADING, 1e6, with_stats=False), 5, warm=3)
     _, st = mv_beamform(x3, W.C3_L, W.C3_T, 1.5, False, W.C3_LOADING, 1e6)
     res["mv_c3"] = {"px_per_s": x3.shape[0] * x3.shape[2] / ms * 1e3, "frames_per_s": 1e3 / ms, "ms": ms,
                     "fp64_systems": int(st.fp64_systems), "max_condition_estimate": float(st.max_condition_estimate)}
     del x3
     # the other sample beamformers on the c0 frame (per-frame kernels, reference float semantics)
     for name in ("DelayAndStdDev", "CoherenceFactorDelayAndSum"):
-        ms = _event_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0, beamformer=name), 10)
+        ms = _graph_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0, beamformer=name), 10)
         res["das_" + name] = {"px_per_s": g0.num_rx * g0.num_depths / ms * 1e3, "ms": ms,
                               **hbm_row(rf0.numel() * 2 + o0.numel() * 4, ms)}
     # MV with the PCG solve on the c0 frame's raw-delayed data (real, 128 lines x 64 channels x 2048)
     from supra_b200.api import HilbertEnvelope, mv_beamform_pcg, temporal_filter
     raw0 = bf0.raw_delay(rf0, 1.0, window_type=1)
     raw0[~(raw0.abs() < 1e30)] = 0.0
-    ms = _event_ms(lambda: mv_beamform_pcg(raw0, 32, 5), 3, warm=1)
+    ms = _event_ms(lambda: mv_beamform_pcg(raw0, 32, 5), 5, warm=3)
     res["mv_pcg_c0"] = {"px_per_s": raw0.shape[0] * raw0.shape[2] / ms * 1e3, "ms": ms, "L": 32, "T": 5}
     del raw0
     # analytic-signal envelope (HilbertEnvelope) of the c0 image: 2 N^2 flops per scanline
