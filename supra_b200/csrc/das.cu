@@ -400,28 +400,87 @@ __global__ void __launch_bounds__(256) dasVariantKernel(DasArgs a) {
 
 // 3D delay-and-sum with a per-scanline element table in shared memory (highest-weight transmit).
 // The table keeps the reference's summation order (x outer, y inner, RxSampleBeamformerDelayAndSum.h:
-// 55-57), each element's position, offsets from the scanline and channel. Once the aperture covers
-// maxElementDistance in both directions and every element of the table (depths where
+// 55-57), each element's position, channel row offset and offsets from the scanline. Once the aperture
+// covers maxElementDistance in both directions and every element of the table (depths where
 // sqrt(aDT^2) >= maxDistX, maxDistY and aDT^2 >= max(dx^2 + dz^2)), the window weights no longer
 // depend on depth: they and their running sum are computed once per scanline in the same order, so
-// results stay bit-identical to sample3D.
-struct __align__(16) Elem3D {
-    float xel, zel, dx, dz;
-    float wDeep;
-    int ch;
-    float r2;
-    int pad;
-};
+// results stay bit-identical to sample3D. The loop takes elements four at a time: delays and
+// weights of all four, then their gathers, then the four additions in element order (an element the
+// reference skips adds nothing). The table is padded to a multiple of four with elements at infinity,
+// whose delays fall beyond every record. Five CTAs per SM (48 registers): the gathers' latency is
+// hidden by occupancy and the four-element groups; eight-element groups need 80 registers and run
+// slower.
 constexpr int kMax3DElems = 1024;
+constexpr int k3DUnroll = 4;
+
+template <typename RF> __device__ __forceinline__ float ldSample(const RF* p);
+template <> __device__ __forceinline__ float ldSample<int16_t>(const int16_t* p) {
+    return static_cast<float>(__ldg(p));  // the conversion unit has room here (the ALU pipes do not)
+}
+template <> __device__ __forceinline__ float ldSample<float>(const float* p) { return __ldg(p); }
+
+// elA[j] = (x, z, deep weight, channel row offset as int bits), elB[j] = (dx, dz, dx^2 + dz^2, 0).
+template <typename RF, bool DEEP>
+__device__ __forceinline__ void das3dAccum(const float4* elA, const float4* elB, const float* lut, int nPad,
+                                           const RF* tx, uint32_t nS, float px, float pz, float ay2, float iD,
+                                           float d, float offset, float aDT2, float invX, float invY,
+                                           float& sample, float& weightAcum, int& numAdds) {
+    for (int j = 0; j < nPad; j += k3DUnroll) {
+        float w[k3DUnroll], frac[k3DUnroll], v0[k3DUnroll], v1[k3DUnroll];
+        int idx[k3DUnroll];
+        bool one[k3DUnroll], two[k3DUnroll];
+#pragma unroll
+        for (int u = 0; u < k3DUnroll; u++) {
+            const float4 A = elA[j + u];
+            bool inR = true;
+            if (DEEP) {
+                w[u] = A.z;
+            } else {
+                const float4 B = elB[j + u];
+                inR = B.z <= aDT2;
+                w[u] = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(B.x, invX)), lutGet(lut, __fmul_rn(B.y, invY))));
+                if (inR) {
+                    weightAcum = __fadd_rn(weightAcum, w[u]);
+                    numAdds++;
+                }
+            }
+            const float qx = __fsub_rn(A.x, px), qz = __fsub_rn(A.y, pz);
+            const float q = __fadd_rn(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qz, qz)), ay2);
+            const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(__fsqrt_rn(q), d)), offset);
+            // floor as unsigned, saturating at 0 for negative (and NaN) positions like the reference's
+            // conversion; positions >= 2^23 give an index >= 2^23, beyond every record
+            const float t = __fadd_rd(fmaxf(delayf, 0.0f), 8388608.0f);
+            const uint32_t delay = __float_as_uint(t) - 0x4B000000u;
+            frac[u] = __fsub_rn(delayf, __fsub_rn(t, 8388608.0f));
+            two[u] = inR && delay < nS - 1;
+            one[u] = two[u] || (inR && delay < nS && frac[u] == 0.0f);
+            idx[u] = static_cast<int>(static_cast<uint32_t>(__float_as_int(A.w)) + delay);  // used when one[u]
+        }
+#pragma unroll
+        for (int u = 0; u < k3DUnroll; u++) {
+            v0[u] = one[u] ? ldSample<RF>(tx + idx[u]) : 0.0f;
+            v1[u] = two[u] ? ldSample<RF>(tx + idx[u] + 1) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < k3DUnroll; u++) {
+            // at the last sample (frac == 0) this is 1 * v0 + 0 * 0 = v0, the reference's single read
+            const float v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac[u]), v0[u]), __fmul_rn(frac[u], v1[u]));
+            if (one[u]) sample = __fadd_rn(sample, __fmul_rn(w[u], v));
+        }
+    }
+}
 
 template <typename RF, typename OUT>
-__global__ void __launch_bounds__(256) das3dTableKernel(DasArgs a) {
+__global__ void __launch_bounds__(256, 5) das3dTableKernel(DasArgs a, int cap) {
     __shared__ float lut[64];
-    __shared__ Elem3D el[kMax3DElems];
-    __shared__ int nEl;
-    __shared__ float sumDeep, maxR2;
+    __shared__ int nEl, maxR2Bits;
+    __shared__ float sumDeep;
+    extern __shared__ float4 table3D[];
+    float4* elA = table3D;
+    float4* elB = table3D + cap;
     const int tid = threadIdx.x;
     if (tid < 64) lut[tid] = a.lut.v[tid];
+    if (tid == 0) maxR2Bits = 0;
     __syncthreads();
     const uint32_t line = blockIdx.y;
     const LineDT s = a.lines[line];
@@ -429,83 +488,87 @@ __global__ void __launch_bounds__(256) das3dTableKernel(DasArgs a) {
     const bool active = (s.activeMask >> k) & 1;
     const int nx = active ? max(static_cast<int>(s.lastX[k]) - static_cast<int>(s.firstX[k]), 0) : 0;
     const int ny = active ? max(static_cast<int>(s.lastY[k]) - static_cast<int>(s.firstY[k]), 0) : 0;
-    const int n0 = min(nx * ny, kMax3DElems);  // the host routes larger apertures to the generic kernel
+    const int n0 = min(nx * ny, cap);  // nx * ny <= maxApertureX * maxApertureY <= cap for every line
     const float invXd = __fdiv_rn(1.0f, s.maxDistX), invYd = __fdiv_rn(1.0f, s.maxDistY);
+    const bool mapped = a.e2c != nullptr;
     for (int j = tid; j < n0; j += 256) {
         const uint32_t ex = s.firstX[k] + j / ny, ey = s.firstY[k] + j % ny;
         const uint32_t e = ex + ey * a.layoutX;
-        Elem3D r;
-        r.ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(e % a.nCh);
-        r.xel = __ldg(a.xe + e);
-        r.zel = __ldg(a.ye + e);
-        r.dx = __fsub_rn(r.xel, s.x);
-        r.dz = __fsub_rn(r.zel, s.z);
-        r.r2 = __fadd_rn(__fmul_rn(r.dx, r.dx), __fmul_rn(r.dz, r.dz));
-        r.wDeep = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(r.dx, invXd)), lutGet(lut, __fmul_rn(r.dz, invYd))));
-        r.pad = 0;
-        el[j] = r;
+        const int ch = mapped ? __ldg(a.e2c + e) : static_cast<int>(e % a.nCh);
+        const float xel = __ldg(a.xe + e), zel = __ldg(a.ye + e);
+        const float dx = __fsub_rn(xel, s.x), dz = __fsub_rn(zel, s.z);
+        const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz));
+        const float wDeep = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(dx, invXd)), lutGet(lut, __fmul_rn(dz, invYd))));
+        // unmapped elements (ch < 0) are removed below; the row offset keeps them recognisable
+        const int chOff = ch < 0 ? -1 : ch * static_cast<int>(a.nS);
+        elA[j] = make_float4(xel, zel, wDeep, __int_as_float(chOff));
+        elB[j] = make_float4(dx, dz, r2, 0.0f);
+        if (!mapped && r2 == r2) atomicMax(&maxR2Bits, __float_as_int(r2));
     }
     __syncthreads();
-    if (tid == 0) {
-        int m = 0;
-        float sum = 0.0f, mr = 0.0f;
-        for (int j = 0; j < n0; j++) {
-            const Elem3D r = el[j];
-            if (r.ch < 0) continue;
-            el[m++] = r;
-            sum = __fadd_rn(sum, r.wDeep);
-            mr = fmaxf(mr, r.r2);
+    if (mapped) {
+        // channel map: drop unmapped elements in order, then the sums over the remaining ones
+        if (tid == 0) {
+            int m = 0;
+            float sum = 0.0f, mr = 0.0f;
+            for (int j = 0; j < n0; j++) {
+                const float4 A = elA[j], B = elB[j];
+                if (__float_as_int(A.w) < 0) continue;
+                elA[m] = A;
+                elB[m] = B;
+                m++;
+                sum = __fadd_rn(sum, A.z);
+                mr = fmaxf(mr, B.z);
+            }
+            nEl = m;
+            sumDeep = sum;
+            maxR2Bits = __float_as_int(mr);
         }
-        nEl = m;
-        sumDeep = sum;
-        maxR2 = mr;
+        __syncthreads();
+    }
+    const int n = mapped ? nEl : n0;
+    const int nPad = (n + k3DUnroll - 1) / k3DUnroll * k3DUnroll;  // <= cap (cap is a multiple of 4)
+    for (int j = n + tid; j < nPad; j += 256) {
+        elA[j] = make_float4(INFINITY, 0.0f, 0.0f, __int_as_float(0));
+        elB[j] = make_float4(0.0f, 0.0f, INFINITY, 0.0f);
     }
     __syncthreads();
+    if (!mapped && tid == 0) {
+        // the deep weights' running sum in element order, overlapped with the other warps' loops
+        float sum = 0.0f;
+        for (int j = 0; j < n; j++) sum = __fadd_rn(sum, elA[j].z);
+        sumDeep = sum;
+    }
+    const float maxR2 = __int_as_float(maxR2Bits);
     const uint32_t r = blockIdx.x * blockDim.x + tid;
-    if (r >= a.nD) return;
-    float acc = 0.0f;
-    if (active) {
+    const bool inRange = r < a.nD;
+    float sample = 0.0f, weightAcum = 0.0f;
+    int numAdds = 0;
+    bool deep = false;
+    if (active && inRange) {
         const float d = __ldg(a.depth + r);
         const float aDT = apertureDT(d, a.dt, a.c, a.F);
         const float aDT2 = __fmul_rn(aDT, aDT);
         const float sq = __fsqrt_rn(aDT2);
         const float invX = __fdiv_rn(1.0f, fminf(sq, s.maxDistX));
         const float invY = __fdiv_rn(1.0f, fminf(sq, s.maxDistY));
-        const bool deep = sq >= s.maxDistX && sq >= s.maxDistY && aDT2 >= maxR2;
-        const float iD = s.initialDelay[k];
+        deep = sq >= s.maxDistX && sq >= s.maxDistY && aDT2 >= maxR2;
         const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
         const float px = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
         const float pz = __fadd_rn(s.z, __fmul_rn(s.dirZ, d));
         const float ay = __fmul_rn(s.dirY, d);
         const float ay2 = __fmul_rn(ay, ay);
-        const int n = nEl;
-        float sample = 0.0f, weightAcum = 0.0f;
-        int numAdds = 0;
-        for (int j = 0; j < n; j++) {
-            const Elem3D e = el[j];
-            float w;
-            if (deep) {
-                w = e.wDeep;
-            } else {
-                if (!(e.r2 <= aDT2)) continue;
-                w = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(e.dx, invX)), lutGet(lut, __fmul_rn(e.dz, invY))));
-                weightAcum = __fadd_rn(weightAcum, w);
-                numAdds++;
-            }
-            const float qx = __fsub_rn(e.xel, px), qz = __fsub_rn(e.zel, pz);
-            const float q = __fadd_rn(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qz, qz)), ay2);
-            const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(__fsqrt_rn(q), d)), a.offset);
-            const uint32_t delay = static_cast<uint32_t>(floorf(delayf));  // saturates at 0 like the reference
-            const float frac = __fsub_rn(delayf, static_cast<float>(delay));
-            const RF* p = tx + static_cast<size_t>(e.ch) * a.nS;
-            if (delay < a.nS - 1) {
-                const float v0 = toFloat(__ldg(p + delay)), v1 = toFloat(__ldg(p + delay + 1));
-                const float v = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac), v0), __fmul_rn(frac, v1));
-                sample = __fadd_rn(sample, __fmul_rn(w, v));
-            } else if (delay < a.nS && frac == 0.0f) {
-                sample = __fadd_rn(sample, __fmul_rn(w, toFloat(__ldg(p + delay))));
-            }
-        }
+        if (deep)
+            das3dAccum<RF, true>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset, aDT2,
+                                 invX, invY, sample, weightAcum, numAdds);
+        else
+            das3dAccum<RF, false>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset, aDT2,
+                                  invX, invY, sample, weightAcum, numAdds);
+    }
+    __syncthreads();  // sumDeep
+    if (!inRange) return;
+    float acc = 0.0f;
+    if (active) {
         if (deep) {
             weightAcum = sumDeep;
             numAdds = n;
@@ -906,10 +969,13 @@ int sb_das_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void* out,
     if (staged) return launchStaged(p, a, rf_dtype, out_dtype, st);
     dim3 grid((p->numDepths + 255) / 256, p->numRx);
     const bool table3D = p->is3D && !interpolate_transmits &&
-                         static_cast<int64_t>(p->maxApertureX) * p->maxApertureY <= kMax3DElems;
+                         static_cast<int64_t>(p->maxApertureX) * p->maxApertureY <= kMax3DElems &&
+                         static_cast<int64_t>(p->numChannels) * p->numSamples <= INT32_MAX;
+    const int cap3D = table3D ? (p->maxApertureX * p->maxApertureY + k3DUnroll - 1) / k3DUnroll * k3DUnroll : 0;
+    const size_t smem3D = 2 * sizeof(float4) * static_cast<size_t>(cap3D);  // <= 32 KB: no opt-in needed
 #define SB_DAS_LAUNCH(RFT, OUTT)                                                        \
     do {                                                                                \
-        if (table3D) das3dTableKernel<RFT, OUTT><<<grid, 256, 0, st>>>(a);             \
+        if (table3D) das3dTableKernel<RFT, OUTT><<<grid, 256, smem3D, st>>>(a, cap3D); \
         else if (p->is3D) dasKernel<RFT, OUTT, true><<<grid, 256, 0, st>>>(a);         \
         else dasKernel<RFT, OUTT, false><<<grid, 256, 0, st>>>(a);                     \
     } while (0)
