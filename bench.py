@@ -192,6 +192,50 @@ def _event_ms(fn, n, warm=2):
     return a.elapsed_time(b) / n
 
 
+def chain_rows(g0, o0, hbm_row):
+    """The processing after the beamformer. (1) c0's chain on its own 2048 x 128 frame: 64-tap Hilbert
+    envelope, 50 dB log compression to uint8, 0.1 mm scan conversion, and the fused env -> log -> scan
+    kernel (these frames sit in L2: latency figures). (2) The same kernels on inputs above the 126 MB
+    L2 for their HBM rates: a 16384 x 2048 float image (128 MB) for the envelope, the IQ magnitude
+    (51-tap filters, decimation 4) and the log compression; the c0 scanlines converted at 0.01 mm
+    (13 B of tables per output pixel) for the scan conversion. Graph-replayed device time."""
+    import torch
+    from supra_b200.api import HilbertFirEnvelope, IQDemodulator, LogCompressor, ScanConverter
+    res = {}
+    img0 = torch.nan_to_num(o0, nan=0.0, posinf=0.0, neginf=0.0)
+    hil = HilbertFirEnvelope(64)
+    logc = LogCompressor()
+    env0 = hil.demodulate(img0)
+    in_max = float(env0.max())
+    sc0 = ScanConverter(g0.scanlines, g0.rx_layout, g0.num_depths, g0.depth_mm, 0.1)
+    row = {"env_ms": _graph_ms(lambda: hil.demodulate(img0), 20),
+           "log_ms": _graph_ms(lambda: logc.compress(env0, 50.0, 1.0, in_max, out_dtype=torch.uint8), 20),
+           "scan_ms": _graph_ms(lambda: sc0.convert(env0, torch.uint8), 20),
+           "fused_env_log_scan_ms": _graph_ms(lambda: sc0.env_log_convert(hil, img0, 50.0, 1.0, in_max, torch.uint8), 20),
+           "image": list(sc0.image_size[:2])}
+    res["chain_c0"] = row
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    big = torch.randn((16384, 2048), generator=gen, device="cuda") * 1000.0
+    n = big.numel()
+    ms = _graph_ms(lambda: hil.demodulate(big), 10)
+    res["hilbert_env_large"] = {"ms": ms, "px_per_s": n / ms * 1e3, **hbm_row(8 * n, ms)}
+    iq = IQDemodulator(40e6, 2.5e6, 51, 51, (7e6,), (1e6,), (1.0,))
+    ms = _graph_ms(lambda: iq.demodulate_magnitude(big, 4), 10)
+    res["iq_magnitude_large"] = {"ms": ms, "px_per_s": n / ms * 1e3, **hbm_row(4 * n + 4 * (n // 4), ms)}
+    ms = _graph_ms(lambda: logc.compress(big, 50.0, 1.0, 4000.0, out_dtype=torch.uint8), 10)
+    res["logcompress_large"] = {"ms": ms, "px_per_s": n / ms * 1e3, **hbm_row(5 * n, ms)}
+    del big
+    scf = ScanConverter(g0.scanlines, g0.rx_layout, g0.num_depths, g0.depth_mm, 0.01)
+    npx = scf.numel
+    ms = _graph_ms(lambda: scf.convert(env0, torch.uint8), 10)
+    res["scan_large"] = {"ms": ms, "image": list(scf.image_size[:2]), "px_per_s": npx / ms * 1e3,
+                         **hbm_row(14 * npx + 4 * env0.numel(), ms)}
+    ms = _graph_ms(lambda: scf.env_log_convert(hil, img0, 50.0, 1.0, in_max, torch.uint8), 10)
+    res["fused_env_log_scan_large"] = {"ms": ms, "px_per_s": npx / ms * 1e3, **hbm_row(14 * npx + 4 * img0.numel(), ms)}
+    return res
+
+
 def extras(wl, plans):
     """Secondary measurements of the other rows (N = 1 only; device time with CUDA events)."""
     import torch
@@ -263,6 +307,7 @@ def extras(wl, plans):
     ms = _event_ms(lambda: temporal_filter(ims), 10)
     res["temporal_filter"] = {"ms": ms, "images": 3, **hbm_row(4 * 4096 * 4096 * 4, ms)}
     del ims
+    res.update(chain_rows(g0, o0, hbm_row))
     # c4: differentiable DAS, 16 frames: adjoint (all three gradients) vs forward
     g4, rf4 = W.c4_batch()
     bf4 = RxBeamformer(g4)

@@ -36,6 +36,117 @@ __global__ void __launch_bounds__(256) hilbertKernel(const IN* __restrict__ in, 
     out[l + static_cast<size_t>(s) * nL] = static_cast<OUT>(__fsqrt_rn(__fadd_rn(__fmul_rn(v, v), __fmul_rn(acc, acc))));
 }
 
+// Tiled envelope: a CTA of 8 warps covers 32 scanlines x 8R samples. The input rows it needs (halo
+// included) are staged once into shared memory, one column per scanline, so that each lane reads
+// its own scanline's samples as aligned float pairs; each lane then computes R consecutive outputs
+// of its scanline, two at a time: products by __fmul_rn (never merged into an FMA), running sums
+// by __fadd2_rn (two IEEE round-to-nearest additions per instruction). A packed multiply feeding a
+// packed add (__fmul2_rn, then __fadd2_rn, as intrinsics or as mul.rn/add.rn.f32x2 in PTX) was
+// measured here to round like a fused multiply-add, so the products stay scalar. Every output sums
+// its taps in the reference's order with a separately rounded multiply and add per tap, so results
+// are bit-identical to hilbertKernel.
+// The Hilbert taps at even offsets from the centre are exactly zero; their terms (finite x times
+// +-0) are +-0 and leave the running sum unchanged, since a sum that starts at +0 never becomes -0.
+// So a tile whose inputs are all finite sums only the nonzero taps (j0 + 2t); a tile holding an
+// infinity or NaN, whose zero-tap terms are NaN, sums every tap. Samples outside the record are
+// staged as 0, whose terms are +-0 as well (the reference skips them).
+constexpr int kHilTileRowsExtra = 8;  // tap padding to a multiple of four, the pair-alignment shift
+
+__host__ __device__ constexpr int hilTileRows(int R, int H) { return 8 * R + 2 * H + kHilTileRowsExtra; }
+// column pitch: even (pairs stay 8-byte aligned) with an odd number of pairs (conflict-free pair reads)
+__host__ __device__ constexpr int hilTilePitch(int R, int H) {
+    return ((hilTileRows(R, H) + 1) & ~1) + ((((hilTileRows(R, H) + 1) & ~1) / 2) % 2 == 0 ? 2 : 0);
+}
+
+template <typename IN, int R, bool LOGC>
+__global__ void __launch_bounds__(256) hilbertTileKernel(const IN* __restrict__ in, float* __restrict__ out,
+                                                         const float* __restrict__ taps, const float* __restrict__ nzTaps,
+                                                         int nS, int nL, int N, int j0, int nz, float inScale, float k) {
+    extern __shared__ __align__(16) float hsm[];
+    const int H = N / 2;
+    const int nzPad = (nz + 3) & ~3;
+    const int pitch = hilTilePitch(R, H);
+    const int rows = hilTileRows(R, H);
+    float* T = hsm;                                  // [32 scanlines][pitch]
+    float* hAll = T + 32 * pitch;                    // taps 0 .. 2H (h[N] = 0 for even N)
+    float* hNz = hAll + ((2 * H + 1 + 3) & ~3);      // nonzero taps, padded with zeros
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    for (int i = tid; i <= 2 * H; i += 256) hAll[i] = i < N ? taps[i] : 0.0f;
+    for (int i = tid; i < nzPad; i += 256) hNz[i] = nzTaps[i];
+    const int off = j0 & 1;
+    const int l0 = blockIdx.x * 32, s0 = blockIdx.y * 8 * R;
+    const int l = l0 + lane;
+    // position p of a column holds sample s0 - H - off + p (0 outside the record or the image)
+    // eight rows per warp in flight: all loads of a batch issue before the first store
+    bool bad = false;
+    for (int p0 = w; p0 < rows; p0 += 64) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int p = p0 + 8 * u, s = s0 - H - off + p;
+            v[u] = (p < rows && s >= 0 && s < nS && l < nL) ? toFloat(in[l + static_cast<size_t>(s) * nL]) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int p = p0 + 8 * u;
+            if (p < rows) {
+                bad |= !isfinite(v[u]);
+                T[lane * pitch + p] = v[u];
+            }
+        }
+    }
+    const bool anyBad = __syncthreads_or(bad);
+    const float* col = T + lane * pitch;
+    const int sw = s0 + R * w;  // this warp's first output sample
+    float2 acc[R / 2];
+#pragma unroll
+    for (int q = 0; q < R / 2; q++) acc[q] = make_float2(0.0f, 0.0f);
+    if (!anyBad) {
+        // output sw + 2q + e (e = 0, 1), nonzero tap t: position R w + 2q + e + j0 + 2t + off, so pair
+        // (2q, 2q + 1) at tap t is pair number kb + q + t of the column
+        const float2* P = reinterpret_cast<const float2*>(col);
+        const int kb = (R * w + j0 + off) >> 1;
+        for (int t = 0; t < nzPad; t += 4) {
+            float2 xv[R / 2 + 3];
+#pragma unroll
+            for (int i = 0; i < R / 2 + 3; i++) xv[i] = P[kb + t + i];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const float hv = hNz[t + u];
+#pragma unroll
+                for (int q = 0; q < R / 2; q++)
+                    acc[q] = __fadd2_rn(acc[q], make_float2(__fmul_rn(xv[q + u].x, hv), __fmul_rn(xv[q + u].y, hv)));
+            }
+        }
+    } else {
+        float a1[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) a1[r] = 0.0f;
+        for (int j = 0; j <= 2 * H; j++) {
+            const float hv = hAll[j];
+#pragma unroll
+            for (int r = 0; r < R; r++) a1[r] = __fadd_rn(a1[r], __fmul_rn(col[R * w + r + j + off], hv));
+        }
+#pragma unroll
+        for (int q = 0; q < R / 2; q++) acc[q] = make_float2(a1[2 * q], a1[2 * q + 1]);
+    }
+    if (l >= nL) return;
+#pragma unroll
+    for (int q = 0; q < R / 2; q++) {
+        const int r = 2 * q;
+        const float2 v = make_float2(col[R * w + r + H + off], col[R * w + r + 1 + H + off]);
+        const float2 e2 = __fadd2_rn(make_float2(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)),
+                                     make_float2(__fmul_rn(acc[q].x, acc[q].x), __fmul_rn(acc[q].y, acc[q].y)));
+        float e0 = __fsqrt_rn(e2.x), e1 = __fsqrt_rn(e2.y);
+        if (LOGC) {  // LogCompressor to a float image (clampCast<float>)
+            e0 = clampCast<float>(logCompress(e0, inScale, k));
+            e1 = clampCast<float>(logCompress(e1, inScale, k));
+        }
+        if (sw + r < nS) out[l + static_cast<size_t>(sw + r) * nL] = e0;
+        if (sw + r + 1 < nS) out[l + static_cast<size_t>(sw + r + 1) * nL] = e1;
+    }
+}
+
 // Adjoint of the envelope (extension without a reference counterpart): env = sqrt(x^2 + h^2) with
 // h = taps (*) x along the samples, so dL/dx[j] = G[j] x[j] / env[j] + sum_s q[s] taps[j - s + N/2]
 // with q[s] = G[s] h[s] / env[s] (0 where env = 0). Pass 1 writes the direct term and q, pass 2
@@ -95,13 +206,54 @@ __global__ void logKernel(const IN* __restrict__ in, OUT* __restrict__ out, size
     for (; i < n; i += stride) out[i] = clampCast<OUT>(logCompress(toFloat(in[i]), inScale, k));
 }
 
+// Four elements per thread as one vector load and one vector store, evict-first (the image streams
+// through once); the last n % 4 elements by the first thread. Input and output aligned to 4 elements.
+template <typename T> struct Vec4;
+template <> struct Vec4<float> {
+    using type = float4;
+    static __device__ __forceinline__ float4 make(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+};
+template <> struct Vec4<int16_t> {
+    using type = short4;
+    static __device__ __forceinline__ short4 make(int16_t a, int16_t b, int16_t c, int16_t d) { return make_short4(a, b, c, d); }
+};
+template <> struct Vec4<uint8_t> {
+    using type = uchar4;
+    static __device__ __forceinline__ uchar4 make(uint8_t a, uint8_t b, uint8_t c, uint8_t d) { return make_uchar4(a, b, c, d); }
+};
+
+template <typename IN, typename OUT>
+__global__ void __launch_bounds__(256) logKernel4(const IN* __restrict__ in, OUT* __restrict__ out, size_t n, float inScale,
+                                                  float k) {
+    const size_t g = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    const size_t n4 = n / 4;
+    if (g < n4) {
+        const auto v = __ldcs(reinterpret_cast<const typename Vec4<IN>::type*>(in) + g);
+        const auto o = Vec4<OUT>::make(clampCast<OUT>(logCompress(toFloat(v.x), inScale, k)),
+                                       clampCast<OUT>(logCompress(toFloat(v.y), inScale, k)),
+                                       clampCast<OUT>(logCompress(toFloat(v.z), inScale, k)),
+                                       clampCast<OUT>(logCompress(toFloat(v.w), inScale, k)));
+        __stcs(reinterpret_cast<typename Vec4<OUT>::type*>(out) + g, o);
+    }
+    if (g == 0)
+        for (size_t i = 4 * n4; i < n; i++) out[i] = clampCast<OUT>(logCompress(toFloat(in[i]), inScale, k));
+}
+
 // ----------------------------------------------------------------------------- IQ magnitude
 // One CTA = 32 scanlines x OT decimated outputs. Phase 1 evaluates the filter-bank magnitude
 // (kernelFilterBankDemodulation, IQDemodulator.cu:68-137) for every input sample the low-pass needs
 // and keeps it in shared memory; phase 2 applies the decimating low-pass (kernelFilterStrided
 // :142-175). No full-resolution intermediate goes to HBM.
 constexpr int IQ_LINES = 32;
-constexpr int IQ_OT = 16;
+constexpr int IQ_OT = 32;
+
+// cos(2 pi ph) for a mixer phase ph in [0, 1): the argument folded into [-pi, pi] (ph - 1 is exact
+// for ph > 1/2) and evaluated by the hardware approximation, as the reference's production build
+// does (--use_fast_math, SupraLib/CMakeLists.txt:65): absolute error about 2^-21.
+__device__ __forceinline__ float mixCos(float ph) {
+    const float p = ph > 0.5f ? __fsub_rn(ph, 1.0f) : ph;
+    return __cosf(__fmul_rn(__fmul_rn(p, 2.0f), static_cast<float>(M_PI)));
+}
 
 template <typename IN, typename OUT>
 __global__ void __launch_bounds__(256) iqMagnitudeKernel(const IN* __restrict__ in, OUT* __restrict__ out, IqArgs a) {
@@ -117,28 +269,33 @@ __global__ void __launch_bounds__(256) iqMagnitudeKernel(const IN* __restrict__ 
         const int s = sIn0 + row, l = l0 + li;
         float v = 0.0f;
         if (l < a.nL && s >= 0 && s < a.nS) {
+            // filter loops unrolled over the 8 slots (guarded) so the sums stay in registers
             float acc[8];
             const float sv = toFloat(in[l + static_cast<size_t>(s) * a.nL]);
-            for (int f = 0; f < a.numFilters; f++) acc[f] = f < 1 ? sv : 0.0f;
+#pragma unroll
+            for (int f = 0; f < 8; f++) acc[f] = f < 1 ? sv : 0.0f;
             if (a.numFilters > 1) {
                 const int start = s - a.bpN / 2, end = s + a.bpN / 2;
                 for (int cs = start, fe = 0; cs <= end; cs++, fe++) {
                     if (cs >= 0 && cs < a.nS) {
                         const float x = toFloat(in[l + static_cast<size_t>(cs) * a.nL]);
-                        for (int f = 1; f < a.numFilters; f++)
-                            acc[f] = __fadd_rn(acc[f], __fmul_rn(x, a.bank[f * (a.bpN + 1) + fe]));
+#pragma unroll
+                        for (int f = 1; f < 8; f++)
+                            if (f < a.numFilters) acc[f] = __fadd_rn(acc[f], __fmul_rn(x, a.bank[f * (a.bpN + 1) + fe]));
                     }
                 }
             }
             float m = 0.0f;
-            for (int f = 0; f < a.numFilters; f++) {
+#pragma unroll
+            for (int f = 0; f < 8; f++) {
+                if (f >= a.numFilters) break;
                 const float ph = __fmul_rn(static_cast<float>(s), a.fOverFs[f]);
                 float phI = __fadd_rn(ph, 0.0f);
                 float phQ = __fadd_rn(ph, 0.75f);
                 phI = __fsub_rn(phI, truncf(phI));
                 phQ = __fsub_rn(phQ, truncf(phQ));
-                const float dI = __fmul_rn(acc[f], cosf(__fmul_rn(__fmul_rn(phI, 2.0f), static_cast<float>(M_PI))));
-                const float dQ = __fmul_rn(acc[f], cosf(__fmul_rn(__fmul_rn(phQ, 2.0f), static_cast<float>(M_PI))));
+                const float dI = __fmul_rn(acc[f], mixCos(phI));
+                const float dQ = __fmul_rn(acc[f], mixCos(phQ));
                 m = __fadd_rn(m, __fmul_rn(a.weights[f], __fsqrt_rn(__fadd_rn(__fmul_rn(dI, dI), __fmul_rn(dQ, dQ)))));
             }
             v = __fmul_rn(a.scale, m);
@@ -204,9 +361,19 @@ __global__ void __launch_bounds__(256) iqComplexKernel(const IN* __restrict__ in
 }  // namespace
 
 int launchLog(const void* in, int inDt, void* out, int outDt, size_t n, float inScale, float k, cudaStream_t st) {
+    if (n == 0) return SB_OK;
+    const size_t inB = inDt == SB_FLOAT32 ? 4 : inDt == SB_INT16 ? 2 : 1;
+    const size_t outB = outDt == SB_FLOAT32 ? 4 : 1;
+    const bool vec = reinterpret_cast<uintptr_t>(in) % (4 * inB) == 0 && reinterpret_cast<uintptr_t>(out) % (4 * outB) == 0 &&
+                     (n / 4 + 255) / 256 <= 0x7fffffffu;
     int blocks = static_cast<int>(std::min<size_t>((n + 255) / 256, static_cast<size_t>(smCount()) * 16));
     if (blocks < 1) blocks = 1;
-#define SB_LOG(INT, OUTT) logKernel<INT, OUTT><<<blocks, 256, 0, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), n, inScale, k)
+    const unsigned blocks4 = static_cast<unsigned>(std::max<size_t>((n / 4 + 255) / 256, 1));
+#define SB_LOG(INT, OUTT)                                                                                                  \
+    do {                                                                                                                   \
+        if (vec) logKernel4<INT, OUTT><<<blocks4, 256, 0, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), n, inScale, k); \
+        else logKernel<INT, OUTT><<<blocks, 256, 0, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), n, inScale, k);       \
+    } while (0)
     if (inDt == SB_FLOAT32 && outDt == SB_UINT8) SB_LOG(float, uint8_t);
     else if (inDt == SB_FLOAT32 && outDt == SB_FLOAT32) SB_LOG(float, float);
     else if (inDt == SB_INT16 && outDt == SB_UINT8) SB_LOG(int16_t, uint8_t);
@@ -216,6 +383,44 @@ int launchLog(const void* in, int inDt, void* out, int outDt, size_t n, float in
     else return fail(SB_ERR_UNSUPPORTED, "log compression %d -> %d unsupported", inDt, outDt);
 #undef SB_LOG
     SB_CHECK_LAUNCH("logKernel");
+    return SB_OK;
+}
+
+int launchHilbert(const sb_hilbert_plan* p, const void* in, int inDt, float* out, int nS, int nL, bool logc,
+                  float inScale, float k, cudaStream_t st) {
+    const int N = static_cast<int>(p->N), H = N / 2;
+    const int tiles16 = ((nL + 31) / 32) * ((nS + 127) / 128);
+    const int R = tiles16 >= 2 * smCount() ? 16 : 4;
+    const int nzPad = (p->nz + 3) & ~3;
+    const size_t shm = (static_cast<size_t>(32) * hilTilePitch(R, H) + ((2 * H + 1 + 3) & ~3) + nzPad) * sizeof(float);
+    if (p->nz > 0 && shm <= 48 * 1024 && (inDt == SB_FLOAT32 || inDt == SB_INT16)) {
+        const dim3 grid((nL + 31) / 32, (nS + 8 * R - 1) / (8 * R));
+#define SB_HT(INT, RR, LG)                                                                                           \
+    hilbertTileKernel<INT, RR, LG><<<grid, 256, shm, st>>>(static_cast<const INT*>(in), out, p->dTaps, p->dNz, nS, nL, \
+                                                           N, p->j0, p->nz, inScale, k)
+        if (inDt == SB_FLOAT32) {
+            if (R == 16) { if (logc) SB_HT(float, 16, true); else SB_HT(float, 16, false); }
+            else { if (logc) SB_HT(float, 4, true); else SB_HT(float, 4, false); }
+        } else {
+            if (R == 16) { if (logc) SB_HT(int16_t, 16, true); else SB_HT(int16_t, 16, false); }
+            else { if (logc) SB_HT(int16_t, 4, true); else SB_HT(int16_t, 4, false); }
+        }
+#undef SB_HT
+        SB_CHECK_LAUNCH("hilbertTileKernel");
+        return SB_OK;
+    }
+    // other filters (no zero-tap pattern, or longer than the tile allows): one thread per output
+    dim3 block(32, 8);
+    dim3 grid((nL + 31) / 32, (nS + 7) / 8);
+    const size_t shm1 = (p->N + 1) * sizeof(float);
+    if (inDt == SB_FLOAT32)
+        hilbertKernel<float, float><<<grid, block, shm1, st>>>(static_cast<const float*>(in), out, p->dTaps, nS, nL, N);
+    else if (inDt == SB_INT16)
+        hilbertKernel<int16_t, float><<<grid, block, shm1, st>>>(static_cast<const int16_t*>(in), out, p->dTaps, nS, nL, N);
+    else
+        return fail(SB_ERR_UNSUPPORTED, "sb_hilbert_env_run: input dtype %d unsupported", inDt);
+    SB_CHECK_LAUNCH("hilbertKernel");
+    if (logc) return launchLog(out, SB_FLOAT32, out, SB_FLOAT32, static_cast<size_t>(nS) * nL, inScale, k, st);
     return SB_OK;
 }
 
@@ -244,11 +449,28 @@ int sb_hilbert_plan_create(uint32_t filter_length, sb_hilbert_plan** plan) {
     SB_REQUIRE(plan && filter_length >= 1 && filter_length <= 1024, "sb_hilbert_plan_create: filter length %u", filter_length);
     *plan = nullptr;
     std::vector<float> taps = firDesign(filter_length, 3, 2, 2.0, 0.0, 0.0);
-    sb_hilbert_plan* p = new sb_hilbert_plan{filter_length, nullptr};
+    sb_hilbert_plan* p = new sb_hilbert_plan{filter_length, nullptr, 0, 0, nullptr};
+    // nonzero taps among j = 0 .. 2 (N / 2) (tap N of an even-length filter is 0): j0, j0 + 2, ...?
+    std::vector<int> nzIdx;
+    for (int j = 0; j <= 2 * static_cast<int>(filter_length / 2); j++)
+        if (j < static_cast<int>(filter_length) && taps[j] != 0.0f) nzIdx.push_back(j);
+    bool stride2 = !nzIdx.empty();
+    for (size_t t = 1; t < nzIdx.size(); t++) stride2 = stride2 && nzIdx[t] == nzIdx[0] + 2 * static_cast<int>(t);
+    std::vector<float> nzTaps;
+    if (stride2) {
+        p->j0 = nzIdx[0];
+        p->nz = static_cast<int>(nzIdx.size());
+        for (int j : nzIdx) nzTaps.push_back(taps[j]);
+        while (nzTaps.size() % 4) nzTaps.push_back(0.0f);
+    }
     cudaError_t e = cudaMalloc(&p->dTaps, filter_length * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpy(p->dTaps, taps.data(), filter_length * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !nzTaps.empty()) e = cudaMalloc(&p->dNz, nzTaps.size() * sizeof(float));
+    if (e == cudaSuccess && !nzTaps.empty())
+        e = cudaMemcpy(p->dNz, nzTaps.data(), nzTaps.size() * sizeof(float), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         cudaFree(p->dTaps);
+        cudaFree(p->dNz);
         delete p;
         return cudaFail(e, "sb_hilbert_plan_create");
     }
@@ -259,6 +481,7 @@ int sb_hilbert_plan_create(uint32_t filter_length, sb_hilbert_plan** plan) {
 int sb_hilbert_plan_destroy(sb_hilbert_plan* p) {
     if (!p) return SB_OK;
     cudaFree(p->dTaps);
+    cudaFree(p->dNz);
     delete p;
     return SB_OK;
 }
@@ -267,19 +490,11 @@ int sb_hilbert_env_run(const sb_hilbert_plan* p, const void* in, int in_dtype, v
                        uint32_t num_scanlines, uint32_t num_samples, sb_stream stream) {
     SB_REQUIRE(p && in && out, "sb_hilbert_env_run: null argument");
     SB_REQUIRE(num_scanlines > 0 && num_samples > 0, "sb_hilbert_env_run: empty image");
-    cudaStream_t st = S(stream);
-    dim3 block(32, 8);
-    dim3 grid((num_scanlines + 31) / 32, (num_samples + 7) / 8);
-    size_t shm = (p->N + 1) * sizeof(float);
-    int nS = static_cast<int>(num_samples), nL = static_cast<int>(num_scanlines), N = static_cast<int>(p->N);
-    if (in_dtype == SB_FLOAT32 && out_dtype == SB_FLOAT32)
-        hilbertKernel<float, float><<<grid, block, shm, st>>>(static_cast<const float*>(in), static_cast<float*>(out), p->dTaps, nS, nL, N);
-    else if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32)
-        hilbertKernel<int16_t, float><<<grid, block, shm, st>>>(static_cast<const int16_t*>(in), static_cast<float*>(out), p->dTaps, nS, nL, N);
-    else
+    SB_REQUIRE(num_scanlines <= INT32_MAX && num_samples <= INT32_MAX, "sb_hilbert_env_run: image too large");
+    if (!((in_dtype == SB_FLOAT32 || in_dtype == SB_INT16) && out_dtype == SB_FLOAT32))
         return fail(SB_ERR_UNSUPPORTED, "sb_hilbert_env_run: %d -> %d unsupported", in_dtype, out_dtype);
-    SB_CHECK_LAUNCH("hilbertKernel");
-    return SB_OK;
+    return launchHilbert(p, in, in_dtype, static_cast<float*>(out), static_cast<int>(num_samples),
+                         static_cast<int>(num_scanlines), false, 0.0f, 0.0f, S(stream));
 }
 
 int sb_hilbert_env_adjoint(const sb_hilbert_plan* p, const float* in, const float* grad_env, float* grad_in,

@@ -38,4 +38,15 @@ void logConstants(double dynamicRange, double gain, double inMax, int inDt, floa
 struct sb_hilbert_plan {
     uint32_t N;
     float* dTaps;  // N Hilbert taps (Hamming window)
+    // The nonzero taps sit at j0, j0 + 2, ..., j0 + 2 (nz - 1) (odd offsets from the centre); dNz holds
+    // them padded with zeros to a multiple of four. nz = 0: no such pattern (generic kernel only).
+    int j0, nz;
+    float* dNz;
 };
+
+namespace sb {
+// Envelope of a float / int16 image [nS][nL] into a float image; with `logc` its log compression
+// (inScale, k) instead, for the env -> log -> scan chain.
+int launchHilbert(const sb_hilbert_plan* p, const void* in, int inDt, float* out, int nS, int nL, bool logc,
+                  float inScale, float k, cudaStream_t st);
+}  // namespace sb

@@ -1,5 +1,5 @@
 // Scan conversion: table construction (2D on the host, 3D on the device in one launch), the
-// table-driven bilinear / trilinear gathers, and the fused envelope -> log -> scan kernel.
+// table-driven bilinear / trilinear gathers, and the envelope -> log -> scan chain.
 //   ScanConverter::updateInternals  Beamformer/ScanConverter.cu:513-815
 //   scanConvert2D / scanConvert3D   Beamformer/ScanConverter.cu:349-428
 #include <array>
@@ -20,6 +20,7 @@ struct sb_scan_plan {
     float* dWX = nullptr;
     float* dWY = nullptr;
     float* dWZ = nullptr;
+    float* dLog = nullptr;  // sb_env_log_scan_run's log-compressed envelope [numSamples][lx * ly]
 };
 
 namespace sb {
@@ -167,85 +168,89 @@ struct ScanArgs {
 
 // bilinear (2D) / trilinear (3D) table gather (ScanConverter.cu:349-428). The 2D reference does
 // not bound its reads; reads past the input are taken as 0 here.
-template <typename IN, typename OUT, bool IS2D>
-__global__ void __launch_bounds__(256) scanKernel(const IN* __restrict__ in, OUT* __restrict__ out, ScanArgs a) {
-    const size_t n = static_cast<size_t>(a.W) * a.H * a.D;
-    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
-    if (i >= n) return;
+template <typename IN, bool IS2D>
+__device__ __forceinline__ float scanPixel(const IN* __restrict__ in, const ScanArgs& a, uint32_t m, uint32_t s,
+                                           float wx, float wy, float wz) {
+    if (!m) return 0.0f;
     const uint32_t L = a.lx * a.ly;
     const size_t inN = static_cast<size_t>(L) * a.nS;
-    float val = 0.0f;
-    if (a.mask[i]) {
-        const uint32_t s = a.sIdx[i];
-        const float wx = a.wX[i], wy = a.wY[i];
-        const float ux = __fsub_rn(1.0f, wx), uy = __fsub_rn(1.0f, wy);
-        if (IS2D) {
-            val = __fadd_rn(__fmul_rn(uy, __fadd_rn(__fmul_rn(ux, rd(in, s, inN)), __fmul_rn(wx, rd(in, s + 1, inN)))),
-                            __fmul_rn(wy, __fadd_rn(__fmul_rn(ux, rd(in, s + L, inN)), __fmul_rn(wx, rd(in, s + 1 + L, inN)))));
-        } else if (static_cast<size_t>(s) + 1 + a.lx + L < static_cast<size_t>(a.nS) * L) {
-            const float wz = a.wZ[i], uz = __fsub_rn(1.0f, wz);
-            auto bl = [&](size_t b) {
-                return __fadd_rn(__fmul_rn(uz, __fadd_rn(__fmul_rn(ux, toFloat(in[b])), __fmul_rn(wx, toFloat(in[b + 1])))),
-                                 __fmul_rn(wz, __fadd_rn(__fmul_rn(ux, toFloat(in[b + a.lx])), __fmul_rn(wx, toFloat(in[b + 1 + a.lx])))));
-            };
-            val = __fadd_rn(__fmul_rn(uy, bl(s)), __fmul_rn(wy, bl(static_cast<size_t>(s) + L)));
-        }
-    }
-    out[i] = clampCast<OUT>(val);
+    const float ux = __fsub_rn(1.0f, wx), uy = __fsub_rn(1.0f, wy);
+    if (IS2D)
+        return __fadd_rn(__fmul_rn(uy, __fadd_rn(__fmul_rn(ux, rd(in, s, inN)), __fmul_rn(wx, rd(in, s + 1, inN)))),
+                         __fmul_rn(wy, __fadd_rn(__fmul_rn(ux, rd(in, s + L, inN)), __fmul_rn(wx, rd(in, s + 1 + L, inN)))));
+    if (!(static_cast<size_t>(s) + 1 + a.lx + L < inN)) return 0.0f;
+    const float uz = __fsub_rn(1.0f, wz);
+    auto bl = [&](size_t b) {
+        return __fadd_rn(__fmul_rn(uz, __fadd_rn(__fmul_rn(ux, toFloat(in[b])), __fmul_rn(wx, toFloat(in[b + 1])))),
+                         __fmul_rn(wz, __fadd_rn(__fmul_rn(ux, toFloat(in[b + a.lx])), __fmul_rn(wx, toFloat(in[b + 1 + a.lx])))));
+    };
+    return __fadd_rn(__fmul_rn(uy, bl(s)), __fmul_rn(wy, bl(static_cast<size_t>(s) + L)));
 }
 
-// Fused Hilbert envelope -> log compression -> table gather: each output pixel evaluates the
-// envelope (FIR over the RF column) and its log at the 4 (2D) / 8 (3D) samples it interpolates.
-struct FusedArgs {
-    ScanArgs s;
-    const float* taps;
-    int N;
-    float inScale, k;
+template <typename OUT> struct Out4;
+template <> struct Out4<uint8_t> {
+    static __device__ __forceinline__ void put(uint8_t* o, float a, float b, float c, float d) {
+        *reinterpret_cast<uchar4*>(o) = make_uchar4(clampCast<uint8_t>(a), clampCast<uint8_t>(b), clampCast<uint8_t>(c),
+                                                    clampCast<uint8_t>(d));
+    }
+};
+template <> struct Out4<int16_t> {
+    static __device__ __forceinline__ void put(int16_t* o, float a, float b, float c, float d) {
+        *reinterpret_cast<short4*>(o) = make_short4(clampCast<int16_t>(a), clampCast<int16_t>(b), clampCast<int16_t>(c),
+                                                    clampCast<int16_t>(d));
+    }
+};
+template <> struct Out4<float> {
+    static __device__ __forceinline__ void put(float* o, float a, float b, float c, float d) {
+        *reinterpret_cast<float4*>(o) = make_float4(clampCast<float>(a), clampCast<float>(b), clampCast<float>(c),
+                                                    clampCast<float>(d));
+    }
 };
 
-__device__ __forceinline__ float envLog(const float* __restrict__ rf, const float* h, int N, uint32_t L, uint32_t nS,
-                                        size_t idx, float inScale, float k) {
-    if (idx >= static_cast<size_t>(L) * nS) return 0.0f;
-    const int s = static_cast<int>(idx / L);
-    const uint32_t l = static_cast<uint32_t>(idx % L);
-    float acc = 0.0f;
-    const int start = s - N / 2, end = s + N / 2;
-    for (int cs = start, fe = 0; cs <= end; cs++, fe++)
-        if (cs >= 0 && cs < static_cast<int>(nS)) acc = __fadd_rn(acc, __fmul_rn(__ldg(rf + l + static_cast<size_t>(cs) * L), h[fe]));
-    const float v = __ldg(rf + idx);
-    const float env = __fsqrt_rn(__fadd_rn(__fmul_rn(v, v), __fmul_rn(acc, acc)));
-    return logCompress(env, inScale, k);
+// Four consecutive output pixels per thread: their table entries as one 4-byte and two (3D: three)
+// 16-byte loads, one vector store (the output is aligned to four elements; the tables are device
+// allocations). VEC = false: one pixel per thread, for an output that is not.
+template <typename IN, typename OUT, bool IS2D, bool VEC>
+__global__ void __launch_bounds__(256) scanKernel(const IN* __restrict__ in, OUT* __restrict__ out, ScanArgs a) {
+    const size_t n = static_cast<size_t>(a.W) * a.H * a.D;
+    const size_t g = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (!VEC) {
+        if (g < n)
+            out[g] = clampCast<OUT>(scanPixel<IN, IS2D>(in, a, a.mask[g], a.sIdx[g], a.wX[g], a.wY[g], IS2D ? 0.0f : a.wZ[g]));
+        return;
+    }
+    const size_t i0 = 4 * g;
+    if (i0 >= n) return;
+    if (i0 + 4 <= n) {
+        const uchar4 m = __ldg(reinterpret_cast<const uchar4*>(a.mask + i0));
+        const uint4 si = __ldg(reinterpret_cast<const uint4*>(a.sIdx + i0));
+        const float4 wx = __ldg(reinterpret_cast<const float4*>(a.wX + i0));
+        const float4 wy = __ldg(reinterpret_cast<const float4*>(a.wY + i0));
+        const float4 wz = IS2D ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : __ldg(reinterpret_cast<const float4*>(a.wZ + i0));
+        Out4<OUT>::put(out + i0, scanPixel<IN, IS2D>(in, a, m.x, si.x, wx.x, wy.x, wz.x),
+                       scanPixel<IN, IS2D>(in, a, m.y, si.y, wx.y, wy.y, wz.y),
+                       scanPixel<IN, IS2D>(in, a, m.z, si.z, wx.z, wy.z, wz.z),
+                       scanPixel<IN, IS2D>(in, a, m.w, si.w, wx.w, wy.w, wz.w));
+        return;
+    }
+    for (size_t i = i0; i < n; i++)
+        out[i] = clampCast<OUT>(scanPixel<IN, IS2D>(in, a, a.mask[i], a.sIdx[i], a.wX[i], a.wY[i], IS2D ? 0.0f : a.wZ[i]));
 }
 
-template <typename OUT, bool IS2D>
-__global__ void __launch_bounds__(256) fusedEnvLogScanKernel(const float* __restrict__ rf, OUT* __restrict__ out, FusedArgs f) {
-    extern __shared__ float h[];
-    for (int i = threadIdx.x; i <= f.N; i += blockDim.x) h[i] = i < f.N ? f.taps[i] : 0.0f;
-    __syncthreads();
-    const ScanArgs& a = f.s;
+template <typename IN, typename OUT>
+int launchScan(bool is2D, const ScanArgs& a, const IN* in, OUT* out, cudaStream_t st) {
     const size_t n = static_cast<size_t>(a.W) * a.H * a.D;
-    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t L = a.lx * a.ly;
-    float val = 0.0f;
-    if (a.mask[i]) {
-        const size_t s = a.sIdx[i];
-        const float wx = a.wX[i], wy = a.wY[i];
-        const float ux = __fsub_rn(1.0f, wx), uy = __fsub_rn(1.0f, wy);
-        auto E = [&](size_t j) { return envLog(rf, h, f.N, L, a.nS, j, f.inScale, f.k); };
-        if (IS2D) {
-            val = __fadd_rn(__fmul_rn(uy, __fadd_rn(__fmul_rn(ux, E(s)), __fmul_rn(wx, E(s + 1)))),
-                            __fmul_rn(wy, __fadd_rn(__fmul_rn(ux, E(s + L)), __fmul_rn(wx, E(s + 1 + L)))));
-        } else if (s + 1 + a.lx + L < static_cast<size_t>(a.nS) * L) {
-            const float wz = a.wZ[i], uz = __fsub_rn(1.0f, wz);
-            auto bl = [&](size_t b) {
-                return __fadd_rn(__fmul_rn(uz, __fadd_rn(__fmul_rn(ux, E(b)), __fmul_rn(wx, E(b + 1)))),
-                                 __fmul_rn(wz, __fadd_rn(__fmul_rn(ux, E(b + a.lx)), __fmul_rn(wx, E(b + 1 + a.lx)))));
-            };
-            val = __fadd_rn(__fmul_rn(uy, bl(s)), __fmul_rn(wy, bl(s + L)));
-        }
+    const bool vec = reinterpret_cast<uintptr_t>(out) % (4 * sizeof(OUT)) == 0;
+    const unsigned blocks = static_cast<unsigned>(((vec ? (n + 3) / 4 : n) + 255) / 256);
+    if (vec) {
+        if (is2D) scanKernel<IN, OUT, true, true><<<blocks, 256, 0, st>>>(in, out, a);
+        else scanKernel<IN, OUT, false, true><<<blocks, 256, 0, st>>>(in, out, a);
+    } else {
+        if (is2D) scanKernel<IN, OUT, true, false><<<blocks, 256, 0, st>>>(in, out, a);
+        else scanKernel<IN, OUT, false, false><<<blocks, 256, 0, st>>>(in, out, a);
     }
-    out[i] = clampCast<OUT>(val);
+    SB_CHECK_LAUNCH("scanKernel");
+    return SB_OK;
 }
 
 ScanArgs scanArgs(const sb_scan_plan* p) {
@@ -299,6 +304,7 @@ int sb_scan_plan_create(const sb_scanline_rx* lines, uint32_t lx, uint32_t ly, u
     if (e == cudaSuccess) e = cudaMalloc(&p->dWX, n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&p->dWY, n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&p->dWZ, n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&p->dLog, static_cast<size_t>(numSamples) * lx * ly * sizeof(float));
     if (e != cudaSuccess) {
         sb_scan_plan_destroy(p);
         return cudaFail(e, "sb_scan_plan_create: cudaMalloc");
@@ -368,6 +374,7 @@ int sb_scan_plan_destroy(sb_scan_plan* p) {
     cudaFree(p->dWX);
     cudaFree(p->dWY);
     cudaFree(p->dWZ);
+    cudaFree(p->dLog);
     delete p;
     return SB_OK;
 }
@@ -411,17 +418,9 @@ int sb_scan_copy_tables(const sb_scan_plan* p, uint8_t* mask, uint32_t* sampleId
 
 int sb_scan_run(const sb_scan_plan* p, const void* in, int in_dtype, void* out, int out_dtype, sb_stream stream) {
     SB_REQUIRE(p && in && out, "sb_scan_run: null argument");
-    ScanArgs a = scanArgs(p);
-    const size_t n = static_cast<size_t>(a.W) * a.H * a.D;
-    const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+    const ScanArgs a = scanArgs(p);
     cudaStream_t st = S(stream);
-#define SB_SCAN(INT, OUTT)                                                                                               \
-    do {                                                                                                                 \
-        if (p->is2D) scanKernel<INT, OUTT, true><<<blocks, 256, 0, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), a); \
-        else scanKernel<INT, OUTT, false><<<blocks, 256, 0, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), a);        \
-        SB_CHECK_LAUNCH("scanKernel");                                                                                   \
-        return SB_OK;                                                                                                    \
-    } while (0)
+#define SB_SCAN(INT, OUTT) return launchScan<INT, OUTT>(p->is2D, a, static_cast<const INT*>(in), static_cast<OUTT*>(out), st)
     if (in_dtype == SB_FLOAT32 && out_dtype == SB_UINT8) SB_SCAN(float, uint8_t);
     if (in_dtype == SB_FLOAT32 && out_dtype == SB_FLOAT32) SB_SCAN(float, float);
     if (in_dtype == SB_FLOAT32 && out_dtype == SB_INT16) SB_SCAN(float, int16_t);
@@ -434,30 +433,24 @@ int sb_scan_run(const sb_scan_plan* p, const void* in, int in_dtype, void* out, 
     return fail(SB_ERR_UNSUPPORTED, "sb_scan_run: %d -> %d unsupported", in_dtype, out_dtype);
 }
 
+// HilbertFirEnvelope -> LogCompressor (float) -> ScanConverter. The envelope and its log are
+// computed once per input sample, by the tiled envelope kernel, into the plan's float image
+// (numSamples x lines: 1 MB for a 2048 x 128 frame, which stays in L2); the table gather reads it
+// from there. HBM traffic: the RF in, the tables and the image out.
 int sb_env_log_scan_run(const sb_hilbert_plan* hilbert, const sb_scan_plan* scan, const float* rf, void* out,
                         int out_dtype, double dynamic_range_db, double gain, double in_max, sb_stream stream) {
     SB_REQUIRE(hilbert && scan && rf && out, "sb_env_log_scan_run: null argument");
     SB_REQUIRE(in_max > 0 && dynamic_range_db > 0, "sb_env_log_scan_run: inMax and dynamic range must be > 0");
-    FusedArgs f;
-    f.s = scanArgs(scan);
-    f.taps = hilbert->dTaps;
-    f.N = static_cast<int>(hilbert->N);
-    logConstants(dynamic_range_db, gain, in_max, SB_FLOAT32, f.inScale, f.k);
-    const size_t n = static_cast<size_t>(f.s.W) * f.s.H * f.s.D;
-    const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
-    const size_t shm = (hilbert->N + 1) * sizeof(float);
+    SB_REQUIRE(out_dtype == SB_UINT8 || out_dtype == SB_FLOAT32, "sb_env_log_scan_run: out dtype %d", out_dtype);
+    float inScale, k;
+    logConstants(dynamic_range_db, gain, in_max, SB_FLOAT32, inScale, k);
     cudaStream_t st = S(stream);
-    if (out_dtype == SB_UINT8) {
-        if (scan->is2D) fusedEnvLogScanKernel<uint8_t, true><<<blocks, 256, shm, st>>>(rf, static_cast<uint8_t*>(out), f);
-        else fusedEnvLogScanKernel<uint8_t, false><<<blocks, 256, shm, st>>>(rf, static_cast<uint8_t*>(out), f);
-    } else if (out_dtype == SB_FLOAT32) {
-        if (scan->is2D) fusedEnvLogScanKernel<float, true><<<blocks, 256, shm, st>>>(rf, static_cast<float*>(out), f);
-        else fusedEnvLogScanKernel<float, false><<<blocks, 256, shm, st>>>(rf, static_cast<float*>(out), f);
-    } else {
-        return fail(SB_ERR_UNSUPPORTED, "sb_env_log_scan_run: out dtype %d", out_dtype);
-    }
-    SB_CHECK_LAUNCH("fusedEnvLogScanKernel");
-    return SB_OK;
+    const int nL = static_cast<int>(scan->lx * scan->ly), nS = static_cast<int>(scan->numSamples);
+    const int r = launchHilbert(hilbert, rf, SB_FLOAT32, scan->dLog, nS, nL, true, inScale, k, st);
+    if (r != SB_OK) return r;
+    const ScanArgs a = scanArgs(scan);
+    if (out_dtype == SB_UINT8) return launchScan<float, uint8_t>(scan->is2D, a, scan->dLog, static_cast<uint8_t*>(out), st);
+    return launchScan<float, float>(scan->is2D, a, scan->dLog, static_cast<float*>(out), st);
 }
 
 }  // extern "C"
