@@ -341,6 +341,15 @@ def profile_case(case: str):
         x = torch.randn((16, 64, 2048), device="cuda") * 1000.0
         from supra_b200.api import mv_beamform_pcg
         mv_beamform_pcg(x, 32, 5)
+    elif case == "chain":
+        # the envelope-chain kernels on inputs above L2: 16384 x 2048 float image (128 MB)
+        from supra_b200.api import HilbertFirEnvelope, IQDemodulator, LogCompressor
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(7)
+        big = torch.randn((16384, 2048), generator=gen, device="cuda") * 1000.0
+        HilbertFirEnvelope(64).demodulate(big)
+        IQDemodulator(40e6, 2.5e6, 51, 51, (7e6,), (1e6,), (1.0,)).demodulate_magnitude(big, 4)
+        LogCompressor().compress(big, 50.0, 1.0, 4000.0, out_dtype=torch.uint8)
     elif case == "das3d":
         from supra_b200 import workloads as W
         g2 = W.c2_geometry()
@@ -367,7 +376,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements (c0, c2, c3, c4)")
     ap.add_argument("--frames", type=int, default=64, help="frames per launch (64 = the named workload)")
-    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg"],
+    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg", "chain"],
                     help="run one small case for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:

@@ -58,10 +58,19 @@ __host__ __device__ constexpr int hilTilePitch(int R, int H) {
     return ((hilTileRows(R, H) + 1) & ~1) + ((((hilTileRows(R, H) + 1) & ~1) / 2) % 2 == 0 ? 2 : 0);
 }
 
+// four consecutive scanlines of one sample row as floats (a 16-byte or an 8-byte load)
+__device__ __forceinline__ float4 load4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float4 load4(const int16_t* p) {
+    const short4 v = __ldg(reinterpret_cast<const short4*>(p));
+    return make_float4(v.x, v.y, v.z, v.w);
+}
+
+// vec4: the scanline count is a multiple of 4 and the input aligned to 4 elements
 template <typename IN, int R, bool LOGC>
 __global__ void __launch_bounds__(256) hilbertTileKernel(const IN* __restrict__ in, float* __restrict__ out,
                                                          const float* __restrict__ taps, const float* __restrict__ nzTaps,
-                                                         int nS, int nL, int N, int j0, int nz, float inScale, float k) {
+                                                         int nS, int nL, int N, int j0, int nz, float inScale, float k,
+                                                         bool vec4) {
     extern __shared__ __align__(16) float hsm[];
     const int H = N / 2;
     const int nzPad = (nz + 3) & ~3;
@@ -77,8 +86,33 @@ __global__ void __launch_bounds__(256) hilbertTileKernel(const IN* __restrict__ 
     const int l0 = blockIdx.x * 32, s0 = blockIdx.y * 8 * R;
     const int l = l0 + lane;
     // position p of a column holds sample s0 - H - off + p (0 outside the record or the image)
-    // eight rows per warp in flight: all loads of a batch issue before the first store
     bool bad = false;
+    if (vec4) {
+        // 4 scanlines x 1 row per thread and load (16 / 8 bytes), 32 rows per CTA pass, 4 passes in flight
+        const int g = tid & 7, ro = tid >> 3;
+        for (int p0 = ro; p0 < rows; p0 += 128) {
+            float4 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int p = p0 + 32 * u, s = s0 - H - off + p;
+                v[u] = (p < rows && s >= 0 && s < nS && l0 + 4 * g < nL)
+                           ? load4(in + l0 + 4 * g + static_cast<size_t>(s) * nL)
+                           : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int p = p0 + 32 * u;
+                if (p < rows) {
+                    bad |= !(isfinite(v[u].x) && isfinite(v[u].y) && isfinite(v[u].z) && isfinite(v[u].w));
+                    T[(4 * g) * pitch + p] = v[u].x;
+                    T[(4 * g + 1) * pitch + p] = v[u].y;
+                    T[(4 * g + 2) * pitch + p] = v[u].z;
+                    T[(4 * g + 3) * pitch + p] = v[u].w;
+                }
+            }
+        }
+    } else
+    // eight rows per warp in flight: all loads of a batch issue before the first store
     for (int p0 = w; p0 < rows; p0 += 64) {
         float v[8];
 #pragma unroll
@@ -258,6 +292,7 @@ __device__ __forceinline__ float mixCos(float ph) {
 template <typename IN, typename OUT>
 __global__ void __launch_bounds__(256) iqMagnitudeKernel(const IN* __restrict__ in, OUT* __restrict__ out, IqArgs a) {
     extern __shared__ float sm[];
+    __shared__ float lps[kIqMaxTaps + 1];               // the low-pass taps
     float* band = sm;                                   // [rows][IQ_LINES]
     const int rows = (IQ_OT - 1) * a.stride + a.lpN + 1;
     const int l0 = blockIdx.x * IQ_LINES;
@@ -302,6 +337,7 @@ __global__ void __launch_bounds__(256) iqMagnitudeKernel(const IN* __restrict__ 
         }
         band[row * IQ_LINES + li] = v;
     }
+    for (int j = tid; j <= a.lpN; j += blockDim.x) lps[j] = a.lp[j];
     __syncthreads();
     for (int idx = tid; idx < IQ_OT * IQ_LINES; idx += blockDim.x) {
         const int o = idx / IQ_LINES, li = idx % IQ_LINES;
@@ -310,8 +346,13 @@ __global__ void __launch_bounds__(256) iqMagnitudeKernel(const IN* __restrict__ 
         if (so >= a.nOut || l >= a.nL || si >= a.nS) continue;
         float acc = 0.0f;
         const int start = si - a.lpN / 2, end = si + a.lpN / 2;
-        for (int cs = start, fe = 0; cs <= end; cs++, fe++) {
-            if (cs >= 0 && cs < a.nS) acc = __fadd_rn(acc, __fmul_rn(band[(cs - sIn0) * IQ_LINES + li], a.lp[fe]));
+        const float* b = band + (start - sIn0) * IQ_LINES + li;
+        if (start >= 0 && end < a.nS) {  // the whole window inside the record
+            for (int fe = 0; fe <= end - start; fe++) acc = __fadd_rn(acc, __fmul_rn(b[fe * IQ_LINES], lps[fe]));
+        } else {
+            for (int cs = start, fe = 0; cs <= end; cs++, fe++) {
+                if (cs >= 0 && cs < a.nS) acc = __fadd_rn(acc, __fmul_rn(b[fe * IQ_LINES], lps[fe]));
+            }
         }
         out[l + static_cast<size_t>(so) * a.nL] = clampCast<OUT>(acc);
     }
@@ -395,9 +436,11 @@ int launchHilbert(const sb_hilbert_plan* p, const void* in, int inDt, float* out
     const size_t shm = (static_cast<size_t>(32) * hilTilePitch(R, H) + ((2 * H + 1 + 3) & ~3) + nzPad) * sizeof(float);
     if (p->nz > 0 && shm <= 48 * 1024 && (inDt == SB_FLOAT32 || inDt == SB_INT16)) {
         const dim3 grid((nL + 31) / 32, (nS + 8 * R - 1) / (8 * R));
+        const size_t eb = inDt == SB_FLOAT32 ? 4 : 2;
+        const bool vec4 = nL % 4 == 0 && reinterpret_cast<uintptr_t>(in) % (4 * eb) == 0;
 #define SB_HT(INT, RR, LG)                                                                                           \
     hilbertTileKernel<INT, RR, LG><<<grid, 256, shm, st>>>(static_cast<const INT*>(in), out, p->dTaps, p->dNz, nS, nL, \
-                                                           N, p->j0, p->nz, inScale, k)
+                                                           N, p->j0, p->nz, inScale, k, vec4)
         if (inDt == SB_FLOAT32) {
             if (R == 16) { if (logc) SB_HT(float, 16, true); else SB_HT(float, 16, false); }
             else { if (logc) SB_HT(float, 4, true); else SB_HT(float, 4, false); }
