@@ -289,8 +289,11 @@ int sb_scan_copy_tables(const sb_scan_plan* plan, uint8_t* mask, uint32_t* sampl
 int sb_scan_run(const sb_scan_plan* plan, const void* in, int in_dtype, void* out, int out_dtype,
                 sb_stream stream);
 
-/* Fused HilbertFirEnvelope -> LogCompressor -> ScanConverter (2D or 3D): FP32 RF [num_samples][scanlines]
- * in, image out (SB_UINT8 or SB_FLOAT32). No envelope or log image is written to HBM. */
+/* HilbertFirEnvelope -> LogCompressor -> ScanConverter (2D or 3D): FP32 RF [num_samples][scanlines]
+ * in, image out (SB_UINT8 or SB_FLOAT32). The log-compressed envelope is computed once per input
+ * sample into a float image owned by the scan plan (num_samples x scanlines, allocated by
+ * sb_scan_plan_create; 1 MB for a 2048 x 128 frame, which stays in L2), then gathered through the
+ * tables. Two launches on `stream`; calls on one plan must not overlap. */
 int sb_env_log_scan_run(const sb_hilbert_plan* hilbert, const sb_scan_plan* scan, const float* rf,
                         void* out, int out_dtype, double dynamic_range_db, double gain, double in_max,
                         sb_stream stream);
