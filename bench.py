@@ -277,6 +277,17 @@ def extras(wl, plans):
     res["das3d_c2"] = {"vox_per_s": g2.num_rx * g2.num_depths / ms * 1e3, "volumes_per_s": 1e3 / ms, "ms": ms,
                        **hbm_row(rf2.numel() * 2 + o2.numel() * 4, ms)}
     del rf2
+    # c2's processing after DAS: 65-tap envelope, 50 dB log, 3D scan conversion to a 0.25 mm grid
+    from supra_b200.api import HilbertFirEnvelope, ScanConverter
+    v2 = torch.nan_to_num(o2, nan=0.0, posinf=0.0, neginf=0.0)
+    hil2 = HilbertFirEnvelope(65)
+    sc2 = ScanConverter(g2.scanlines, g2.rx_layout, g2.num_depths, g2.depth_mm, 0.25)
+    env2 = hil2.demodulate(v2)
+    in_max2 = float(env2.max())
+    res["chain_c2"] = {"env_ms": _graph_ms(lambda: hil2.demodulate(v2), 20),
+                       "scan_ms": _graph_ms(lambda: sc2.convert(env2, torch.uint8), 20),
+                       "env_log_scan_ms": _graph_ms(lambda: sc2.env_log_convert(hil2, v2, 50.0, 1.0, in_max2, torch.uint8), 20),
+                       "grid": list(sc2.image_size), "voxels": sc2.numel}
     # c3: complex MV, 128 x 2048 systems of 32 x 32, FP64 re-solve above 1e6
     g3, x3 = W.c3_raw_delayed()
     ms = _event_ms(lambda: mv_beamform(x3, W.C3_L, W.C3_T, 1.5, False, W.C3_LOADING, 1e6, with_stats=False), 5, warm=3)

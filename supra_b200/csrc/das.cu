@@ -398,6 +398,126 @@ __global__ void __launch_bounds__(256) dasVariantKernel(DasArgs a) {
     static_cast<OUT*>(a.out)[line + static_cast<size_t>(r) * a.nRx] = clampCast<OUT>(acc);
 }
 
+// DelayAndStdDev / CoherenceFactorDelayAndSum, 2D, highest-weight transmit (the common case of
+// dasVariantKernel): the scanline's elements (position, offset from the scanline, channel row offset or
+// -1 for an unmapped element) sit in a shared-memory table, padded to a multiple of four with unmapped
+// entries. Each pass takes elements four at a time: aperture test, weight and running weight sum in
+// element order, delays, then the eight gathers together, then the reducer's updates in element order,
+// so the arithmetic and its order are those of variant2D (bit-identical).
+constexpr int kVarUnroll = 4;
+
+template <typename RF, int BF, int PASS>
+__device__ __forceinline__ void variantPass(const float4* el, int nPad, const float* lut, const RF* tx, uint32_t nS,
+                                            float aDT, float invMax, float xz, float dy2, float depth, float iD,
+                                            float offset, float mean, float& sample, float& weightAcum, int& numAdds,
+                                            float& value, float& cs, float& energy) {
+    for (int j = 0; j < nPad; j += kVarUnroll) {
+        float w[kVarUnroll], frac[kVarUnroll], v0[kVarUnroll], v1[kVarUnroll];
+        int32_t idx[kVarUnroll];
+        bool inAp[kVarUnroll], one[kVarUnroll], two[kVarUnroll];
+#pragma unroll
+        for (int u = 0; u < kVarUnroll; u++) {
+            const float4 e = el[j + u];
+            const int chOff = __float_as_int(e.z);
+            inAp[u] = chOff >= 0 && fabsf(e.y) <= aDT;
+            w[u] = 0.0f;
+            if (inAp[u]) {
+                w[u] = lutGet(lut, __fmul_rn(e.y, invMax));
+                weightAcum = __fadd_rn(weightAcum, w[u]);
+                numAdds++;
+            }
+            const float ex = __fsub_rn(e.x, xz);
+            const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2));
+            const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(dist, depth)), offset);
+            const int32_t delay = static_cast<int32_t>(floorf(delayf));
+            frac[u] = __fsub_rn(delayf, static_cast<float>(delay));
+            two[u] = inAp[u] && static_cast<uint32_t>(delay) < nS - 1;
+            one[u] = two[u] || (inAp[u] && static_cast<uint32_t>(delay) < nS && frac[u] == 0.0f);
+            idx[u] = static_cast<int32_t>(static_cast<uint32_t>(chOff) + static_cast<uint32_t>(delay));  // used when one[u]
+        }
+#pragma unroll
+        for (int u = 0; u < kVarUnroll; u++) {
+            v0[u] = one[u] ? toFloat(__ldg(tx + idx[u])) : 0.0f;
+            v1[u] = two[u] ? toFloat(__ldg(tx + idx[u] + 1)) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kVarUnroll; u++) {
+            if (one[u]) {
+                const float v = two[u] ? __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac[u]), v0[u]), __fmul_rn(frac[u], v1[u]))
+                                       : v0[u];
+                if (PASS == 0) sample = __fadd_rn(sample, __fmul_rn(w[u], v));
+                value = BF == SB_BF_DELAY_AND_STDDEV ? __fmul_rn(w[u], v) : v;
+            }
+            if (inAp[u]) {  // an element whose sample lies outside the record reuses the previous value
+                if (BF == SB_BF_COHERENCE_FACTOR_DAS) {
+                    cs = __fadd_rn(cs, value);
+                    energy = __fadd_rn(energy, __fmul_rn(value, value));
+                } else if (PASS == 1) {
+                    const float t = __fsub_rn(value, mean);
+                    cs = __fadd_rn(cs, __fmul_rn(t, t));
+                }
+            }
+        }
+    }
+}
+
+template <typename RF, typename OUT, int BF>
+__global__ void __launch_bounds__(256) dasVariantTableKernel(DasArgs a) {
+    __shared__ float lut[64];
+    __shared__ float4 el[kMaxApertureElems];
+    const int tid = threadIdx.x;
+    if (tid < 64) lut[tid] = a.lut.v[tid];
+    const uint32_t line = blockIdx.y;
+    const LineDT s = a.lines[line];
+    const int k = s.highest;
+    const bool active = (s.activeMask >> k) & 1;
+    const int n = active ? max(static_cast<int>(s.lastX[k]) - static_cast<int>(s.firstX[k]), 0) : 0;  // <= 256 (host)
+    const int nPad = (n + kVarUnroll - 1) / kVarUnroll * kVarUnroll;
+    for (int j = tid; j < nPad; j += 256) {
+        float4 r = make_float4(0.0f, 0.0f, __int_as_float(-1), 0.0f);
+        if (j < n) {
+            const int e = s.firstX[k] + j;
+            const int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(static_cast<uint32_t>(e) % a.nCh);
+            const float xel = __ldg(a.xe + e);
+            r = make_float4(xel, __fsub_rn(xel, s.x), __int_as_float(ch < 0 ? -1 : ch * static_cast<int>(a.nS)), 0.0f);
+        }
+        el[j] = r;
+    }
+    __syncthreads();
+    const uint32_t r = blockIdx.x * blockDim.x + tid;
+    if (r >= a.nD) return;
+    float acc = 0.0f;
+    if (active) {
+        const float d = __ldg(a.depth + r);
+        const float aDT = apertureDT(d, a.dt, a.c, a.F);
+        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+        const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
+        const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
+        const float dy = __fmul_rn(s.dirY, d);
+        const float dy2 = __fmul_rn(dy, dy);
+        const float iD = s.initialDelay[k];
+        float sample = 0.0f, weightAcum = 0.0f, value = 0.0f, cs = 0.0f, energy = 0.0f;
+        int numAdds = 0;
+        variantPass<RF, BF, 0>(el, nPad, lut, tx, a.nS, aDT, invMax, xz, dy2, d, iD, a.offset, 0.0f, sample,
+                               weightAcum, numAdds, value, cs, energy);
+        float v = 0.0f;
+        if (BF == SB_BF_DELAY_AND_STDDEV) {
+            const float mean = numAdds > 0 ? __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds)) : 0.0f;
+            weightAcum = 0.0f;
+            numAdds = 0;
+            value = 0.0f;
+            variantPass<RF, BF, 1>(el, nPad, lut, tx, a.nS, aDT, invMax, xz, dy2, d, iD, a.offset, mean, sample,
+                                   weightAcum, numAdds, value, cs, energy);
+            if (numAdds > 0) v = __fmul_rn(__fdiv_rn(__fsqrt_rn(cs), weightAcum), static_cast<float>(numAdds));
+        } else if (numAdds > 0) {
+            const float das = __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds));
+            v = __fmul_rn(__fdiv_rn(__fdiv_rn(__fmul_rn(cs, cs), energy), static_cast<float>(numAdds)), das);
+        }
+        acc = __fadd_rn(acc, v);
+    }
+    static_cast<OUT*>(a.out)[line + static_cast<size_t>(r) * a.nRx] = clampCast<OUT>(acc);
+}
+
 // 3D delay-and-sum with a per-scanline element table in shared memory (highest-weight transmit).
 // The table keeps the reference's summation order (x outer, y inner, RxSampleBeamformerDelayAndSum.h:
 // 55-57), each element's position, channel row offset and offsets from the scanline. Once the aperture
@@ -1006,10 +1126,14 @@ int sb_das_run_beamformer(const sb_das_plan* plan, int sample_beamformer, const 
                        interpolate_transmits, additional_offset, st);
     if (err != SB_OK) return err;
     dim3 grid((p->numDepths + 255) / 256, p->numRx);
-#define SB_BF_LAUNCH(RFT, OUTT, BFV)                                                    \
-    do {                                                                                \
-        if (p->is3D) dasVariantKernel<RFT, OUTT, true, BFV><<<grid, 256, 0, st>>>(a);   \
-        else dasVariantKernel<RFT, OUTT, false, BFV><<<grid, 256, 0, st>>>(a);          \
+    // 2D, highest-weight transmit, aperture within the element table: the table kernel
+    const bool table = !p->is3D && !interpolate_transmits && p->maxApertureX <= kMaxApertureElems &&
+                       static_cast<int64_t>(p->numChannels) * p->numSamples <= INT32_MAX;
+#define SB_BF_LAUNCH(RFT, OUTT, BFV)                                                                     \
+    do {                                                                                                 \
+        if (table && BFV != SB_BF_TEST_SIGNAL) dasVariantTableKernel<RFT, OUTT, BFV><<<grid, 256, 0, st>>>(a); \
+        else if (p->is3D) dasVariantKernel<RFT, OUTT, true, BFV><<<grid, 256, 0, st>>>(a);               \
+        else dasVariantKernel<RFT, OUTT, false, BFV><<<grid, 256, 0, st>>>(a);                           \
     } while (0)
 #define SB_BF_TYPES(BFV)                                                                \
     do {                                                                                \

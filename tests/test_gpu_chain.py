@@ -120,3 +120,22 @@ def test_fused_env_log_scan_c0(oracle):
     assert got.shape == ref.shape == (396, 383)
     d = np.abs(got.astype(int) - ref.astype(int))
     assert d.max() <= 1, d.max()
+
+
+def test_env_log_scan_3d(oracle):
+    """The 3D chain after DAS (c2's processing): 65-tap envelope, log compression and trilinear scan
+    conversion, against the oracle's envelope, log and gather applied with the plan's own tables (the
+    3D tables themselves are compared in test_scan_tables_3d); uint8 within 1 LSB."""
+    from supra_b200.api import HilbertFirEnvelope, ScanConverter
+    g = small_matrix(num_samples=512)
+    rng = np.random.Generator(np.random.PCG64(12))
+    vol = (rng.standard_normal((g.num_depths, g.num_rx)) * 1000).astype(np.float32)
+    env = oracle.hilbert_env(vol, 65)
+    in_max = float(env.max())
+    logc = oracle.logcompress(env, 50.0, 1.0, in_max, np.float32)
+    sc = ScanConverter(g.scanlines, g.rx_layout, g.num_depths, g.depth_mm, 0.25)
+    ref = oracle.scan_apply(logc, g.rx_layout[0], g.rx_layout[1], sc.tables(), np.uint8)
+    got = sc.env_log_convert(HilbertFirEnvelope(65), torch.from_numpy(vol).cuda(), 50.0, 1.0, in_max,
+                             torch.uint8).cpu().numpy()
+    assert got.shape == ref.shape and ref.any()
+    assert np.abs(got.astype(int) - ref.astype(int)).max() <= 1
