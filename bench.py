@@ -361,6 +361,20 @@ def profile_case(case: str):
         HilbertFirEnvelope(64).demodulate(big)
         IQDemodulator(40e6, 2.5e6, 51, 51, (7e6,), (1e6,), (1.0,)).demodulate_magnitude(big, 4)
         LogCompressor().compress(big, 50.0, 1.0, 4000.0, out_dtype=torch.uint8)
+    elif case == "misc":
+        # one launch each: c0 DAS (single-frame pack kernel), DelayAndStdDev on c0, the FFT envelope of
+        # the c0 image, scan conversion of the c0 envelope at 0.01 mm, temporal filter of 3 x 64 MB
+        from supra_b200 import synth
+        from supra_b200.api import HilbertEnvelope, HilbertFirEnvelope, ScanConverter, temporal_filter
+        g0, rf0 = synth.c0_frame(0, device="cuda")
+        bf0 = RxBeamformer(g0)
+        img = bf0.beamform(rf0, 1.0, window_type=1)
+        bf0.beamform(rf0, 1.0, window_type=1, beamformer="DelayAndStdDev")
+        img = torch.nan_to_num(img, nan=0.0, posinf=0.0, neginf=0.0)
+        HilbertEnvelope(g0.num_depths).envelope(img)
+        env = HilbertFirEnvelope(64).demodulate(img)
+        ScanConverter(g0.scanlines, g0.rx_layout, g0.num_depths, g0.depth_mm, 0.01).convert(env, torch.uint8)
+        temporal_filter([torch.randn((4096, 4096), device="cuda") for _ in range(3)])
     elif case == "das3d":
         from supra_b200 import workloads as W
         g2 = W.c2_geometry()
@@ -387,7 +401,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements (c0, c2, c3, c4)")
     ap.add_argument("--frames", type=int, default=64, help="frames per launch (64 = the named workload)")
-    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg", "chain"],
+    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg", "chain", "misc"],
                     help="run one small case for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:
