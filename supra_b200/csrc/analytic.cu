@@ -36,6 +36,12 @@ constexpr int kAThreads = 64;
 
 constexpr int kASplit = 8;  // CTAs per cluster sharing one output tile
 
+__device__ __forceinline__ float4 load4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float4 load4(const int16_t* p) {
+    const short4 v = __ldg(reinterpret_cast<const short4*>(p));
+    return make_float4(v.x, v.y, v.z, v.w);
+}
+
 // The 4 x 4 partial sums of this thread over the chunks m0 = first, first + step, ... (x tiles staged
 // in xs, kernel values in ks).
 template <typename IN>
@@ -48,20 +54,48 @@ __device__ __forceinline__ void analyticPartial(const IN* __restrict__ in, const
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) tot[i][j] = 0.0f;
-    for (int m0 = first; m0 < N; m0 += step) {
-        __syncthreads();  // the previous chunk's reads are done
-        for (int e = tid; e < kAT * kAT; e += kAThreads) {
-            const int mm = e / kAT, ll = e % kAT;
-            const int m = m0 + mm, l = l0 + ll;
-            xs[mm][ll] = (m < N && l < nL) ? toFloat(in[static_cast<size_t>(m) * nL + l]) : 0.0f;
+    // the next chunk's x tile (4 groups of 4 scanlines per thread) and kernel value are fetched into
+    // registers while the current chunk is summed
+    float4 px[4];
+    float pk = 0.0f;
+    const bool vec = nL % 4 == 0 && reinterpret_cast<uintptr_t>(in) % (4 * sizeof(IN)) == 0;
+    auto fetch = [&](int m0) {
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = tid + kAThreads * u, mm = e >> 3, c = (e & 7) * 4;
+            const int m = m0 + mm, l = l0 + c;
+            float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (m < N) {
+                const IN* row = in + static_cast<size_t>(m) * nL;
+                if (vec && l + 3 < nL) {
+                    v = load4(row + l);
+                } else {
+                    if (l < nL) v.x = toFloat(row[l]);
+                    if (l + 1 < nL) v.y = toFloat(row[l + 1]);
+                    if (l + 2 < nL) v.z = toFloat(row[l + 2]);
+                    if (l + 3 < nL) v.w = toFloat(row[l + 3]);
+                }
+            }
+            px[u] = v;
         }
-        for (int e = tid; e < 2 * kAT - 1; e += kAThreads) {
-            int d = n0 - m0 + e - (kAT - 1);  // in (-2N, N)
+        if (tid < 2 * kAT - 1) {
+            int d = n0 - m0 + tid - (kAT - 1);  // in (-2N, N)
             d %= N;
             if (d < 0) d += N;
-            ks[e] = __ldg(kern + d);
+            pk = __ldg(kern + d);
         }
+    };
+    if (first < N) fetch(first);
+    for (int m0 = first; m0 < N; m0 += step) {
+        __syncthreads();  // the previous chunk's reads are done
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = tid + kAThreads * u;
+            *reinterpret_cast<float4*>(&xs[e >> 3][(e & 7) * 4]) = px[u];
+        }
+        if (tid < 2 * kAT - 1) ks[tid] = pk;
         __syncthreads();
+        if (m0 + step < N) fetch(m0 + step);
         float acc[4][4];
 #pragma unroll
         for (int i = 0; i < 4; i++)

@@ -207,9 +207,10 @@ template <> struct Out4<float> {
     }
 };
 
-// Four consecutive output pixels per thread: their table entries as one 4-byte and two (3D: three)
-// 16-byte loads, one vector store (the output is aligned to four elements; the tables are device
-// allocations). VEC = false: one pixel per thread, for an output that is not.
+// Eight consecutive output pixels per thread, as two groups of four: each group's table entries as
+// one 4-byte and two (3D: three) 16-byte loads and one vector store (the output is aligned to four
+// elements; the tables are device allocations). VEC = false: one pixel per thread, for an output
+// that is not.
 template <typename IN, typename OUT, bool IS2D, bool VEC>
 __global__ void __launch_bounds__(256) scanKernel(const IN* __restrict__ in, OUT* __restrict__ out, ScanArgs a) {
     const size_t n = static_cast<size_t>(a.W) * a.H * a.D;
@@ -219,18 +220,28 @@ __global__ void __launch_bounds__(256) scanKernel(const IN* __restrict__ in, OUT
             out[g] = clampCast<OUT>(scanPixel<IN, IS2D>(in, a, a.mask[g], a.sIdx[g], a.wX[g], a.wY[g], IS2D ? 0.0f : a.wZ[g]));
         return;
     }
-    const size_t i0 = 4 * g;
+    // two groups of four pixels: both groups' table loads, then all their gathers, are in flight together
+    const size_t i0 = 8 * g;
     if (i0 >= n) return;
-    if (i0 + 4 <= n) {
-        const uchar4 m = __ldg(reinterpret_cast<const uchar4*>(a.mask + i0));
-        const uint4 si = __ldg(reinterpret_cast<const uint4*>(a.sIdx + i0));
-        const float4 wx = __ldg(reinterpret_cast<const float4*>(a.wX + i0));
-        const float4 wy = __ldg(reinterpret_cast<const float4*>(a.wY + i0));
-        const float4 wz = IS2D ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : __ldg(reinterpret_cast<const float4*>(a.wZ + i0));
-        Out4<OUT>::put(out + i0, scanPixel<IN, IS2D>(in, a, m.x, si.x, wx.x, wy.x, wz.x),
-                       scanPixel<IN, IS2D>(in, a, m.y, si.y, wx.y, wy.y, wz.y),
-                       scanPixel<IN, IS2D>(in, a, m.z, si.z, wx.z, wy.z, wz.z),
-                       scanPixel<IN, IS2D>(in, a, m.w, si.w, wx.w, wy.w, wz.w));
+    if (i0 + 8 <= n) {
+        uchar4 m[2];
+        uint4 si[2];
+        float4 wx[2], wy[2], wz[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const size_t b = i0 + 4 * h;
+            m[h] = __ldg(reinterpret_cast<const uchar4*>(a.mask + b));
+            si[h] = __ldg(reinterpret_cast<const uint4*>(a.sIdx + b));
+            wx[h] = __ldg(reinterpret_cast<const float4*>(a.wX + b));
+            wy[h] = __ldg(reinterpret_cast<const float4*>(a.wY + b));
+            wz[h] = IS2D ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : __ldg(reinterpret_cast<const float4*>(a.wZ + b));
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+            Out4<OUT>::put(out + i0 + 4 * h, scanPixel<IN, IS2D>(in, a, m[h].x, si[h].x, wx[h].x, wy[h].x, wz[h].x),
+                           scanPixel<IN, IS2D>(in, a, m[h].y, si[h].y, wx[h].y, wy[h].y, wz[h].y),
+                           scanPixel<IN, IS2D>(in, a, m[h].z, si[h].z, wx[h].z, wy[h].z, wz[h].z),
+                           scanPixel<IN, IS2D>(in, a, m[h].w, si[h].w, wx[h].w, wy[h].w, wz[h].w));
         return;
     }
     for (size_t i = i0; i < n; i++)
@@ -241,7 +252,7 @@ template <typename IN, typename OUT>
 int launchScan(bool is2D, const ScanArgs& a, const IN* in, OUT* out, cudaStream_t st) {
     const size_t n = static_cast<size_t>(a.W) * a.H * a.D;
     const bool vec = reinterpret_cast<uintptr_t>(out) % (4 * sizeof(OUT)) == 0;
-    const unsigned blocks = static_cast<unsigned>(((vec ? (n + 3) / 4 : n) + 255) / 256);
+    const unsigned blocks = static_cast<unsigned>(((vec ? (n + 7) / 8 : n) + 255) / 256);
     if (vec) {
         if (is2D) scanKernel<IN, OUT, true, true><<<blocks, 256, 0, st>>>(in, out, a);
         else scanKernel<IN, OUT, false, true><<<blocks, 256, 0, st>>>(in, out, a);
