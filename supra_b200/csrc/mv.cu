@@ -412,7 +412,7 @@ __device__ __forceinline__ MvOut<T> solveRegs(GE* Gs, int GP, int L, int sz, T l
 // when r.s <= 1e-30 or when |r| <= thr; then y = sum_v xbar_v a_v / (sum_v a_v * K^p). Row i of R
 // sits in registers of lane i % 32 (q = i / 32); R v broadcasts v_j from its lane.
 template <int NR, class GE>
-__device__ __forceinline__ MvOut<float> solvePcgRegs(const GE* Gs, int GP, int sz, float loading, int lane,
+__device__ __forceinline__ MvOut<float> solvePcgRegs(const GE* Gs, int GP, float* vbuf, int sz, float loading, int lane,
                                                      const V<float> (&xbar)[NR], float power, int K, int maxIt, float thr) {
     // R stays in the shared-memory tile (rows of pitch GP, read as aligned pairs); the covariance
     // accumulators of the sliding window are live across the solve, so R is not copied to registers
@@ -427,12 +427,9 @@ __device__ __forceinline__ MvOut<float> solvePcgRegs(const GE* Gs, int GP, int s
     // o = R v on the sz x sz block. The loop runs over whole groups of four columns (a warp-uniform
     // trip count, no per-column branch): the vectors are zero on rows >= sz, so the columns past sz
     // (finite window sums of the tile) contribute nothing. Four independent accumulators per row.
-    auto pick = [&](const float (&v)[NR], int qq) {
-        float r = v[0];
-#pragma unroll
-        for (int k = 1; k < NR; k++) r = qq == k ? v[k] : r;
-        return r;
-    };
+    // v is staged in the warp's vector buffer (32 NR floats) and read as 16-byte broadcasts: one
+    // shared-memory read per four columns instead of four shuffles (the SM's shuffle unit is shared
+    // by all its warps; the two products per iteration would otherwise issue 16 NR shuffles per row group)
     const int jmax = (sz + 3) & ~3;
     auto matvec = [&](const float (&v)[NR], float (&o)[NR]) {
         float p4[NR][4];
@@ -440,10 +437,13 @@ __device__ __forceinline__ MvOut<float> solvePcgRegs(const GE* Gs, int GP, int s
         for (int q = 0; q < NR; q++)
 #pragma unroll
             for (int c = 0; c < 4; c++) p4[q][c] = 0.0f;
-        for (int j = 0; j < jmax; j += 4) {
-            float vj[4];
+        __syncwarp();  // the previous product's reads of vbuf are done
 #pragma unroll
-            for (int c = 0; c < 4; c++) vj[c] = __shfl_sync(kFull, pick(v, (j + c) >> 5), (j + c) & 31);
+        for (int q = 0; q < NR; q++) vbuf[lane + 32 * q] = v[q];
+        __syncwarp();
+        for (int j = 0; j < jmax; j += 4) {
+            const float4 vv = *reinterpret_cast<const float4*>(vbuf + j);
+            const float vj[4] = {vv.x, vv.y, vv.z, vv.w};
 #pragma unroll
             for (int q = 0; q < NR; q++) {
                 const GE* row = &Gs[(valid[q] ? lane + 32 * q : 0) * GP + j];
@@ -653,8 +653,10 @@ template <bool C, int NR> struct MvLayout {
         return alignUp(static_cast<size_t>(slots) * GR * sizeof(V<float>), 16);
     }
     __host__ __device__ static size_t gBytes() { return alignUp(static_cast<size_t>(GR) * GP * sizeof(Elem<C>), 16); }
+    // the PCG solve's search vector (real data only), read back as 16-byte broadcasts
+    __host__ __device__ static size_t vecBytes() { return C ? 0 : alignUp(static_cast<size_t>(GR) * sizeof(float), 16); }
     __host__ __device__ static size_t perWarp(uint32_t slots, uint32_t pitch) {
-        return ringBytes(slots, pitch) + metaBytes(slots) + d0Bytes(slots) + gBytes();
+        return ringBytes(slots, pitch) + metaBytes(slots) + d0Bytes(slots) + gBytes() + vecBytes();
     }
 };
 
@@ -745,6 +747,8 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
     SampleMeta* meta = reinterpret_cast<SampleMeta*>(base + L_::ringBytes(R, a.ringPitch));
     V<float>* d0c = reinterpret_cast<V<float>*>(base + L_::ringBytes(R, a.ringPitch) + L_::metaBytes(R));
     Elem<C>* Gs = reinterpret_cast<Elem<C>*>(base + L_::ringBytes(R, a.ringPitch) + L_::metaBytes(R) + L_::d0Bytes(R));
+    float* vbuf = reinterpret_cast<float*>(base + L_::ringBytes(R, a.ringPitch) + L_::metaBytes(R) + L_::d0Bytes(R) +
+                                           L_::gBytes());
     const In* xl = static_cast<const In*>(a.in) + static_cast<size_t>(line) * a.nCh * a.nS;
     Out* out = static_cast<Out*>(a.out);
 
@@ -874,7 +878,7 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
         if (!C && a.pcg) {
             if constexpr (!C) {
                 if (tr > 0.0f && isfinite(tr))
-                    y = solvePcgRegs<NR, Elem<C>>(Gs, L_::GP, ms.sz, loading, lane, xbar, a.power, ms.K, a.pcgMaxIt,
+                    y = solvePcgRegs<NR, Elem<C>>(Gs, L_::GP, vbuf, ms.sz, loading, lane, xbar, a.power, ms.K, a.pcgMaxIt,
                                                   a.pcgThr).y;
             }
         } else if (tr > 0.0f && isfinite(tr)) {
