@@ -425,22 +425,33 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         if (MODE == 1) continue;  // the next item's first barrier orders the table's reuse
         // one barrier per item: the segment's RF is complete; its IQ outputs [so0, so1) for every frame
         __syncthreads();
-        const int cntOut = max(0, so1 - so0) * nf;
-        for (int idx = tid; idx < cntOut; idx += NT) {
-            const int so = so0 + idx / nf;
-            const int f = idx % nf;
-            float re = 0.0f, im = 0.0f;
+        // one decimated output per thread for all frames of the pack: each tap's low-pass weight and
+        // mixer phasor are loaded once for the pack's frames; interior outputs skip the record-edge tests
+        const int nso = max(0, so1 - so0);
+        for (int o = tid; o < nso; o += NT) {
+            const int so = so0 + o;
             const int base = so * a.dec - a.half;
+            const bool interior = base >= 0 && base + a.taps <= nD;
+            float re[FP], im[FP];
+#pragma unroll
+            for (int f = 0; f < FP; f++) re[f] = im[f] = 0.0f;
             for (int j = 0; j < a.taps; j++) {
                 const int nn = base + j;
-                if (nn >= 0 && nn < nD) {
-                    const float x = seg[f][nn - rStart] * a.lp[j];
-                    const float2 w = __ldg(a.rot + nn);
-                    re = fmaf(x, w.x, re);
-                    im = fmaf(x, w.y, im);
+                if (!interior && (nn < 0 || nn >= nD)) continue;
+                const float lpj = a.lp[j];
+                const float2 w = __ldg(a.rot + nn);
+#pragma unroll
+                for (int f = 0; f < FP; f++) {
+                    if (f < nf) {
+                        const float x = seg[f][nn - rStart] * lpj;
+                        re[f] = fmaf(x, w.x, re[f]);
+                        im[f] = fmaf(x, w.y, im[f]);
+                    }
                 }
             }
-            P.iq[f][pi.line + static_cast<size_t>(so) * P.nRx] = make_float2(re, im);
+#pragma unroll
+            for (int f = 0; f < FP; f++)
+                if (f < nf) P.iq[f][pi.line + static_cast<size_t>(so) * P.nRx] = make_float2(re[f], im[f]);
         }
         // the next item's first barrier orders these reads of seg before its writes
     }
