@@ -339,10 +339,10 @@ def profile_case(case: str):
     from supra_b200.api import BatchedDasIq, RxBeamformer, mv_beamform
     from supra_b200.workloads import c1_workload
     if case == "batch":
-        wl = c1_workload(num_frames=24, device="cuda")  # packs of 4 frames are full
+        wl = c1_workload(num_frames=24, device="cuda")  # 8 frames per probe: packs of 8 frames are full
         plans = [RxBeamformer(g) for g in wl.geometries]
-        b = BatchedDasIq([(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)], ctas_per_sm=8, depth_tile=128,
-                         frames_per_pack=4)
+        b = BatchedDasIq([(plans[p], rf) for p, rf in zip(wl.frame_probe, wl.rf)], ctas_per_sm=4, depth_tile=256,
+                         frames_per_pack=8)
         for _ in range(2):
             b.run(use_graph=False)
     elif case == "mv":

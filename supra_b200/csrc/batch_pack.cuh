@@ -191,9 +191,9 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         g.off = static_cast<uint32_t>(e.ch) + idx;  // e.ch holds the row offset
         return g;
     };
-    if constexpr (K >= 8) {
+    if constexpr (K >= 6) {
         // wide packs: one element's gathers in flight while the next element's geometry is computed
-        // (two sample registers per frame instead of four, so 8 frames fit the register budget)
+        // (two sample registers per frame instead of four, so 6 and 8 frames fit the register budget)
         G g = geom(j0, true);
         for (int j = j0; j < j1; j++) {
             int16_t a[K], b[K];
@@ -396,8 +396,10 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         const int so0 = static_cast<int>(pi.seg0) / a.dec;
         const int so1 = min(static_cast<int>(pi.seg1) / a.dec, nD / a.dec);
         const int nBlocks = (rEnd - rStart + NT - 1) / NT;
-        // frames of a partial pack take the narrower loops (a pack of 4 frames holding 1 or 2)
-        const int kw = nf > kHalf ? FP : (nf > 1 ? kHalf : 1);
+        // frames of a partial pack take the narrower loops (a pack of 4 frames holding 1 or 2; a pack of
+        // 8 holding 5 or 6 takes the 6-frame loop)
+        constexpr int kSix = FP == 8 ? 6 : FP;
+        const int kw = nf > kSix ? FP : nf > kHalf ? kSix : (nf > 1 ? kHalf : 1);
         for (int k = 0; k < nBlocks; k++) {
             const int r = rStart + k * NT + tid;
             PackAcc<FP> acc;
@@ -406,6 +408,7 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             if (r < rEnd && valid) {
                 const float d = __ldg(P.depth + r);
                 if (kw == FP) packRow<FP, FP, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
+                else if (FP == 8 && kw == kSix) packRow<FP, kSix, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
                 else if (kw == kHalf) packRow<FP, kHalf, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
                 else packRow<FP, 1, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
             }
