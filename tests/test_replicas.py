@@ -60,3 +60,20 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
     args = argparse.Namespace(steps=1, warmup=0, gpus=2)
     assert bench.run_reference(args, rank=1) is None
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_json_line(capsys):
+    """One bounded step of the reference arm on the host cores (rank 0): its JSON line carries the
+    headline metric, a cpu_baseline describing the run and an e2e entry without device copies."""
+    import argparse
+    import json
+
+    import bench
+    args = argparse.Namespace(steps=1, warmup=0, gpus=1)
+    bench.run_reference(args, rank=0)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["value"] > 0 and line["higher_is_better"] is True and line["steps"] == 1
+    cb = line["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
