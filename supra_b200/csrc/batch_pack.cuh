@@ -194,6 +194,10 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
     if constexpr (K >= 6) {
         // wide packs: one element's gathers in flight while the next element's geometry is computed
         // (two sample registers per frame instead of four, so 6 and 8 frames fit the register budget)
+        // The gathers of element j + kPrefetchAhead are announced to L2 at element j's delay index
+        // (neighbouring elements' delays differ by a few samples): a prefetch holds no register, and the
+        // one-element look-ahead alone leaves the DRAM latency of these gathers exposed (c1: -9%).
+        constexpr int kPrefetchAhead = 2;
         G g = geom(j0, true);
         for (int j = j0; j < j1; j++) {
             int16_t a[K], b[K];
@@ -201,6 +205,14 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
             for (int f = 0; f < K; f++) {
                 a[f] = __ldg(tb[f] + g.off);
                 b[f] = __ldg(tb[f] + g.off + 1);
+            }
+            if (j + kPrefetchAhead < j1) {
+                // row offset of element j + kPrefetchAhead plus element j's sample index (< nS - 1):
+                // an address inside that channel's row
+                const uint32_t offp = static_cast<uint32_t>(el[j + kPrefetchAhead].ch) +
+                                      (g.off - static_cast<uint32_t>(el[j].ch));
+#pragma unroll
+                for (int f = 0; f < K; f++) asm volatile("prefetch.global.L2 [%0];" ::"l"(tb[f] + offp));
             }
             const G gn = geom(min(j + 1, j1 - 1), j + 1 < j1);
 #pragma unroll
