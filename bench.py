@@ -295,6 +295,9 @@ def extras(wl, plans):
     res["mv_c3"] = {"px_per_s": x3.shape[0] * x3.shape[2] / ms * 1e3, "frames_per_s": 1e3 / ms, "ms": ms,
                     "fp64_systems": int(st.fp64_systems), "max_condition_estimate": float(st.max_condition_estimate)}
     del x3
+    # RawDelay of the c0 frame: [128 lines][64 channels][2048 depths] float out (67 MB)
+    ms = _graph_ms(lambda: bf0.raw_delay(rf0, 1.0, window_type=1), 10)
+    res["rawdelay_c0"] = {"ms": ms, **hbm_row(rf0.numel() * 2 + g0.num_rx * g0.num_channels * g0.num_depths * 4, ms)}
     # the other sample beamformers on the c0 frame (per-frame kernels, reference float semantics)
     for name in ("DelayAndStdDev", "CoherenceFactorDelayAndSum"):
         ms = _graph_ms(lambda: bf0.beamform(rf0, 1.0, window_type=1, out=o0, beamformer=name), 10)
