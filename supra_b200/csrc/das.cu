@@ -755,6 +755,93 @@ __global__ void __launch_bounds__(256) rawDelayKernel(DasArgs a) {
     for (int j = written; j < static_cast<int>(a.nCh); j++) out[static_cast<size_t>(j) * a.nD] = clampCast<OUT>(0.0f);
 }
 
+// RawDelay with the scanline's elements in a shared-memory table (apertures up to
+// kMaxApertureElems elements): the weight sum over the whole aperture first, then the written slots
+// four elements at a time (delays and weights of all four, their gathers together, then the four
+// stores), in rawDelayKernel's arithmetic (bit-identical).
+template <typename RF, typename OUT>
+__global__ void __launch_bounds__(256) rawDelayTableKernel(DasArgs a) {
+    __shared__ float lut[64];
+    __shared__ float4 el[kMaxApertureElems];  // (x, dx, channel row offset as int bits, 0)
+    const int tid = threadIdx.x;
+    if (tid < 64) lut[tid] = a.lut.v[tid];
+    const uint32_t line = blockIdx.y;
+    const LineDT s = a.lines[line];
+    const int k = s.highest;
+    const bool active = (s.activeMask >> k) & 1;
+    const int n = active ? max(static_cast<int>(s.lastX[k]) - static_cast<int>(s.firstX[k]), 0) : 0;  // <= 256 (host)
+    const int nw = min(n, static_cast<int>(a.nCh));                          // slots written
+    const int nPad = (nw + kVarUnroll - 1) / kVarUnroll * kVarUnroll;        // <= 256
+    for (int j = tid; j < max(n, nPad); j += 256) {
+        float4 r = make_float4(0.0f, INFINITY, __int_as_float(0), 0.0f);     // padding: outside every aperture
+        if (j < n) {
+            const int e = s.firstX[k] + j;
+            const float xel = __ldg(a.xe + e);
+            r = make_float4(xel, __fsub_rn(xel, s.x), __int_as_float(static_cast<int>((static_cast<uint32_t>(e) % a.nCh) * a.nS)), 0.0f);
+        }
+        el[j] = r;
+    }
+    __syncthreads();
+    const uint32_t r = blockIdx.x * blockDim.x + tid;
+    if (r >= a.nD) return;
+    OUT* out = static_cast<OUT*>(a.out) + static_cast<size_t>(line) * a.nCh * a.nD + r;
+    int written = 0;
+    if (active) {
+        const float d = __ldg(a.depth + r);
+        const float aDT = apertureDT(d, a.dt, a.c, a.F);
+        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+        float weightAcum = 0.0f;
+        int numAdds = 0;
+        for (int j = 0; j < n; j++) {
+            const float dx = el[j].y;
+            if (fabsf(dx) <= aDT) {
+                weightAcum = __fadd_rn(weightAcum, lutGet(lut, __fmul_rn(dx, invMax)));
+                numAdds++;
+            }
+        }
+        const float scale = numAdds > 0 ? __fmul_rn(__fdiv_rn(1.0f, weightAcum), static_cast<float>(numAdds)) : 1.0f;
+        const RF* tx = static_cast<const RF*>(a.rf) + static_cast<size_t>(s.txIdx[k]) * a.nCh * a.nS;
+        const float xz = __fadd_rn(s.x, __fmul_rn(s.dirX, d));
+        const float dy = __fmul_rn(s.dirY, d);
+        const float dy2 = __fmul_rn(dy, dy);
+        const float iD = s.initialDelay[k];
+        for (int j0 = 0; j0 < nPad; j0 += kVarUnroll) {
+            float w[kVarUnroll], frac[kVarUnroll], v0[kVarUnroll], v1[kVarUnroll];
+            int32_t idx[kVarUnroll];
+            bool one[kVarUnroll], two[kVarUnroll];
+#pragma unroll
+            for (int u = 0; u < kVarUnroll; u++) {
+                const float4 e = el[j0 + u];
+                const bool inAp = fabsf(e.y) <= aDT;
+                w[u] = inAp ? lutGet(lut, __fmul_rn(e.y, invMax)) : 0.0f;
+                const float ex = __fsub_rn(e.x, xz);
+                const float delayf = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2)), d));
+                const int32_t delay = static_cast<int32_t>(floorf(delayf));
+                frac[u] = __fsub_rn(delayf, static_cast<float>(delay));
+                two[u] = inAp && static_cast<uint32_t>(delay) < a.nS - 1;
+                one[u] = two[u] || (inAp && static_cast<uint32_t>(delay) < a.nS && frac[u] == 0.0f);
+                idx[u] = static_cast<int32_t>(static_cast<uint32_t>(__float_as_int(e.z)) + static_cast<uint32_t>(delay));
+            }
+#pragma unroll
+            for (int u = 0; u < kVarUnroll; u++) {
+                v0[u] = one[u] ? toFloat(__ldg(tx + idx[u])) : 0.0f;
+                v1[u] = two[u] ? toFloat(__ldg(tx + idx[u] + 1)) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < kVarUnroll; u++) {
+                float sample = 0.0f;
+                if (two[u])
+                    sample = __fmul_rn(w[u], __fadd_rn(__fmul_rn(__fsub_rn(1.0f, frac[u]), v0[u]), __fmul_rn(frac[u], v1[u])));
+                else if (one[u])
+                    sample = __fmul_rn(w[u], v0[u]);
+                if (j0 + u < nw) out[static_cast<size_t>(j0 + u) * a.nD] = clampCast<OUT>(__fmul_rn(sample, scale));
+            }
+        }
+        written = nw;
+    }
+    for (int j = written; j < static_cast<int>(a.nCh); j++) out[static_cast<size_t>(j) * a.nD] = clampCast<OUT>(0.0f);
+}
+
 // Staged per-frame 2D DAS: one CTA per (scanline, chunksPerCta chunks of NT depths).
 template <typename RF, typename OUT, int NT>
 __global__ void __launch_bounds__(NT) dasStagedKernel(FrameDesc f, WindowLut lut, void* out, uint32_t maxW,
@@ -1163,10 +1250,18 @@ int sb_rawdelay_run(const sb_das_plan* plan, const void* rf, int rf_dtype, void*
     int err = fillArgs(p, a, rf, out, f_number, speed_of_sound_mm_s, window_type, window_parameter, 0, 0, st);
     if (err != SB_OK) return err;
     dim3 grid((p->numDepths + 255) / 256, p->numRx);
-    if (rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32) rawDelayKernel<int16_t, float><<<grid, 256, 0, st>>>(a);
-    else if (rf_dtype == SB_INT16) rawDelayKernel<int16_t, int16_t><<<grid, 256, 0, st>>>(a);
-    else if (out_dtype == SB_FLOAT32) rawDelayKernel<float, float><<<grid, 256, 0, st>>>(a);
-    else rawDelayKernel<float, int16_t><<<grid, 256, 0, st>>>(a);
+    // apertures within the element table: the table kernel
+    const bool table = p->maxApertureX <= kMaxApertureElems && static_cast<int64_t>(p->numChannels) * p->numSamples <= INT32_MAX;
+#define SB_RD(RFT, OUTT)                                                                 \
+    do {                                                                                 \
+        if (table) rawDelayTableKernel<RFT, OUTT><<<grid, 256, 0, st>>>(a);              \
+        else rawDelayKernel<RFT, OUTT><<<grid, 256, 0, st>>>(a);                         \
+    } while (0)
+    if (rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_RD(int16_t, float);
+    else if (rf_dtype == SB_INT16) SB_RD(int16_t, int16_t);
+    else if (out_dtype == SB_FLOAT32) SB_RD(float, float);
+    else SB_RD(float, int16_t);
+#undef SB_RD
     SB_CHECK_LAUNCH("rawDelayKernel");
     return SB_OK;
 }
