@@ -61,6 +61,10 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once nvidia-smi reports (its start-up can take longer than the region)
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
@@ -397,8 +401,10 @@ def profile_case(case: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    # defaults: 200 GPU steps (about 0.2 s timed, so nvidia-smi's 0.1 s samples fall inside), or 3 CPU
+    # steps of about 10 s each for the reference arm
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -407,6 +413,10 @@ def main():
     ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg", "chain", "misc"],
                     help="run one small case for ncu and exit")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 3 if args.impl == "reference" else 200
+    if args.warmup is None:
+        args.warmup = 1 if args.impl == "reference" else 5
     if args.profile_case:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
