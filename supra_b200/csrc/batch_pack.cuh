@@ -196,7 +196,8 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         // (two sample registers per frame instead of four, so 6 and 8 frames fit the register budget)
         // The gathers of element j + kPrefetchAhead are announced to L2 at element j's delay index
         // (neighbouring elements' delays differ by a few samples): a prefetch holds no register, and the
-        // one-element look-ahead alone leaves the DRAM latency of these gathers exposed (c1: -9%).
+        // one-element look-ahead alone leaves the DRAM latency of these gathers exposed (-9% on a batch of
+        // 64 frames of 64/128/192-element probes).
         constexpr int kPrefetchAhead = 2;
         G g = geom(j0, true);
         for (int j = j0; j < j1; j++) {
