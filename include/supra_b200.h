@@ -204,8 +204,12 @@ int sb_mock_reader_destroy(sb_mock_reader* reader);
  * Limits: num_elements <= SB_DAS_STATIC_MAX_ELEMENTS, num_depths <= SB_DAS_STATIC_MAX_DEPTHS,
  * num_rx <= SB_DAS_STATIC_MAX_SCANLINES; larger geometries are rejected with SB_ERR_INVALID_ARG.
  * The first call on a device looks up the scratch area's device address (once per device); make that
- * first call before any stream capture. All calls share the one scratch area: calls whose work
- * overlaps on the GPU (different streams, or threads) race and must be serialised by the caller. */
+ * first call before any stream capture. A device reset (cudaDeviceReset) after that first call is not
+ * supported: the looked-up address would be stale. All calls share the one scratch area: calls whose
+ * work overlaps on the GPU (different streams, or threads) race and must be serialised by the caller.
+ * Results are bit-identical to sb_das_run's (2D int16 -> float frames run the same single-frame
+ * kernel). A staged copy that never arrives raises a flag kept in the scratch area, reported (and
+ * cleared) by sb_check_device_errors like the library's other device errors. */
 #define SB_DAS_STATIC_MAX_ELEMENTS 1024
 #define SB_DAS_STATIC_MAX_DEPTHS 8192
 #define SB_DAS_STATIC_MAX_SCANLINES 1024

@@ -27,12 +27,20 @@ _lib = None
 _ref = None
 
 
+def reference_root() -> Optional[str]:
+    """The reference's source tree (the directory holding src/SupraLib), named by the SUPRA_REF
+    environment variable; None when it is unset or holds no such tree."""
+    root = os.environ.get("SUPRA_REF", "")
+    return root if root and os.path.isdir(os.path.join(root, "src", "SupraLib")) else None
+
+
 def build(ref: bool = True) -> None:
-    """Compile the oracle (and the reference checker when the reference sources are present)."""
+    """Compile the oracle (and the reference checker when SUPRA_REF names the reference sources)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "all"])
-    if ref and os.path.isdir("/root/reference/src/SupraLib"):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
-        subprocess.check_call(["make", "-s", "-C", HERE, "refgpu"])
+    root = reference_root()
+    if ref and root:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF={root}"])
+        subprocess.check_call(["make", "-s", "-C", HERE, "refgpu", f"REF={root}"])
 
 
 def lib() -> C.CDLL:

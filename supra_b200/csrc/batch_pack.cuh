@@ -59,6 +59,18 @@ struct PackArgs {
 
 __device__ __forceinline__ int floorDiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
+// Depths per work item of the single-frame path (MODE 1).
+constexpr uint32_t kSinglePackRows = 128;
+
+// MODE 1 work item `it` without an item table: (scanline, 128-depth segment), deepest segments first
+// and scanlines inner, the order the planned single-frame path writes into its table.
+__host__ __device__ __forceinline__ PackItem singleItem(uint32_t it, uint32_t nRx, uint32_t nD) {
+    const uint32_t nSeg = (nD + kSinglePackRows - 1) / kSinglePackRows;
+    const uint32_t k = nSeg - 1 - it / nRx;
+    const uint32_t seg1 = (k + 1) * kSinglePackRows < nD ? (k + 1) * kSinglePackRows : nD;
+    return PackItem{0u, it % nRx, k * kSinglePackRows, seg1};
+}
+
 template <int FP>
 struct PackAcc {
     float v[FP];
@@ -331,7 +343,7 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         __syncthreads();
         const uint32_t it = itemIdx;
         if (it >= a.nItems) return;
-        const PackItem pi = a.items[it];
+        const PackItem pi = (MODE == 1 && !a.items) ? singleItem(it, a.single.nRx, a.single.nD) : a.items[it];
         const PackDev& P = MODE == 1 ? a.single : a.packs[pi.pack];
         const LineK s = reduceLine(P.lines[pi.line]);
         const int nf = P.nf;

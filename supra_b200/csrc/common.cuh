@@ -68,5 +68,8 @@ int smCount();
 // Per-device int in global memory that kernels set when a bounded wait gives up (nullptr if it
 // could not be allocated).
 int* deviceErrorFlag();
+// sb_das_run_static's wait-failure flag on the current device (in its static scratch), or null
+// before that entry point's first call there.
+int* staticWaitFlag();
 
 }  // namespace sb

@@ -77,6 +77,13 @@ int sb_check_device_errors(int reset) {
     int h = 0;
     SB_CUDA(cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost));
     if (reset && h) SB_CUDA(cudaMemset(f, 0, sizeof(int)));
+    // the allocation-free DAS entry point keeps its own flag in its static scratch
+    if (int* fs = sb::staticWaitFlag()) {
+        int hs = 0;
+        SB_CUDA(cudaMemcpy(&hs, fs, sizeof(int), cudaMemcpyDeviceToHost));
+        if (reset && hs) SB_CUDA(cudaMemset(fs, 0, sizeof(int)));
+        h |= hs;
+    }
     if (h) return sb::fail(SB_ERR_TIMEOUT, "a device-side bounded wait gave up (staged channel data never arrived)");
     return SB_OK;
 }

@@ -953,16 +953,16 @@ FrameDesc frameOf(const sb_das_plan* p, const DasArgs& a) {
 // kernel with one frame, in the reference's exact arithmetic (MODE 1). Items are (scanline, 128-depth
 // segment), deepest segments first (they hold the most aperture elements), so a single frame still
 // spreads over every SM.
-constexpr int kSinglePackRows = 128;
 constexpr int kSinglePackThreads = 128;
+
+int launchSinglePackKernel(const DasArgs& a, const PackItem* items, uint32_t nItems, uint32_t* counter,
+                           cudaStream_t st);
 
 int launchSinglePack(sb_das_plan* p, const DasArgs& a, cudaStream_t st) {
     if (!p->packItems) {
         std::vector<PackItem> items;
         const uint32_t nSeg = (p->numDepths + kSinglePackRows - 1) / kSinglePackRows;
-        for (uint32_t k = nSeg; k-- > 0;)
-            for (uint32_t l = 0; l < p->numRx; l++)
-                items.push_back({0u, l, k * kSinglePackRows, std::min(p->numDepths, (k + 1) * kSinglePackRows)});
+        for (uint32_t it = 0; it < nSeg * p->numRx; it++) items.push_back(singleItem(it, p->numRx, p->numDepths));
         void* di = nullptr;
         uint32_t* dc = nullptr;
         cudaError_t e = cudaMalloc(&di, items.size() * sizeof(PackItem));
@@ -977,11 +977,18 @@ int launchSinglePack(sb_das_plan* p, const DasArgs& a, cudaStream_t st) {
         p->packCounter = dc;
         p->packItemCount = static_cast<uint32_t>(items.size());
     }
+    return launchSinglePackKernel(a, static_cast<const PackItem*>(p->packItems), p->packItemCount, p->packCounter, st);
+}
+
+// The single-frame pack kernel over `nItems` items: from the table `items`, or, when it is null, the
+// items singleItem() derives from the item index. `counter` is the work counter (reset here).
+int launchSinglePackKernel(const DasArgs& a, const PackItem* items, uint32_t nItems, uint32_t* counter,
+                           cudaStream_t st) {
     PackArgs pa;
     std::memset(&pa, 0, sizeof(pa));
-    pa.items = static_cast<const PackItem*>(p->packItems);
-    pa.nItems = p->packItemCount;
-    pa.counter = p->packCounter;
+    pa.items = items;
+    pa.nItems = nItems;
+    pa.counter = counter;
     pa.dec = 1;
     pa.lut = a.lut;
     PackDev& d = pa.single;
@@ -1000,9 +1007,8 @@ int launchSinglePack(sb_das_plan* p, const DasArgs& a, cudaStream_t st) {
     d.nf = 1;
     d.rf[0] = static_cast<const int16_t*>(a.rf);
     d.rfOut[0] = static_cast<float*>(a.out);
-    SB_CUDA(cudaMemsetAsync(p->packCounter, 0, sizeof(uint32_t), st));
-    const unsigned grid = static_cast<unsigned>(
-        std::min<size_t>(static_cast<size_t>(smCount()) * 8, (p->packItemCount + 1)));
+    SB_CUDA(cudaMemsetAsync(counter, 0, sizeof(uint32_t), st));
+    const unsigned grid = static_cast<unsigned>(std::min<size_t>(static_cast<size_t>(smCount()) * 8, (nItems + 1)));
     batchPackKernel<1, kSinglePackThreads, 8, 1><<<grid, kSinglePackThreads, 0, st>>>(pa);
     SB_CHECK_LAUNCH("batchPackKernel");
     return SB_OK;
@@ -1287,7 +1293,8 @@ constexpr size_t kOffYe = kOffXe + r256(kSE * sizeof(float));
 constexpr size_t kOffDepth = kOffYe + r256(kSE * sizeof(float));
 constexpr size_t kOffLines = kOffDepth + r256(kSD * sizeof(float));
 constexpr size_t kOffErr = kOffLines + r256(kSL * sizeof(LineDT));
-constexpr size_t kStaticScratchBytes = kOffErr + 256;
+constexpr size_t kOffCounter = kOffErr + 256;
+constexpr size_t kStaticScratchBytes = kOffCounter + 256;
 
 }  // namespace
 }  // namespace sb
@@ -1302,7 +1309,9 @@ namespace {
 std::mutex g_staticMutex;
 unsigned char* g_staticBase[64] = {nullptr};
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device, looked up once per device (the first
+// call of sb_das_run_static on that device). A device reset after that call is not supported: the
+// cached address would be stale.
 int staticScratchBase(unsigned char** base) {
     int dev = 0;
     SB_CUDA(cudaGetDevice(&dev));
@@ -1319,6 +1328,16 @@ int staticScratchBase(unsigned char** base) {
 }
 
 }  // namespace
+
+// The wait-failure flag of sb_das_run_static's staged kernel on the current device, or null before
+// the first call there. sb_check_device_errors reads and clears it with the library's own flag.
+int* staticWaitFlag() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_staticMutex);
+    return g_staticBase[dev] ? reinterpret_cast<int*>(g_staticBase[dev] + kOffErr) : nullptr;
+}
+
 }  // namespace sb
 
 extern "C" int sb_das_run_static(const sb_geometry* g, const void* rf, int rf_dtype, void* out, int out_dtype,
@@ -1370,7 +1389,10 @@ extern "C" int sb_das_run_static(const sb_geometry* g, const void* rf, int rf_dt
     float* ye = reinterpret_cast<float*>(base + kOffYe);
     float* dDT = reinterpret_cast<float*>(base + kOffDepth);
     LineDT* lines = reinterpret_cast<LineDT*>(base + kOffLines);
+    // the wait-failure flag keeps its value across calls (zero when the module loads) until
+    // sb_check_device_errors reads and clears it
     int* flag = reinterpret_cast<int*>(base + kOffErr);
+    uint32_t* counter = reinterpret_cast<uint32_t*>(base + kOffCounter);
     const size_t nE = g->num_elements, nD = g->num_depths, nRx = g->num_rx;
     SB_CUDA(cudaMemcpyAsync(xeMM, g->element_x_mm, nE * sizeof(float), cudaMemcpyHostToDevice, st));
     SB_CUDA(cudaMemcpyAsync(yeMM, g->element_y_mm, nE * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -1378,7 +1400,6 @@ extern "C" int sb_das_run_static(const sb_geometry* g, const void* rf, int rf_dt
     SB_CUDA(cudaMemcpyAsync(linesMM, g->scanlines, nRx * sizeof(sb_scanline_rx), cudaMemcpyHostToDevice, st));
     if (g->element_to_channel)
         SB_CUDA(cudaMemcpyAsync(e2c, g->element_to_channel, nE * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    SB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));  // the wait-failure flag starts clear on every call
     const double dt = 1.0 / g->sampling_frequency_hz;
     const double factor = 1 / 1.0 / (speed_of_sound_mm_s * dt);
     const double factorTime = 1 / 1.0 / dt;
@@ -1409,6 +1430,14 @@ extern "C" int sb_das_run_static(const sb_geometry* g, const void* rf, int rf_dt
     a.interpTx = interpolate_transmits ? 1 : 0;
     a.lut = makeLut(window_type, window_parameter);
     const bool is3D = g->rx_layout[0] > 1 && g->rx_layout[1] > 1;
+    // 2D int16 -> float with the highest-weight transmit: the single-frame pack kernel of sb_das_run
+    // (the reference's exact arithmetic), its work items derived from the item index, its work counter
+    // in the scratch area
+    if (!is3D && !interpolate_transmits && rf_dtype == SB_INT16 && out_dtype == SB_FLOAT32 &&
+        maxAx <= kMaxApertureElems && g->num_samples >= 2) {
+        const uint32_t nItems = (g->num_depths + kSinglePackRows - 1) / kSinglePackRows * g->num_rx;
+        return launchSinglePackKernel(a, nullptr, nItems, counter, st);
+    }
     const size_t rfSize = rf_dtype == SB_INT16 ? 2 : 4;
     const uint32_t maxW = stagedMaxW(g->num_channels, rfSize);
     const bool staged = !is3D && !interpolate_transmits && maxAx <= kMaxApertureElems && (g->num_samples * rfSize) % 16 == 0 &&

@@ -201,12 +201,14 @@ __device__ void planChunk(CtaState& st, RF* smemRF, int b, const FrameDesc& f, c
 }
 
 // Waits for stage b (bounded). All threads call it; returns false if the copies never completed.
+// The result is the same in every thread of the CTA (false if any thread's wait gave up), so the
+// CTA returns, or goes on to its next barrier, as a whole.
 __device__ __forceinline__ bool waitChunk(CtaState& st, int b) {
-    bool done = true;
-    if (st.staged[b]) done = mbarWaitBounded(&st.bar[b], st.phase[b], kWaitLimit);
-    __syncthreads();
+    int done = 1;
+    if (st.staged[b]) done = mbarWaitBounded(&st.bar[b], st.phase[b], kWaitLimit) ? 1 : 0;
+    done = __syncthreads_and(done);
     if (threadIdx.x == 0 && st.staged[b]) st.phase[b] ^= 1u;
-    return done;
+    return done != 0;
 }
 
 template <typename RF>

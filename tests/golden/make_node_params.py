@@ -2,7 +2,7 @@
 default) that the reference's receive-path node constructors declare with
 m_valueRangeDictionary.set<T>(...), read from the reference sources as text.
 
-    python tests/golden/make_node_params.py [reference root, default /root/reference]
+    python tests/golden/make_node_params.py [reference root, default $SUPRA_REF]
 
 The fixture lets tests check the node layer's tables where the reference tree is absent.
 """
@@ -60,7 +60,9 @@ def value(tok, typ):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SUPRA_REF", "")
+    if not root:
+        sys.exit("name the reference's source tree: argument or SUPRA_REF")
     bf = os.path.join(root, "src", "SupraLib", "Beamformer")
     out = {}
     for node, fname in NODES.items():

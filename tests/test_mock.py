@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from conftest import small_linear, small_matrix
+from oracle.oracle import reference_root
 
 MOCK = os.path.join(os.path.dirname(__file__), "golden", "mock")
 
@@ -55,7 +56,7 @@ def test_json_writer_round_trip(tmp_path, make):
     assert np.array_equal(f32bits(m.element_y), f32bits(g.element_y))
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src/SupraLib"), reason="reference sources not present")
+@pytest.mark.skipif(reference_root() is None, reason="reference sources not named by SUPRA_REF")
 def test_reference_reads_library_json(tmp_path, oracle):
     """The reference's reader on the library's JSON gives what the library's reader gives."""
     from supra_b200.mock import MockMetadata, write_mock_json

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import bf_geometries, random_rf, small_linear, small_matrix
+from oracle.oracle import reference_root
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "ref_pins.npz")
 
@@ -72,7 +73,7 @@ def test_sample_beamformers_bit_exact_vs_reference(oracle, gold):
     assert np.array_equal(bits(oracle.das_bf(g, rf, 0)), bits(oracle.das(g, rf)))
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src/SupraLib"), reason="reference sources not present")
+@pytest.mark.skipif(reference_root() is None, reason="reference sources not named by SUPRA_REF")
 def test_live_reference_checker(oracle):
     """Rebuilds oracle/_ref from the reference sources and compares a c0-sized DAS frame."""
     oracle.build(ref=True)

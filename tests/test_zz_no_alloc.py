@@ -1,56 +1,69 @@
 """The allocation-free DAS entry point (sb_das_run_static), for callers that cannot allocate device
 memory (hosts that hand out buffers only from their own pre-reserved pool, real-time frame loops
 that cannot afford cudaMalloc/cudaFree). Called through the C ABI and compared with the planned
-entry point (sb_das_plan_create + sb_das_run) on two calls in a row. Named to be collected last."""
+entry point (sb_das_plan_create + sb_das_run) on calls in a row, on every branch the static entry
+point takes: 2D int16 -> float (the single-frame pack kernel, also bit-exact against the oracle),
+3D, interpolated transmits, float channel data, int16 output and a channel map. Both entry points
+run kernels with the reference's exact arithmetic, so results are compared bit for bit. Named to be
+collected last."""
 import ctypes as C
 
 import numpy as np
 import pytest
 import torch
 
-from conftest import random_rf, small_linear
+from conftest import random_rf, small_linear, small_matrix
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-5  # relative to the frame peak, as the other DAS parity tests
+_OUT = {"f32": torch.float32, "i16": torch.int16}
 
 
-def planned(lib, geom, rf, **kw):
+def _codes(rf, out_dtype):
+    from supra_b200 import abi
+    rfc = abi.SB_INT16 if rf.dtype == torch.int16 else abi.SB_FLOAT32
+    oc = abi.SB_FLOAT32 if out_dtype == torch.float32 else abi.SB_INT16
+    return rfc, oc
+
+
+def planned(lib, geom, rf, F, c, w, itx=0, off=0, out_dtype=torch.float32):
     from supra_b200 import abi
     g = geom.ctypes()
     plan = C.c_void_p()
     assert lib.sb_das_plan_create(C.byref(g), C.byref(plan)) == abi.SB_OK
-    out = torch.empty((geom.num_depths, geom.num_rx), dtype=torch.float32, device="cuda")
-    st = lib.sb_das_run(plan, C.c_void_p(rf.data_ptr()), abi.SB_INT16, C.c_void_p(out.data_ptr()), abi.SB_FLOAT32,
-                        kw["F"], kw["c"], kw["w"], 0.0, 0, 0, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    out = torch.empty((geom.num_depths, geom.num_rx), dtype=out_dtype, device="cuda")
+    rfc, oc = _codes(rf, out_dtype)
+    st = lib.sb_das_run(plan, C.c_void_p(rf.data_ptr()), rfc, C.c_void_p(out.data_ptr()), oc, F, c, w, 0.0, itx, off,
+                        C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert st == abi.SB_OK, lib.sb_last_error()
     torch.cuda.synchronize()
     lib.sb_das_plan_destroy(plan)
     return out
 
 
-def static(lib, geom, rf, **kw):
+def static(lib, geom, rf, F, c, w, itx=0, off=0, out_dtype=torch.float32):
     from supra_b200 import abi
     g = geom.ctypes()
-    out = torch.full((geom.num_depths, geom.num_rx), float("nan"), dtype=torch.float32, device="cuda")
-    st = lib.sb_das_run_static(C.byref(g), C.c_void_p(rf.data_ptr()), abi.SB_INT16, C.c_void_p(out.data_ptr()),
-                               abi.SB_FLOAT32, kw["F"], kw["c"], kw["w"], 0.0, 0, 0,
-                               C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    # start from a value no path writes, so a pixel left unwritten shows
+    fill = float("nan") if out_dtype == torch.float32 else 12345
+    out = torch.full((geom.num_depths, geom.num_rx), fill, dtype=out_dtype, device="cuda")
+    rfc, oc = _codes(rf, out_dtype)
+    st = lib.sb_das_run_static(C.byref(g), C.c_void_p(rf.data_ptr()), rfc, C.c_void_p(out.data_ptr()), oc, F, c, w,
+                               0.0, itx, off, C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert st == abi.SB_OK, lib.sb_last_error()
     torch.cuda.synchronize()
     return out
 
 
-def close(a, b):
-    a = a.cpu().numpy().astype(np.float64)
-    b = b.cpu().numpy().astype(np.float64)
-    same = (a == b) | (np.isnan(a) & np.isnan(b))
-    peak = np.nanmax(np.abs(b[np.abs(b) < 1e30]))
-    err = np.nanmax(np.abs(np.where(same, 0.0, a - b)))
-    return err <= TOL * peak
+def same_bits(a, b):
+    a = a.cpu().numpy()
+    b = b.cpu().numpy()
+    if a.dtype == np.float32:
+        a, b = a.view(np.uint32), b.view(np.uint32)
+    return a.shape == b.shape and np.array_equal(a, b)
 
 
-def test_static_das_matches_planned_two_calls():
+def test_static_das_matches_planned_two_calls(oracle):
     from supra_b200 import abi
     from supra_b200.geometry import linear_probe_geometry
     lib = abi.load_library()
@@ -59,14 +72,49 @@ def test_static_das_matches_planned_two_calls():
     g2 = small_linear()
     rf1 = torch.from_numpy(random_rf(g1, seed=31, amp=30000)).cuda()
     rf2 = torch.from_numpy(random_rf(g2, seed=32)).cuda()
-    ref1 = planned(lib, g1, rf1, F=1.0, c=1540e3, w=1)
-    ref2 = planned(lib, g2, rf2, F=0.8, c=1500e3, w=2)
-    out1 = static(lib, g1, rf1, F=1.0, c=1540e3, w=1)
-    out2 = static(lib, g2, rf2, F=0.8, c=1500e3, w=2)
-    assert close(out1, ref1)
-    assert close(out2, ref2)
+    ref1 = planned(lib, g1, rf1, 1.0, 1540e3, 1)
+    ref2 = planned(lib, g2, rf2, 0.8, 1500e3, 2)
+    out1 = static(lib, g1, rf1, 1.0, 1540e3, 1)
+    out2 = static(lib, g2, rf2, 0.8, 1500e3, 2)
+    assert same_bits(out1, ref1)
+    assert same_bits(out2, ref2)
+    # the oracle (the reference's FP32 semantics; 0/0 pixels clamp to -FLT_MAX)
+    exp = oracle.das(g2, rf2.cpu().numpy(), 0.8, c_mm_s=1500e3, window=2)
+    exp = np.where(np.isnan(exp), -np.float32(3.4028235e38), exp).astype(np.float32)
+    assert np.array_equal(out2.cpu().numpy().view(np.uint32), exp.view(np.uint32))
     # and once more the first geometry after the second
-    assert close(static(lib, g1, rf1, F=1.0, c=1540e3, w=1), ref1)
+    assert same_bits(static(lib, g1, rf1, 1.0, 1540e3, 1), ref1)
+    assert lib.sb_check_device_errors(1) == abi.SB_OK
+
+
+def _channel_mapped():
+    g = small_linear()
+    m = np.arange(g.num_elements, dtype=np.int32) % g.num_channels
+    m[5] = -1
+    m[17] = -1
+    g.element_to_channel = m
+    return g
+
+
+@pytest.mark.parametrize("case", ["3d", "interp_tx", "float_rf", "int16_out", "channel_map", "offset"])
+def test_static_das_other_branches(case):
+    """Each branch twice in a row (second call with other data), bit for bit against sb_das_run."""
+    from supra_b200 import abi
+    lib = abi.load_library()
+    g = small_matrix() if case == "3d" else _channel_mapped() if case == "channel_map" else small_linear()
+    kw = {"F": 1.0, "c": 1540e3, "w": 1}
+    if case == "interp_tx":
+        kw["itx"] = 1
+    if case == "offset":
+        kw["off"] = 3
+    if case == "int16_out":
+        kw["out_dtype"] = torch.int16
+    for seed in (41, 42):
+        x = random_rf(g, seed=seed, amp=3000 if case != "int16_out" else 300)
+        rf = torch.from_numpy(x.astype(np.float32) if case == "float_rf" else x).cuda()
+        ref = planned(lib, g, rf, **kw)
+        got = static(lib, g, rf, **kw)
+        assert same_bits(got, ref), (case, seed)
     assert lib.sb_check_device_errors(1) == abi.SB_OK
 
 
