@@ -340,6 +340,104 @@ def extras(wl, plans):
     return res
 
 
+def reference_gpu_rows(res):
+    """The reference's own kernels on this GPU (BASELINE row B2): the reference's sources built with its
+    production flags (--use_fast_math, release), oracle/_ref/libsupra_ref_gpu_fast.so, each called as its
+    node calls it per frame (kernels + pooled output allocation), CUDA-event time per call on the call's
+    stream. Beside each: the library's time for the same input from `res` and the speed-up. Even FIR
+    lengths read one tap past the reference's filter buffer, so the envelope comparison uses 65 taps."""
+    import ctypes as C
+    import torch
+    from oracle import oracle as O
+    from supra_b200 import synth
+    from supra_b200 import workloads as W
+    from supra_b200.api import HilbertFirEnvelope, mv_beamform
+    lib = O.refgpu_fast_lib()
+    if lib is None:
+        return {"unavailable": "oracle/_ref/libsupra_ref_gpu_fast.so not built (make -C oracle refgpu)"}
+    out = {"build": "reference sources, nvcc --use_fast_math -O2, NDEBUG (SupraLib/CMakeLists.txt:65)",
+           "timing": "CUDA events around back-to-back calls of the reference's class method on its stream"}
+
+    def row(name, ref_ms, ours_ms, what):
+        out[name] = {"reference_ms": ref_ms, "ours_ms": ours_ms,
+                     "speedup": (ref_ms / ours_ms) if (ref_ms and ours_ms and ref_ms > 0) else None, "what": what}
+
+    def geo(g):
+        return g.ctypes()
+
+    g0, rf0 = synth.c0_frame(0, device="cpu")
+    x0 = np.ascontiguousarray(rf0.numpy())
+    gc = geo(g0)
+    ms = lib.refg_time_das(C.byref(gc), C.c_void_p(x0.ctypes.data), C.c_double(1.0),
+                           C.c_double(g0.speed_of_sound_mm_s), 1, 0, C.c_double(g0.depth_mm), 20)
+    row("das_c0", ms, res.get("das_c0", {}).get("ms"), "2D DAS, c0 frame (128 lines x 2048 depths, int16 in)")
+    for bf, name in ((1, "das_DelayAndStdDev"), (2, "das_CoherenceFactorDelayAndSum")):
+        ms = lib.refg_time_das(C.byref(gc), C.c_void_p(x0.ctypes.data), C.c_double(1.0),
+                               C.c_double(g0.speed_of_sound_mm_s), 1, bf, C.c_double(g0.depth_mm), 10)
+        row(name, ms, res.get(name, {}).get("ms"), "sample beamformer on the c0 frame")
+    ms = lib.refg_time_rawdelay(C.byref(gc), C.c_void_p(x0.ctypes.data), C.c_double(1.0),
+                                C.c_double(g0.speed_of_sound_mm_s), 1, C.c_double(g0.depth_mm), 10)
+    row("rawdelay_c0", ms, res.get("rawdelay_c0", {}).get("ms"), "RawDelay of the c0 frame")
+    g2 = W.c2_geometry()
+    x2 = np.ascontiguousarray(W.c2_volume(g2).cpu().numpy())
+    gc2 = geo(g2)
+    ms = lib.refg_time_das(C.byref(gc2), C.c_void_p(x2.ctypes.data), C.c_double(1.0),
+                           C.c_double(g2.speed_of_sound_mm_s), 1, 0, C.c_double(g2.depth_mm), 3)
+    row("das3d_c2", ms, res.get("das3d_c2", {}).get("ms"), "3D DAS, c2 volume (32 x 32 lines x 1024 depths)")
+    del x2
+    # envelope chain on a 16384 x 2048 float image (128 MB, above L2)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    big = torch.randn((16384, 2048), generator=gen, device="cuda") * 1000.0
+    hb = np.ascontiguousarray(big.cpu().numpy())
+    ms = lib.refg_time_hilbert(C.c_void_p(hb.ctypes.data), C.c_uint32(2048), C.c_uint32(16384), C.c_uint32(65), 10)
+    hil = HilbertFirEnvelope(65)
+    row("hilbert_env_large_65taps", ms, _graph_ms(lambda: hil.demodulate(big), 10),
+        "Hilbert FIR envelope, 65 taps, 16384 x 2048 float image")
+    f = np.array([7e6]), np.array([1e6]), np.array([1.0])
+    fa = [np.ascontiguousarray(v, np.float64) for v in f]
+    ms = lib.refg_time_iq(C.c_void_p(hb.ctypes.data), C.c_uint32(2048), C.c_uint32(16384), C.c_double(40e6),
+                          C.c_double(7e6), C.c_double(2.5e6), C.c_uint32(51), C.c_uint32(51), C.c_uint32(4),
+                          C.c_uint32(1), *(C.c_void_p(v.ctypes.data) for v in fa), 10)
+    row("iq_magnitude_large", ms, res.get("iq_magnitude_large", {}).get("ms"),
+        "IQ magnitude, 51-tap filters, decimation 4, 16384 x 2048 float image")
+    ms = lib.refg_time_logcompress(C.c_void_p(hb.ctypes.data), C.c_uint32(2048), C.c_uint32(16384), C.c_double(50.0),
+                                   C.c_double(1.0), C.c_double(4000.0), 10)
+    row("logcompress_large", ms, res.get("logcompress_large", {}).get("ms"),
+        "log compression to uint8, 16384 x 2048 float image")
+    del big, hb
+    # scan conversion of the c0 envelope at 0.1 mm
+    img0 = np.abs(np.random.Generator(np.random.PCG64(3)).standard_normal((g0.num_depths, g0.num_rx))).astype(np.float32)
+    rs = O.RefScan(g0.scanlines, g0.rx_layout, g0.num_depths, g0.depth_mm, 0.1, lib=lib)
+    ms = lib.refg_time_scan(rs.h, C.c_void_p(img0.ctypes.data), 20)
+    row("scan_c0", ms, res.get("chain_c0", {}).get("scan_ms"), "2D scan conversion of the c0 frame to 0.1 mm, uint8")
+    del rs
+    # FFT envelope of the c0 image, temporal filter of 3 x 64 MB
+    ms = lib.refg_time_fft_env(C.c_void_p(img0.ctypes.data), C.c_uint32(g0.num_rx), C.c_uint32(g0.num_depths), 10)
+    row("analytic_env_c0", ms, res.get("analytic_env_c0", {}).get("ms"), "FFT (analytic-signal) envelope, c0 image")
+    t = np.random.Generator(np.random.PCG64(4)).standard_normal((4096, 4096)).astype(np.float32)
+    ms = lib.refg_time_temporal(C.c_void_p(t.ctypes.data), C.c_uint32(3), C.c_uint32(4096), C.c_uint32(4096), 10)
+    row("temporal_filter", ms, res.get("temporal_filter", {}).get("ms"), "temporal filter of 3 float 4096 x 4096 images")
+    del t
+    # minimum variance on the c0 frame's raw-delayed data (real), 2000 depths (the reference's MV
+    # handles at most 2000 samples), L 32, +-5; the library with the reference's loading trace/L
+    from supra_b200.api import RxBeamformer
+    raw = RxBeamformer(g0).raw_delay(rf0.cuda(), 1.0, window_type=1)
+    raw[~(raw.abs() < 1e30)] = 0.0
+    raw = raw[:, :, :2000].contiguous()
+    rh = np.ascontiguousarray(raw.cpu().numpy())
+    ms = lib.refg_time_mv(C.c_void_p(rh.ctypes.data), C.c_uint32(128), C.c_uint32(64), C.c_uint32(2000), C.c_uint32(32),
+                          C.c_uint32(5), C.c_double(1.5), 1)
+    ours = _event_ms(lambda: mv_beamform(raw, 32, 5, 1.5, False, 1.0, 1e6, with_stats=False), 5, warm=2)
+    row("mv_c0_2000", ms, ours, "MV (real, loading trace/L), c0 raw-delayed 128 lines x 64 channels x 2000 depths, L 32, +-5")
+    ms = lib.refg_time_mvpcg(C.c_void_p(rh.ctypes.data), C.c_uint32(128), C.c_uint32(64), C.c_uint32(2000),
+                             C.c_uint32(32), C.c_uint32(5), C.c_double(1.5), 2)
+    from supra_b200.api import mv_beamform_pcg
+    ours = _event_ms(lambda: mv_beamform_pcg(raw, 32, 5), 5, warm=2)
+    row("mv_pcg_c0_2000", ms, ours, "MV-PCG, same input")
+    return out
+
+
 def profile_case(case: str):
     """One small invocation for an ncu capture (no timing)."""
     import torch
@@ -408,6 +506,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own GPU kernels")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements (c0, c2, c3, c4)")
     ap.add_argument("--frames", type=int, default=64, help="frames per launch (64 = the named workload)")
     ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg", "chain", "misc"],
@@ -506,6 +605,11 @@ def main():
         extra = extras(wl, plans)
         extra["per_frame_path"]["batched_speedup"] = value / extra["per_frame_path"]["px_per_s"]
 
+    # baseline leg (rank 0, one GPU): the reference's own GPU kernels on this GPU beside the library's
+    # rows, and the reference's CPU path on the host cores
+    ref_gpu = None
+    if rank == 0 and world == 1 and extra is not None and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_rows(extra)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -536,6 +640,7 @@ def main():
                          else "batchDasIqKernel",
                          "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms},
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),

@@ -274,6 +274,108 @@ def refg_iq(img: np.ndarray, fs: float, reference_frequency: float, cutoff: floa
     return out.reshape(-1, nRx)
 
 
+class RefScan:
+    """ScanConverter of the reference on the GPU: tables of updateInternals and convert()."""
+
+    def __init__(self, scanlines: np.ndarray, layout, num_samples: int, depth_mm: float, resolution_mm: float,
+                 lib=None):
+        self.lib = lib or refgpu_lib()
+        self.lib.refg_scan_create.restype = _vp
+        sl = np.ascontiguousarray(scanlines)
+        self.h = _vp(self.lib.refg_scan_create(_vp(_p(sl)), C.c_uint32(layout[0]), C.c_uint32(layout[1]),
+                                               C.c_uint32(num_samples), C.c_double(depth_mm),
+                                               C.c_double(resolution_mm)))
+        size = np.zeros(3, np.uint32)
+        self.lib.refg_scan_size(self.h, _vp(_p(size)))
+        self.size = tuple(int(v) for v in size)
+        self.numel = int(np.prod(self.size))
+        self.is2D = layout[0] == 1 or layout[1] == 1
+        self.num_rx = int(layout[0]) * int(layout[1])
+        self.num_samples = num_samples
+
+    def tables(self) -> dict:
+        n = self.numel
+        t = {"mask": np.zeros(n, np.uint8), "sample_idx": np.zeros(n, np.uint32), "weight_x": np.zeros(n, np.float32),
+             "weight_y": np.zeros(n, np.float32), "weight_z": np.zeros(n, np.float32)}
+        assert self.lib.refg_scan_tables(self.h, *(_vp(_p(t[k])) for k in ("mask", "sample_idx", "weight_x",
+                                                                            "weight_y", "weight_z"))) == 0
+        return t
+
+    def convert(self, img: np.ndarray, uint8=True) -> np.ndarray:
+        x = np.ascontiguousarray(img, np.float32)
+        assert x.size == self.num_rx * self.num_samples
+        out = np.zeros(self.numel, np.uint8 if uint8 else np.float32)
+        assert self.lib.refg_scan_convert(self.h, _vp(_p(x)), _vp(_p(out)), C.c_int(int(uint8))) == 0
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.refg_scan_destroy(self.h)
+            self.h = None
+
+
+def refg_mv(raw: np.ndarray, subarray_size: int, temporal_smoothing: int, scaling_power=1.5) -> np.ndarray:
+    """RxBeamformerMV::performRxBeamforming of the reference on the GPU (cuBLAS batched LU), real
+    raw-delayed data [scanlines][channels][samples], samples <= 2000: image [samples][scanlines]."""
+    x = np.ascontiguousarray(raw, np.float32)
+    nRx, nCh, nS = x.shape
+    assert nS <= 2000, "the reference's MV handles at most 2000 samples"
+    out = np.zeros(nS * nRx, np.float32)
+    assert refgpu_lib().refg_mv(_vp(_p(x)), _vp(_p(out)), C.c_uint32(nRx), C.c_uint32(nCh), C.c_uint32(nS),
+                                C.c_uint32(subarray_size), C.c_uint32(temporal_smoothing),
+                                C.c_double(scaling_power)) == 0
+    return out.reshape(nS, nRx)
+
+
+def refg_mvpcg(raw: np.ndarray, subarray_size: int, temporal_smoothing: int, max_iterations_override=0,
+               convergence_threshold=1e-10, scaling_power=1.5) -> np.ndarray:
+    """RxBeamformerMVpcg::performRxBeamforming of the reference on the GPU: image [samples][scanlines]."""
+    x = np.ascontiguousarray(raw, np.float32)
+    nRx, nCh, nS = x.shape
+    out = np.zeros(nS * nRx, np.float32)
+    assert refgpu_lib().refg_mvpcg(_vp(_p(x)), _vp(_p(out)), C.c_uint32(nRx), C.c_uint32(nCh), C.c_uint32(nS),
+                                   C.c_uint32(subarray_size), C.c_uint32(temporal_smoothing),
+                                   C.c_uint32(max_iterations_override), C.c_double(convergence_threshold),
+                                   C.c_double(scaling_power)) == 0
+    return out.reshape(nS, nRx)
+
+
+def refg_temporal(images, weights) -> np.ndarray:
+    """TemporalFilter::filter of the reference on the GPU over float images (oldest first)."""
+    ims = [np.ascontiguousarray(a, np.float32) for a in images]
+    h, w = ims[0].shape
+    ptrs = (C.c_void_p * len(ims))(*[_p(a) for a in ims])
+    wt = np.ascontiguousarray(weights, np.float64)
+    out = np.zeros((h, w), np.float32)
+    assert refgpu_lib().refg_temporal(ptrs, C.c_uint32(len(ims)), _vp(_p(wt)), C.c_uint32(w), C.c_uint32(h),
+                                      _vp(_p(out))) == 0
+    return out
+
+
+def refg_fft_env(img: np.ndarray) -> np.ndarray:
+    """HilbertEnvelope::computeHilbertEnvelope of the reference on the GPU (cuFFT)."""
+    x = np.ascontiguousarray(img, np.float32)
+    out = np.zeros_like(x)
+    assert refgpu_lib().refg_fft_env(_vp(_p(x)), _vp(_p(out)), C.c_uint32(x.shape[1]), C.c_uint32(x.shape[0])) == 0
+    return out
+
+
+# the same reference sources built with the reference's production flags (--use_fast_math): the
+# per-kernel timing baseline on the GPU
+REF_GPU_FAST_LIB = os.path.join(HERE, "_ref", "libsupra_ref_gpu_fast.so")
+_refgf = None
+
+
+def refgpu_fast_lib() -> Optional[C.CDLL]:
+    global _refgf
+    if _refgf is None and os.path.exists(REF_GPU_FAST_LIB):
+        _refgf = C.CDLL(REF_GPU_FAST_LIB)
+        for name in ("refg_time_das", "refg_time_rawdelay", "refg_time_hilbert", "refg_time_logcompress", "refg_time_iq",
+                     "refg_time_scan", "refg_time_mv", "refg_time_mvpcg", "refg_time_fft_env", "refg_time_temporal"):
+            getattr(_refgf, name).restype = C.c_float
+    return _refgf
+
+
 def das_adjoint64(geom, rf: np.ndarray, apod, gout: np.ndarray, c_mm_s=None, f_number=1.0, window=1, window_param=0.0):
     """FP64 reference gradient of the apodised 2D DAS: (grad_rf, grad_apod, grad_c)."""
     g = geom.ctypes()

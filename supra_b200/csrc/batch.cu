@@ -409,7 +409,8 @@ int launchBatch(sb_batch_plan* p, int nt, int ctas, int fp, int staged, cudaStre
             if (nt == 128) { if (mb >= 12) SB_PACK_LAUNCH(4, 128, 12); else SB_PACK_LAUNCH(4, 128, 8); }
             else { if (mb >= 6) SB_PACK_LAUNCH(4, 256, 6); else if (mb >= 5) SB_PACK_LAUNCH(4, 256, 5); else SB_PACK_LAUNCH(4, 256, 4); }
         } else {
-            if (nt == 128) SB_PACK_LAUNCH(8, 128, 8); else { if (mb >= 5) SB_PACK_LAUNCH(8, 256, 5); else SB_PACK_LAUNCH(8, 256, 4); }
+            if (nt == 128) SB_PACK_LAUNCH(8, 128, 8);
+            else { if (mb >= 5) SB_PACK_LAUNCH(8, 256, 5); else if (mb == 4) SB_PACK_LAUNCH(8, 256, 4); else SB_PACK_LAUNCH(8, 256, 3); }
         }
 #undef SB_PACK_LAUNCH
         SB_CHECK_LAUNCH("batchPackKernel");
@@ -665,7 +666,7 @@ int sb_batch_autotune(sb_batch_plan* p, const char* cache_path, int32_t* ctas_pe
     }
     // {ctas per SM, depth tile, frames per pack, staged}
     const int shapes[][4] = {{1, 384, 1, 0}, {4, 256, 4, 0}, {5, 256, 4, 0}, {6, 256, 4, 0}, {8, 128, 4, 0},
-                             {12, 128, 4, 0}, {4, 256, 8, 0}, {5, 256, 8, 0}, {8, 128, 8, 0}, {1, 128, 4, 1},
+                             {12, 128, 4, 0}, {3, 256, 8, 0}, {4, 256, 8, 0}, {5, 256, 8, 0}, {8, 128, 8, 0}, {1, 128, 4, 1},
                              {1, 128, 2, 1},  {2, 128, 2, 1}};
     float best = 1e30f;
     int bestC = p->ctasPerSm, bestT = p->nt, bestF = p->fp, bestG = p->staged;

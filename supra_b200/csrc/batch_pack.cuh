@@ -158,7 +158,11 @@ __device__ __forceinline__ void packDepth(const ElemRec* el, int n, const float*
 // of elements inside the aperture (contiguous when the table is ordered by x) and each weight is the
 // window-LUT entry of dx / min(aDT, maxElementDistance), summed into wsum in element order (the
 // reference's order).
-template <int FP, int K, bool USE_OFFSET, bool DEEP, bool EXACT>
+//
+// INTERIOR: every element's delay lies in [0, nS - 1) (checked by the caller), so the record-edge cases
+// drop out. DX2: the scanline is not steered laterally (dirX == 0), so x_e - x_line(d) = dx for every
+// depth and the table's first field holds dx * dx (the same float product the general form computes).
+template <int FP, int K, bool USE_OFFSET, bool DEEP, bool EXACT, bool INTERIOR, bool DX2>
 __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, int j1, const float* lut, const PackDev& P,
                                                    const LineK& s, const int16_t* const (&tb)[FP], float d,
                                                    float invMax, float& wsum, PackAcc<FP>& acc) {
@@ -183,15 +187,32 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
             const float ws = __fadd_rn(wsum, w);
             wsum = count ? ws : wsum;
         }
-        const float ex = __fsub_rn(e.xel, xz);
-        float t = __fadd_rn(s.iD, __fadd_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2)), d));
+        float ex2;
+        if constexpr (DX2) {
+            ex2 = e.xel;
+        } else {
+            const float ex = __fsub_rn(e.xel, xz);
+            ex2 = __fmul_rn(ex, ex);
+        }
+        float t = __fadd_rn(s.iD, __fadd_rn(__fsqrt_rn(__fadd_rn(ex2, dy2)), d));
         const float delayf = USE_OFFSET ? __fadd_rn(t, P.offset) : t;
         float fl;
         const int32_t delay = floorIdx(delayf, fl);
         const float frac = __fsub_rn(delayf, fl);
+        G g;
+        if constexpr (INTERIOR) {
+            if constexpr (EXACT) {
+                g.wA = w;
+                g.wB = frac;
+            } else {
+                g.wB = __fmul_rn(w, frac);
+                g.wA = __fmul_rn(w, __fsub_rn(1.0f, frac));
+            }
+            g.off = static_cast<uint32_t>(e.ch) + static_cast<uint32_t>(delay);
+            return g;
+        }
         const bool interior = static_cast<uint32_t>(delay) < nS - 1;
         const bool lastOne = !interior && static_cast<uint32_t>(delay) < nS && frac == 0.0f;
-        G g;
         const uint32_t idx = interior ? static_cast<uint32_t>(delay) : (lastOne ? nS - 2 : 0u);
         if constexpr (EXACT) {  // (weight, fraction) for the reference's arithmetic, see packDepth
             g.wA = (interior || lastOne) ? w : 0.0f;
@@ -211,6 +232,19 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         // one-element look-ahead alone leaves the DRAM latency of these gathers exposed (-9% on a batch of
         // 64 frames of 64/128/192-element probes).
         constexpr int kPrefetchAhead = 2;
+        // the frames' sums in pairs: one packed FMA (two IEEE fused multiply-adds) per pair of frames,
+        // the same rounding as one fmaf per frame
+        static_assert(K % 2 == 0, "wide loops take pairs of frames");
+        float2 acc2[K / 2];
+#pragma unroll
+        for (int f = 0; f < K; f += 2) acc2[f / 2] = make_float2(acc.v[f], acc.v[f + 1]);
+        // one lane per frame announces the warp's window: frame f from lane 31 - f (the deepest
+        // lanes stay longest in the loop), two 128-byte lines from the shallowest active lane's index
+        const int pfFrame = 31 - static_cast<int>(threadIdx.x & 31);
+        const int16_t* tbl = tb[0];
+#pragma unroll
+        for (int f = 1; f < K; f++) tbl = pfFrame == f ? tb[f] : tbl;
+        const bool pfLane = pfFrame < K;
         G g = geom(j0, true);
         for (int j = j0; j < j1; j++) {
             int16_t a[K], b[K];
@@ -224,14 +258,30 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
                 // an address inside that channel's row
                 const uint32_t offp = static_cast<uint32_t>(el[j + kPrefetchAhead].ch) +
                                       (g.off - static_cast<uint32_t>(el[j].ch));
-#pragma unroll
-                for (int f = 0; f < K; f++) asm volatile("prefetch.global.L2 [%0];" ::"l"(tb[f] + offp));
+                const unsigned m = __activemask();
+                const uint32_t offw = __shfl_sync(m, offp, __ffs(m) - 1);
+                if (pfLane) {
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(tbl + offw));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(tbl + offw + 64));
+                }
             }
             const G gn = geom(min(j + 1, j1 - 1), j + 1 < j1);
+            const float2 wA2 = make_float2(g.wA, g.wA), wB2 = make_float2(g.wB, g.wB);
 #pragma unroll
-            for (int f = 0; f < K; f++)
-                acc.v[f] = fmaf(g.wB, s16ToFloat(b[f]), fmaf(g.wA, static_cast<float>(a[f]), acc.v[f]));
+            for (int f = 0; f < K; f += 2) {
+                // int16 -> float: a by the conversion unit, b as (1.5 * 2^23 + b) - 1.5 * 2^23 (exact),
+                // both subtractions of a pair in one packed add
+                const float2 va = make_float2(static_cast<float>(a[f]), static_cast<float>(a[f + 1]));
+                const float2 vb = __fadd2_rn(make_float2(__int_as_float(0x4B400000 + b[f]), __int_as_float(0x4B400000 + b[f + 1])),
+                                             make_float2(-12582912.0f, -12582912.0f));
+                acc2[f / 2] = __ffma2_rn(wB2, vb, __ffma2_rn(wA2, va, acc2[f / 2]));
+            }
             g = gn;
+        }
+#pragma unroll
+        for (int f = 0; f < K; f += 2) {
+            acc.v[f] = acc2[f / 2].x;
+            acc.v[f + 1] = acc2[f / 2].y;
         }
         return;
     }
@@ -289,26 +339,55 @@ __device__ __forceinline__ void apertureRange(const ElemRec* el, int n, float aD
 // One beamformed depth for the first K frames of the pack: the deep path (every element active
 // with its precomputed weight), the aperture range of an x-ordered table, or the element-by-element
 // aperture test; then the reference's normalisation (sum / weight sum * count) and clamped cast.
+// dx2: the table's first field holds dx * dx (unsteered line); otherwise the element's x.
 template <int FP, int K, bool EXACT>
 __device__ __forceinline__ void packRow(const ElemRec* el, int n, const float* lut, const PackDev& P, const LineK& s,
                                         const int16_t* const (&tb)[FP], int nf, float d, int deepOk, int sortedX,
-                                        float sumDeep, int cntDeep, PackAcc<FP>& acc) {
+                                        float sumDeep, int cntDeep, bool dx2, PackAcc<FP>& acc) {
     const float aDT = apertureDTf(d, P.dt, P.c, P.F);
     const bool useOffset = P.offset != 0.0f;
     float wsum = 0.0f;
     int cnt = 0;
-    if (deepOk && aDT >= s.maxDistX && n > 0) {
-        if (useOffset) packDepthPipelined<FP, K, true, true, EXACT>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
-        else packDepthPipelined<FP, K, false, true, EXACT>(el, 0, n, lut, P, s, tb, d, 0.0f, wsum, acc);
-        wsum = sumDeep;
-        cnt = cntDeep;
-    } else if (sortedX) {
-        const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
-        int j0, j1;
-        apertureRange(el, n, aDT, j0, j1);
-        if (useOffset) packDepthPipelined<FP, K, true, false, EXACT>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
-        else packDepthPipelined<FP, K, false, false, EXACT>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc);
-        cnt = j1 - j0;
+    const bool deep = deepOk && aDT >= s.maxDistX && n > 0;
+    if (deep || sortedX) {
+        float invMax = 0.0f;
+        int j0 = 0, j1 = n;
+        if (!deep) {
+            invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
+            apertureRange(el, n, aDT, j0, j1);
+        }
+        // Every delay of the range inside [0, nS - 1)? Delays grow with |dx| (the table is ordered by dx, so
+        // the largest |dx| is at an end of the range) and each is at least iD + d (+ offset): bounding the
+        // two ends bounds all, with the same float operations the loop uses. For unsteered lines only
+        // (dx2 holds dx * dx); voted over the warp so that its lanes take the same loop.
+        bool inRange = false;
+        if (dx2 && j1 > j0) {
+            const float dyy = __fmul_rn(s.dirY, d);
+            const float dy2 = __fmul_rn(dyy, dyy);
+            const float lo = useOffset ? __fadd_rn(__fadd_rn(s.iD, d), P.offset) : __fadd_rn(s.iD, d);
+            const float e2 = fmaxf(el[j0].xel, el[j1 - 1].xel);
+            const float t = __fadd_rn(s.iD, __fadd_rn(__fsqrt_rn(__fadd_rn(e2, dy2)), d));
+            const float hi = useOffset ? __fadd_rn(t, P.offset) : t;
+            inRange = lo >= 0.0f && hi < static_cast<float>(P.nS - 1);
+        }
+        inRange = __all_sync(__activemask(), inRange);
+#define SB_PACK_ROW(OFS, DP)                                                                                          \
+    do {                                                                                                              \
+        if (inRange) packDepthPipelined<FP, K, OFS, DP, EXACT, true, true>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc); \
+        else if (dx2) packDepthPipelined<FP, K, OFS, DP, EXACT, false, true>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc); \
+        else packDepthPipelined<FP, K, OFS, DP, EXACT, false, false>(el, j0, j1, lut, P, s, tb, d, invMax, wsum, acc); \
+    } while (0)
+        if (deep) {
+            if (useOffset) SB_PACK_ROW(true, true);
+            else SB_PACK_ROW(false, true);
+            wsum = sumDeep;
+            cnt = cntDeep;
+        } else {
+            if (useOffset) SB_PACK_ROW(true, false);
+            else SB_PACK_ROW(false, false);
+            cnt = j1 - j0;
+        }
+#undef SB_PACK_ROW
     } else {
         const float invMax = __fdiv_rn(1.0f, fminf(aDT, s.maxDistX));
         if (useOffset) packDepth<FP, K, false, true, EXACT>(el, n, lut, P, s, tb, nf, d, aDT, invMax, wsum, cnt, acc);
@@ -333,7 +412,7 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
     // the item's beamformed depths (segment + low-pass halo), for the IQ epilogue of MODE 0
     __shared__ float seg[MODE == 0 ? FP : 1][MODE == 0 ? kPackRows : 1];
     __shared__ uint32_t itemIdx;
-    __shared__ int nEl, cntDeep, deepOk, sortedX;
+    __shared__ int nEl, cntDeep, deepOk, sortedX, dx2Line;
     __shared__ float sumDeep;
     const int tid = threadIdx.x;
     if (tid < 64) lut[tid] = a.lut.v[tid];
@@ -377,6 +456,10 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
                 }
             const int sortedAll = __syncthreads_and(sortedMine);
             const int okAll = __syncthreads_and(okMine);
+            // an unsteered line ordered by x keeps dx * dx in place of x (its only use from here on)
+            const bool toDx2 = valid && sortedAll && s.dirX == 0.0f;
+            if (toDx2)
+                for (int j = tid; j < n0; j += NT) el[j].xel = __fmul_rn(el[j].dx, el[j].dx);
             if (tid == 0) {
                 float sum = 0.0f;
                 const int m = valid ? n0 : 0;
@@ -386,6 +469,7 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
                 cntDeep = m;
                 deepOk = okAll;
                 sortedX = sortedAll;
+                dx2Line = toDx2 ? 1 : 0;
             }
         }
         __syncthreads();
@@ -408,9 +492,11 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             cntDeep = m;
             deepOk = ok;
             sortedX = sorted;
+            dx2Line = 0;
         }
         __syncthreads();
         const int n = nEl;
+        const bool dx2 = dx2Line != 0;
         const int16_t* tb[FP];
 #pragma unroll
         for (int f = 0; f < FP; f++)
@@ -432,10 +518,10 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             for (int f = 0; f < FP; f++) acc.v[f] = 0.0f;
             if (r < rEnd && valid) {
                 const float d = __ldg(P.depth + r);
-                if (kw == FP) packRow<FP, FP, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
-                else if (FP == 8 && kw == kSix) packRow<FP, kSix, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
-                else if (kw == kHalf) packRow<FP, kHalf, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
-                else packRow<FP, 1, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, acc);
+                if (kw == FP) packRow<FP, FP, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                else if (FP == 8 && kw == kSix) packRow<FP, kSix, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                else if (kw == kHalf) packRow<FP, kHalf, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                else packRow<FP, 1, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
             }
             if (MODE == 1) {
                 if (r < rEnd) P.rfOut[0][pi.line + static_cast<size_t>(r) * P.nRx] = acc.v[0];

@@ -1,0 +1,162 @@
+"""The library against the reference's own scan converter, minimum-variance beamformers, temporal
+filter and FFT envelope, run on the same GPU and the same inputs.
+
+oracle/_ref/libsupra_ref_gpu.so is built (make -C oracle refgpu) from the reference's sources
+(ScanConverter.cu, RxBeamformerMV.cu, RxBeamformerMVpcg.cu, TemporalFilter.cu, HilbertEnvelope.cu
+and the others) as a release build without fast-math and without FMA contraction. Expected results:
+  * scan-conversion tables (mask, sample index, weights): bit-exact in 2D and in 3D on every pixel
+    the reference's mask marks. The reference's 2D table loop runs serially in the checker (built
+    without OpenMP), so a pixel on a shared scanline edge takes the later quad;
+  * scan conversion (the table gathers): uint8 within 1 LSB and float within 1e-6 of the peak;
+  * temporal filter: bit-exact;
+  * MV (cuBLAS batched LU in the reference, FP32 Cholesky here): both are FP32 solves of the same
+    loaded systems, and both are compared with the FP64 restatement. The library's error against
+    FP64 must not exceed the reference's own by more than 2x, and the two outputs must agree within
+    the stated fraction of the peak. Only records of at most 2000 samples are used: the reference's
+    MV reads past its 2000-entry buffers beyond that;
+  * MV-PCG: the reference iterates in FP32 with atomics in its products, so it is not
+    bit-reproducible itself. Outputs must agree within 2e-4 of the peak on at least 99% of the
+    pixels;
+  * FFT envelope (cuFFT in the reference, an exact circulant Hilbert product here): within 1e-5 of
+    the peak.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import small_linear, small_matrix
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref(oracle):
+    if oracle.refgpu_lib() is None:
+        pytest.skip("reference GPU kernels not built (make -C oracle refgpu needs the reference sources)")
+    return oracle
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def _scan_geometries():
+    from supra_b200.geometry import linear_probe_geometry
+    from supra_b200.workloads import c2_geometry
+    g0 = linear_probe_geometry(128, 0.3, 64, 2048, 40e6, aperture=64, focus_mm=20.0)  # the c0 probe
+    return {"c0_0.1mm": (g0, 0.1), "lin_0.05mm": (small_linear(), 0.05), "mat_0.2mm": (small_matrix(), 0.2),
+            "c2_0.25mm": (c2_geometry(), 0.25)}
+
+
+@pytest.mark.parametrize("name", ["c0_0.1mm", "lin_0.05mm", "mat_0.2mm", "c2_0.25mm"])
+def test_scan_tables_bit_exact_vs_reference(ref, name):
+    from supra_b200.api import ScanConverter
+    g, res = _scan_geometries()[name]
+    rs = ref.RefScan(g.scanlines, g.rx_layout, g.num_depths, g.depth_mm, res)
+    sc = ScanConverter(g.scanlines, g.rx_layout, g.num_depths, g.depth_mm, res)
+    t = sc.tables()
+    r = rs.tables()
+    assert tuple(t["size"]) == rs.size, (t["size"], rs.size)
+    assert np.array_equal(t["mask"], r["mask"]), f"{np.count_nonzero(t['mask'] != r['mask'])} mask entries differ"
+    m = r["mask"].astype(bool)
+    assert m.any()
+    keys = ("sample_idx", "weight_x", "weight_y") + (() if rs.is2D else ("weight_z",))
+    for k in keys:
+        a = t[k][m].view(np.uint32)
+        b = r[k][m].view(np.uint32)
+        assert np.array_equal(a, b), f"{k}: {np.count_nonzero(a != b)} of {a.size} differ"
+
+
+@pytest.mark.parametrize("name", ["c0_0.1mm", "mat_0.2mm"])
+@pytest.mark.parametrize("uint8", [True, False])
+def test_scan_convert_vs_reference(ref, name, uint8):
+    from supra_b200.api import ScanConverter
+    g, res = _scan_geometries()[name]
+    rng = np.random.Generator(np.random.PCG64(8))
+    img = np.abs(rng.standard_normal((g.num_depths, g.num_rx)) * 80.0).astype(np.float32)
+    rs = ref.RefScan(g.scanlines, g.rx_layout, g.num_depths, g.depth_mm, res)
+    want = rs.convert(img, uint8=uint8)
+    sc = ScanConverter(g.scanlines, g.rx_layout, g.num_depths, g.depth_mm, res)
+    got = sc.convert(torch.from_numpy(img).cuda(), torch.uint8 if uint8 else torch.float32).cpu().numpy().ravel()
+    assert got.shape == want.shape
+    if uint8:
+        assert np.abs(got.astype(int) - want.astype(int)).max() <= 1
+    else:
+        assert np.max(np.abs(got - want)) <= 1e-6 * np.max(np.abs(want))
+
+
+def test_temporal_filter_bit_exact_vs_reference(ref):
+    from supra_b200.api import temporal_filter
+    rng = np.random.Generator(np.random.PCG64(9))
+    ims = [(rng.standard_normal((333, 257)) * 1000).astype(np.float32) for _ in range(4)]
+    w = [0.1, 0.2, 0.3, 0.4]
+    want = ref.refg_temporal(ims, w)
+    got = temporal_filter([torch.from_numpy(x).cuda() for x in ims], w).cpu().numpy()
+    assert np.array_equal(bits(got), bits(want))
+
+
+@pytest.mark.parametrize("nS,nL", [(2048, 128), (1000, 37)])
+def test_fft_envelope_vs_reference(ref, nS, nL):
+    from supra_b200.api import HilbertEnvelope
+    rng = np.random.Generator(np.random.PCG64(10))
+    x = (rng.standard_normal((nS, nL)) * 1000).astype(np.float32)
+    want = ref.refg_fft_env(x)
+    got = HilbertEnvelope(nS).envelope(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want))
+
+
+def _mv_input(nRx, nCh, nS, seed, aperture_zeros=False):
+    """Real raw-delayed-like data; with aperture_zeros, channels outside a depth-dependent aperture are
+    zero as in RawDelay's output, but every sample keeps at least one nonzero channel."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    x = (rng.standard_normal((nRx, nCh, nS)) * 500).astype(np.float32)
+    if aperture_zeros:
+        for d in range(nS):
+            half = min(nCh // 2, 2 + (d * nCh) // nS)  # the aperture widens with depth, full at mid-record
+            lo, hi = nCh // 2 - half, nCh // 2 + half
+            x[:, :lo, d] = 0.0
+            x[:, hi:, d] = 0.0
+    return x
+
+
+@pytest.mark.parametrize("L,T,zeros", [(16, 2, False), (32, 5, False), (32, 3, True)])
+def test_mv_vs_reference(ref, oracle, L, T, zeros):
+    """sb_mv_run (loading trace/sz, as the reference) against RxBeamformerMV. Where the active
+    aperture is narrower than L the reference's un-reset smoothing buffer carries entries of earlier
+    systems outside the active block (a documented deviation), so those samples are excluded."""
+    from supra_b200.api import mv_beamform
+    x = _mv_input(8, 64, 1000, 20 + L, aperture_zeros=zeros)
+    want = ref.refg_mv(x, L, T, 1.5)
+    fp64 = oracle.mv(x, L, T, precision=64)
+    got, st = mv_beamform(torch.from_numpy(x).cuda(), L, T, 1.5, False, 1.0, 0.0)
+    got = got.cpu().numpy()
+    active = np.count_nonzero(x != 0.0, axis=1)  # [scanline][sample] nonzero channels
+    keep = np.ones(got.shape, bool)
+    if zeros:
+        # samples whose temporal window holds a narrower aperture than L (any of its 2T + 1 samples)
+        narrow = (active < L).T  # [sample][scanline]
+        for dt in range(-T, T + 1):
+            keep &= ~np.roll(narrow, dt, axis=0)
+    peak = np.max(np.abs(fp64[keep]))
+    err_ref = np.max(np.abs(want[keep] - fp64[keep])) / peak
+    err_ours = np.max(np.abs(got[keep] - fp64[keep])) / peak
+    err_pair = np.max(np.abs(got[keep] - want[keep])) / peak
+    print(f"MV L={L} T={T}: reference vs FP64 {err_ref:.3g}, library vs FP64 {err_ours:.3g}, "
+          f"library vs reference {err_pair:.3g} of peak over {np.count_nonzero(keep)} samples")
+    assert np.count_nonzero(keep) > got.size // 2
+    assert err_ours <= max(2.0 * err_ref, 1e-6)
+    assert err_pair <= 1e-4
+
+
+@pytest.mark.parametrize("L,T", [(16, 2), (32, 5)])
+def test_mv_pcg_vs_reference(ref, L, T):
+    from supra_b200.api import mv_beamform_pcg
+    rng = np.random.Generator(np.random.PCG64(30 + L))
+    x = rng.standard_normal((8, 64, 1024)).astype(np.float32)  # unit scale: the FP32 PCG stays accurate
+    want = ref.refg_mvpcg(x, L, T)
+    got = mv_beamform_pcg(torch.from_numpy(x).cuda(), subarray_size=L, temporal_smoothing=T).cpu().numpy()
+    peak = np.max(np.abs(want))
+    ok = np.abs(got - want) <= 2e-4 * peak
+    print(f"MV-PCG L={L} T={T}: {np.mean(ok) * 100:.3f}% within 2e-4 of peak, "
+          f"max {np.max(np.abs(got - want)) / peak:.3g}")
+    assert np.mean(ok) >= 0.99
