@@ -431,10 +431,10 @@ def reference_gpu_rows(res):
     ours = _event_ms(lambda: mv_beamform(raw, 32, 5, 1.5, False, 1.0, 1e6, with_stats=False), 5, warm=2)
     row("mv_c0_2000", ms, ours, "MV (real, loading trace/L), c0 raw-delayed 128 lines x 64 channels x 2000 depths, L 32, +-5")
     ms = lib.refg_time_mvpcg(C.c_void_p(rh.ctypes.data), C.c_uint32(128), C.c_uint32(64), C.c_uint32(2000),
-                             C.c_uint32(32), C.c_uint32(5), C.c_double(1.5), 2)
+                             C.c_uint32(32), C.c_uint32(5), C.c_double(1e-4), C.c_double(1.5), 2)
     from supra_b200.api import mv_beamform_pcg
-    ours = _event_ms(lambda: mv_beamform_pcg(raw, 32, 5), 5, warm=2)
-    row("mv_pcg_c0_2000", ms, ours, "MV-PCG, same input")
+    ours = _event_ms(lambda: mv_beamform_pcg(raw, 32, 5, convergence_threshold=1e-4), 5, warm=2)
+    row("mv_pcg_c0_2000", ms, ours, "MV-PCG (convergence threshold 1e-4, the node's default), same input")
     return out
 
 

@@ -328,7 +328,7 @@ def refg_mv(raw: np.ndarray, subarray_size: int, temporal_smoothing: int, scalin
 
 
 def refg_mvpcg(raw: np.ndarray, subarray_size: int, temporal_smoothing: int, max_iterations_override=0,
-               convergence_threshold=1e-10, scaling_power=1.5) -> np.ndarray:
+               convergence_threshold=1e-4, scaling_power=1.5) -> np.ndarray:
     """RxBeamformerMVpcg::performRxBeamforming of the reference on the GPU: image [samples][scanlines]."""
     x = np.ascontiguousarray(raw, np.float32)
     nRx, nCh, nS = x.shape

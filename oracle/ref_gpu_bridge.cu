@@ -369,11 +369,11 @@ float refg_time_mv(const float* raw, uint32_t numRx, uint32_t numCh, uint32_t nu
 }
 
 float refg_time_mvpcg(const float* raw, uint32_t numRx, uint32_t numCh, uint32_t numS, uint32_t subArraySize,
-                      uint32_t temporalSmoothing, double scalingPower, int iters) {
+                      uint32_t temporalSmoothing, double convergenceThreshold, double scalingPower, int iters) {
     auto rd = delayedOf(raw, numRx, numCh, numS);
     return timeCalls(rd->getData<float>()->getStream(), iters, [&]() {
-        RxBeamformerMVpcg::performRxBeamforming<float, float>(rd, subArraySize, temporalSmoothing, 0, 1e-10,
-                                                              scalingPower, false);
+        RxBeamformerMVpcg::performRxBeamforming<float, float>(rd, subArraySize, temporalSmoothing, 0,
+                                                              convergenceThreshold, scalingPower, false);
     });
 }
 

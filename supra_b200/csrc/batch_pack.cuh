@@ -238,13 +238,15 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         float2 acc2[K / 2];
 #pragma unroll
         for (int f = 0; f < K; f += 2) acc2[f / 2] = make_float2(acc.v[f], acc.v[f + 1]);
-        // one lane per frame announces the warp's window: frame f from lane 31 - f (the deepest
-        // lanes stay longest in the loop), two 128-byte lines from the shallowest active lane's index
-        const int pfFrame = 31 - static_cast<int>(threadIdx.x & 31);
+        // Each lane announces one frame, frame lane % K, at its own depth's index: the lanes of a frame
+        // (every K-th lane, depths K apart) cover the warp's 32-depth window of that row with one
+        // prefetch instruction per element for all K frames.
         const int16_t* tbl = tb[0];
+        {
+            const int pf = static_cast<int>(threadIdx.x & 31) % K;
 #pragma unroll
-        for (int f = 1; f < K; f++) tbl = pfFrame == f ? tb[f] : tbl;
-        const bool pfLane = pfFrame < K;
+            for (int f = 1; f < K; f++) tbl = pf == f ? tb[f] : tbl;
+        }
         G g = geom(j0, true);
         for (int j = j0; j < j1; j++) {
             int16_t a[K], b[K];
@@ -258,12 +260,7 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
                 // an address inside that channel's row
                 const uint32_t offp = static_cast<uint32_t>(el[j + kPrefetchAhead].ch) +
                                       (g.off - static_cast<uint32_t>(el[j].ch));
-                const unsigned m = __activemask();
-                const uint32_t offw = __shfl_sync(m, offp, __ffs(m) - 1);
-                if (pfLane) {
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(tbl + offw));
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(tbl + offw + 64));
-                }
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(tbl + offp));
             }
             const G gn = geom(min(j + 1, j1 - 1), j + 1 < j1);
             const float2 wA2 = make_float2(g.wA, g.wA), wB2 = make_float2(g.wB, g.wB);
@@ -512,7 +509,11 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         constexpr int kSix = FP == 8 ? 6 : FP;
         const int kw = nf > kSix ? FP : nf > kHalf ? kSix : (nf > 1 ? kHalf : 1);
         for (int k = 0; k < nBlocks; k++) {
-            const int r = rStart + k * NT + tid;
+            // deeper rows hold wider apertures (more elements): odd blocks give the warps their rows in
+            // mirrored order, so that over an item each warp sums a mix of shallow and deep rows and
+            // the warps reach the item's barrier together
+            const int wb = tid & ~31;
+            const int r = rStart + k * NT + (((k & 1) && MODE == 0) ? (NT - 32 - wb) + (tid & 31) : tid);
             PackAcc<FP> acc;
 #pragma unroll
             for (int f = 0; f < FP; f++) acc.v[f] = 0.0f;
@@ -546,9 +547,10 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             const int so = so0 + o;
             const int base = so * a.dec - a.half;
             const bool interior = base >= 0 && base + a.taps <= nD;
-            float re[FP], im[FP];
+            // (re, im) of each frame in one packed FMA per tap: two IEEE fused multiply-adds
+            float2 z[FP];
 #pragma unroll
-            for (int f = 0; f < FP; f++) re[f] = im[f] = 0.0f;
+            for (int f = 0; f < FP; f++) z[f] = make_float2(0.0f, 0.0f);
             for (int j = 0; j < a.taps; j++) {
                 const int nn = base + j;
                 if (!interior && (nn < 0 || nn >= nD)) continue;
@@ -557,15 +559,14 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
 #pragma unroll
                 for (int f = 0; f < FP; f++) {
                     if (f < nf) {
-                        const float x = seg[f][nn - rStart] * lpj;
-                        re[f] = fmaf(x, w.x, re[f]);
-                        im[f] = fmaf(x, w.y, im[f]);
+                        const float x = __fmul_rn(seg[f][nn - rStart], lpj);
+                        z[f] = __ffma2_rn(make_float2(x, x), w, z[f]);
                     }
                 }
             }
 #pragma unroll
             for (int f = 0; f < FP; f++)
-                if (f < nf) P.iq[f][pi.line + static_cast<size_t>(so) * P.nRx] = make_float2(re[f], im[f]);
+                if (f < nf) P.iq[f][pi.line + static_cast<size_t>(so) * P.nRx] = z[f];
         }
         // the next item's first barrier orders these reads of seg before its writes
     }

@@ -104,3 +104,81 @@ def grad_c(geom, rf, apod, dec, c_mm_s, gout):
                     acc += w * float(apod[e]) * (rf[tx, ch, i + 1] - rf[tx, ch, i]) * (-path / (c_mm_s * c_mm_s * dt))
             total += g * len(terms) / den * acc
     return total
+
+
+class SmoothModelTorch:
+    """The same FP64 model as forward() (decisions of the FP32 path at the nominal c, delays in FP64
+    from the mm geometry), vectorised with torch over every (scanline, depth, element) of the
+    highest-weight transmit, for geometries where the Python loops are too slow. Linear arrays
+    (the element's lateral position and the scanline's lateral direction only)."""
+
+    def __init__(self, geom, c_mm_s, lut, f_number=1.0, device="cuda"):
+        import torch
+        f32, f64 = torch.float32, torch.float64
+        dt = 1.0 / geom.sampling_frequency_hz
+        factor = 1.0 / (c_mm_s * dt)
+        self.geom, self.dt, self.device = geom, dt, device
+        nE, nD, nRx, nCh = geom.num_elements, geom.num_depths, geom.num_rx, geom.num_channels
+        xe = torch.tensor(geom.element_x.astype(np.float64) * factor, dtype=f64, device=device).to(f32)
+        dep = torch.tensor(geom.depths.astype(np.float64) * factor, dtype=f64, device=device).to(f32)
+        dtf = torch.tensor(np.float32(dt), device=device)
+        cf = torch.tensor(np.float32(c_mm_s), device=device)
+        two_f = torch.tensor(np.float32(2 * np.float32(f_number)), device=device)
+        aDT = (((dep * dtf) * cf) / two_f / cf) / dtf  # [nD], float32, one rounding per operation
+        lut_t = torch.tensor(np.asarray(lut, np.float32), device=device)
+        lines = geom.scanlines
+        ks = [int(np.argmax(s["tx_weights"])) for s in lines]
+        first = np.array([int(s["tx"][k]["first"][0]) for s, k in zip(lines, ks)])
+        last = np.array([int(s["tx"][k]["last"][0]) for s, k in zip(lines, ks)])
+        nA = int(max(1, (last - first).max()))
+        e_idx = torch.tensor(first, device=device)[:, None] + torch.arange(nA, device=device)[None, :]  # [nRx][nA]
+        in_ap = e_idx < torch.tensor(last, device=device)[:, None]
+        e_c = torch.clamp(e_idx, max=nE - 1)
+        x = torch.tensor([np.float32(s["position"][0] * factor) for s in lines], device=device)
+        maxd = torch.tensor([np.float32(s["max_element_distance"][0] * factor) for s in lines], device=device)
+        dx = xe[e_c] - x[:, None]  # [nRx][nA] float32
+        inv = 1.0 / torch.minimum(aDT[None, :], maxd[:, None])  # [nRx][nD]
+        member = (dx.abs()[:, None, :] <= aDT[None, :, None]) & in_ap[:, None, :]  # [nRx][nD][nA]
+        rel = dx[:, None, :] * inv[:, :, None]
+        rel = torch.where(torch.isnan(rel), torch.full_like(rel, -1.0), rel).clamp(-1.0, 1.0)
+        v = (rel + 1.0) * torch.tensor(np.float32(31.5), device=device)
+        idx = torch.floor(v.to(f64) + 0.5).long()  # roundf of a non-negative float
+        w = lut_t[idx].to(f64) * member.to(f64)
+        self.member, self.w = member, w
+        self.count = member.sum(dim=2).to(f64)  # [nRx][nD]
+        self.e = e_c
+        self.ch = (e_c % nCh)
+        self.tx = torch.tensor([int(s["tx"][k]["tx_idx"]) for s, k in zip(lines, ks)], device=device)
+        self.t0 = torch.tensor([s["tx"][k]["initial_delay"] / dt for s, k in zip(lines, ks)], dtype=f64,
+                               device=device)
+        self.px = torch.tensor([s["position"][0] for s in lines], dtype=f64, device=device)
+        self.dirx = torch.tensor([s["direction"][0] for s in lines], dtype=f64, device=device)
+        self.diry = torch.tensor([s["direction"][1] for s in lines], dtype=f64, device=device)
+        self.xe_mm = torch.tensor(geom.element_x.astype(np.float64), device=device)
+        self.d_mm = torch.tensor(geom.depths.astype(np.float64), device=device)
+
+    def forward(self, rf, c_mm_s, apod=None):
+        """rf [num_tx][num_channels][num_samples] (torch, any float type, on the model's device) ->
+        FP64 image [num_depths][num_rx] (0 where no element is in the aperture, NaN where the weights
+        of the aperture's elements sum to 0)."""
+        import torch
+        g = self.geom
+        nS = g.num_samples
+        W = self.w if apod is None else self.w * apod.to(torch.float64)[self.e][:, None, :]
+        den = W.sum(dim=2)
+        lat = self.xe_mm[self.e][:, None, :] - (self.px[:, None, None] + self.dirx[:, None, None] * self.d_mm[None, :, None])
+        path = torch.hypot(lat, (self.diry[:, None] * self.d_mm[None, :])[:, :, None]) + self.d_mm[None, :, None]
+        tau = self.t0[:, None, None] + path / (c_mm_s * self.dt)
+        i = torch.floor(tau)
+        fr = tau - i
+        i = i.long()
+        ok = (i >= 0) & (i < nS - 1)
+        ic = torch.clamp(i, 0, nS - 2)
+        base = (self.tx[:, None, None] * g.num_channels + self.ch[:, None, :]) * nS
+        flat = rf.reshape(-1).to(torch.float64)
+        v0 = flat[base + ic]
+        v1 = flat[base + ic + 1]
+        num = (W * torch.where(ok, (1 - fr) * v0 + fr * v1, torch.zeros_like(fr))).sum(dim=2)
+        out = num / den * self.count  # [nRx][nD]
+        out = torch.where(self.count == 0, torch.zeros_like(out), out)  # no element in the aperture: 0
+        return out.T.contiguous()

@@ -149,14 +149,24 @@ def test_mv_vs_reference(ref, oracle, L, T, zeros):
 
 
 @pytest.mark.parametrize("L,T", [(16, 2), (32, 5)])
-def test_mv_pcg_vs_reference(ref, L, T):
+def test_mv_pcg_vs_reference(ref, oracle, L, T):
+    """Both run Jacobi-PCG in FP32 from a = 1 with the node's default threshold 1e-4. Of the systems the
+    reference's own iteration solves to within 1e-4 of the peak of the FP64 PCG, at least 99.9% of the
+    library's are within 2e-4 of the reference's; the library loses no more systems than the reference
+    (twice its count plus 0.1%)."""
     from supra_b200.api import mv_beamform_pcg
     rng = np.random.Generator(np.random.PCG64(30 + L))
-    x = rng.standard_normal((8, 64, 1024)).astype(np.float32)  # unit scale: the FP32 PCG stays accurate
-    want = ref.refg_mvpcg(x, L, T)
-    got = mv_beamform_pcg(torch.from_numpy(x).cuda(), subarray_size=L, temporal_smoothing=T).cpu().numpy()
-    peak = np.max(np.abs(want))
-    ok = np.abs(got - want) <= 2e-4 * peak
-    print(f"MV-PCG L={L} T={T}: {np.mean(ok) * 100:.3f}% within 2e-4 of peak, "
-          f"max {np.max(np.abs(got - want)) / peak:.3g}")
-    assert np.mean(ok) >= 0.99
+    x = rng.standard_normal((8, 64, 1024)).astype(np.float32)
+    want = ref.refg_mvpcg(x, L, T, convergence_threshold=1e-4)
+    got = mv_beamform_pcg(torch.from_numpy(x).cuda(), subarray_size=L, temporal_smoothing=T,
+                          convergence_threshold=1e-4).cpu().numpy()
+    fp64 = oracle.mv_pcg(x, L, T, threshold=1e-4, precision=64)
+    peak = np.max(np.abs(fp64))
+    stable = np.abs(want - fp64) <= 1e-4 * peak
+    agree = np.abs(got - want) <= 2e-4 * peak
+    lost_ours = np.count_nonzero(np.abs(got - fp64) > 2e-4 * peak)
+    print(f"MV-PCG L={L} T={T}: reference stable on {np.mean(stable) * 100:.3f}%, library within 2e-4 of the "
+          f"reference on {np.mean(agree[stable]) * 100:.3f}% of those; lost systems: library {lost_ours}, "
+          f"reference {np.count_nonzero(~stable)}")
+    assert np.mean(agree[stable]) >= 0.999
+    assert lost_ours <= 2 * np.count_nonzero(~stable) + 1e-3 * got.size

@@ -63,3 +63,22 @@ def test_adjoint_identity_rf(oracle, small_case):
     lhs = _dot(oracle.das(g, d, 1.0, window=1, apod=apod, precision=64), gout)
     rhs = float(np.sum(d.astype(np.float64) * grf))
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+def test_vectorised_smooth_model_matches_loops(oracle, small_case):
+    """SmoothModelTorch (used for the c4-size finite differences on the GPU) against the loop model on
+    the CPU: the same decisions and the same FP64 forward at c0 and at c0 + 10 mm/s."""
+    import torch
+    import adjoint_model as M
+    g, rf, apod, _ = small_case
+    c0 = g.speed_of_sound_mm_s
+    lut = oracle.window_lut(1)
+    dec = M.decisions(g, c0, lut)
+    tm = M.SmoothModelTorch(g, c0, lut, device="cpu")
+    rf64 = rf.astype(np.float64)
+    for c in (c0, c0 + 10.0):
+        want = M.forward(g, rf64, apod, dec, c)
+        got = tm.forward(torch.from_numpy(rf), c, torch.from_numpy(apod)).numpy()
+        both = np.isfinite(want) & np.isfinite(got)
+        assert np.array_equal(np.isfinite(want), np.isfinite(got))
+        assert np.max(np.abs(got[both] - want[both])) <= 1e-9 * np.max(np.abs(want[both]))
