@@ -356,7 +356,8 @@ def reference_gpu_rows(res):
     if lib is None:
         return {"unavailable": "oracle/_ref/libsupra_ref_gpu_fast.so not built (make -C oracle refgpu)"}
     out = {"build": "reference sources, nvcc --use_fast_math -O2, NDEBUG (SupraLib/CMakeLists.txt:65)",
-           "timing": "CUDA events around back-to-back calls of the reference's class method on its stream"}
+           "timing": "CUDA events around back-to-back calls of the reference's class method on its stream; "
+                     "smallest of 5 repetitions"}
 
     def row(name, ref_ms, ours_ms, what):
         out[name] = {"reference_ms": ref_ms, "ours_ms": ours_ms,
@@ -485,6 +486,9 @@ def profile_case(case: str):
         g2 = W.c2_geometry()
         rf2 = W.c2_volume(g2)
         RxBeamformer(g2).beamform(rf2, 1.0, window_type=1)
+    elif case == "refgpu":
+        # the reference's own kernels (production flags) on the rows' inputs, for their launch list
+        print(json.dumps(reference_gpu_rows({}), default=str)[:200])
     elif case == "adjoint":
         from supra_b200 import workloads as W
         g4, rf4 = W.c4_batch(frames=2)
@@ -509,7 +513,7 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own GPU kernels")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements (c0, c2, c3, c4)")
     ap.add_argument("--frames", type=int, default=64, help="frames per launch (64 = the named workload)")
-    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg", "chain", "misc"],
+    ap.add_argument("--profile-case", choices=["batch", "mv", "adjoint", "das3d", "pcg", "chain", "misc", "refgpu"],
                     help="run one small case for ncu and exit")
     args = ap.parse_args()
     if args.steps is None:

@@ -238,15 +238,6 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         float2 acc2[K / 2];
 #pragma unroll
         for (int f = 0; f < K; f += 2) acc2[f / 2] = make_float2(acc.v[f], acc.v[f + 1]);
-        // Each lane announces one frame, frame lane % K, at its own depth's index: the lanes of a frame
-        // (every K-th lane, depths K apart) cover the warp's 32-depth window of that row with one
-        // prefetch instruction per element for all K frames.
-        const int16_t* tbl = tb[0];
-        {
-            const int pf = static_cast<int>(threadIdx.x & 31) % K;
-#pragma unroll
-            for (int f = 1; f < K; f++) tbl = pf == f ? tb[f] : tbl;
-        }
         G g = geom(j0, true);
         for (int j = j0; j < j1; j++) {
             int16_t a[K], b[K];
@@ -260,7 +251,8 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
                 // an address inside that channel's row
                 const uint32_t offp = static_cast<uint32_t>(el[j + kPrefetchAhead].ch) +
                                       (g.off - static_cast<uint32_t>(el[j].ch));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(tbl + offp));
+#pragma unroll
+                for (int f = 0; f < K; f++) asm volatile("prefetch.global.L2 [%0];" ::"l"(tb[f] + offp));
             }
             const G gn = geom(min(j + 1, j1 - 1), j + 1 < j1);
             const float2 wA2 = make_float2(g.wA, g.wA), wB2 = make_float2(g.wB, g.wB);

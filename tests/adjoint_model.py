@@ -157,6 +157,18 @@ class SmoothModelTorch:
         self.xe_mm = torch.tensor(geom.element_x.astype(np.float64), device=device)
         self.d_mm = torch.tensor(geom.depths.astype(np.float64), device=device)
 
+    def tau_range(self, c_mm_s):
+        """(smallest, largest) delay in samples over each pixel's aperture elements at c:
+        [num_depths][num_rx] each (+inf / -inf for an empty aperture)."""
+        import torch
+        lat = self.xe_mm[self.e][:, None, :] - (self.px[:, None, None] + self.dirx[:, None, None] * self.d_mm[None, :, None])
+        path = torch.hypot(lat, (self.diry[:, None] * self.d_mm[None, :])[:, :, None]) + self.d_mm[None, :, None]
+        tau = self.t0[:, None, None] + path / (c_mm_s * self.dt)
+        inf = torch.full_like(tau, float("inf"))
+        lo = torch.where(self.member, tau, inf).amin(dim=2)
+        hi = torch.where(self.member, tau, -inf).amax(dim=2)
+        return lo.T.contiguous(), hi.T.contiguous()
+
     def forward(self, rf, c_mm_s, apod=None):
         """rf [num_tx][num_channels][num_samples] (torch, any float type, on the model's device) ->
         FP64 image [num_depths][num_rx] (0 where no element is in the aperture, NaN where the weights

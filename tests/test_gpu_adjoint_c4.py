@@ -1,7 +1,9 @@
 """The differentiable DAS at its stated shape: 16 frames of the 128-element c0 geometry (FP32 channel
 data [16][128 transmits][64 channels][2048 samples], 1 GiB), the loss 1/2 ||env(DAS(rf; apod, c)) -
 target||^2 with the 64-tap Hilbert FIR envelope, and the target rendered at a seeded true speed of
-sound c_true ~ U[1450, 1600] m/s. The forward and the gradients run through the libtorch autograd
+sound c_true ~ U[1450, 1600] m/s. The loss covers the pixels whose aperture delays stay inside the
+record (where a delay crosses the record's end, a term jumps between 0 and a sample value and the
+loss is not continuous in c). The forward and the gradients run through the libtorch autograd
 Functions (torch.ops.supra_b200.das_apod / .envelope) at c = 1540 m/s.
 
 Checks, with the tolerances written here:
@@ -64,11 +66,20 @@ def c4():
         t = torch.where(t.abs() < 1e30, t, torch.zeros_like(t))
         target = envelope(t, hil)
     c0 = 1540e3
+    # The loss covers the pixels whose aperture delays all stay inside the record (1 <= tau <= nS - 3 at
+    # c0): where a delay crosses the record's end a term jumps between 0 and a sample value, so the loss
+    # would not be continuous in c there (a finite difference in c would pick up the jumps)
+    import adjoint_model as M
+    from oracle import oracle as O
+    model = M.SmoothModelTorch(g, c0, O.window_lut(1), device="cuda")
+    tlo, thi = model.tau_range(c0)
+    inrec = (tlo >= 1.0) & (thi <= g.num_samples - 3.0)
     rf_g = rf.clone().requires_grad_(True)
     ap = apod.clone().requires_grad_(True)
     c = torch.tensor(c0, dtype=torch.float64, device="cuda", requires_grad=True)
     s = das_apod(bf, rf_g, ap, c)
-    valid = s.detach().abs() < 1e30  # no gradient through the reference's clamped 0/0 pixels
+    # no gradient through the reference's clamped 0/0 pixels, nor through pixels outside the record
+    valid = (s.detach().abs() < 1e30) & inrec[None]
     s = torch.where(valid, s, torch.zeros_like(s))
     loss = 0.5 * ((envelope(s, hil) - target) ** 2).sum()
     loss.backward()
@@ -76,7 +87,7 @@ def c4():
     return {"g": g, "rf": rf.cpu().numpy(), "target": target.double().cpu(), "valid": valid.cpu(), "c0": c0,
             "s32": s.detach().double().cpu(),
             "c_true": c_true, "loss": float(loss), "grad_rf": rf_g.grad, "grad_apod": ap.grad.cpu().numpy(),
-            "grad_c": float(c.grad)}
+            "grad_c": float(c.grad), "model": model, "inrec_frac": float(inrec.float().mean())}
 
 
 def _loss64(oracle, case, apod, c_mm_s, taps):
@@ -164,7 +175,7 @@ def test_c4_grad_c_finite_differences_at_stated_step(oracle, c4):
     gc = c4["grad_c"]
     h = 10.0  # mm/s = 1e-2 m/s
     fd_oracle = (_loss64(oracle, c4, apod, c4["c0"] + h, taps) - _loss64(oracle, c4, apod, c4["c0"] - h, taps)) / (2 * h)
-    model = M.SmoothModelTorch(g, c4["c0"], oracle.window_lut(1), device="cuda")
+    model = c4["model"]
     valid = c4["valid"].cuda()
     target = c4["target"].cuda()
     rfs = [torch.from_numpy(c4["rf"][f]).cuda() for f in range(c4["rf"].shape[0])]
@@ -183,6 +194,7 @@ def test_c4_grad_c_finite_differences_at_stated_step(oracle, c4):
     dev_oracle = abs(gc - fd_oracle) / abs(fd_oracle)
     dev_smooth = abs(gc - fd_smooth) / abs(fd_smooth)
     dev_conv = abs(gc - fd_conv) / abs(fd_conv)
+    print(f"c4 loss over {c4['inrec_frac'] * 100:.1f}% of the pixels (aperture delays inside the record)")
     print(f"c4 grad_c {gc:.6g}: central differences at 1e-2 m/s of the FP32-decision forward {fd_oracle:.6g} "
           f"(deviation {dev_oracle:.3g}), of the smooth FP64 model {fd_smooth:.6g} (deviation {dev_smooth:.3g}); "
           f"smooth model at 1e-4 m/s {fd_conv:.6g} (deviation {dev_conv:.3g})")
