@@ -134,3 +134,20 @@ def test_mv_rejects_unsupported():
     xc = torch.zeros((2, 80, 64), device="cuda", dtype=torch.complex64)
     with pytest.raises(SupraError):
         mv_beamform(xc, subarray_size=40)
+
+
+def test_mv_c3_shape_error_vs_fp64(oracle):
+    """The c3 workload (complex raw-delayed [128 lines][128 channels][2048 depths] with two interferers,
+    L = 32, +-5, loading trace/(100 L), FP64 re-solve above a condition estimate of 1e6) against the
+    all-FP64 restatement on every 16th scanline; the measured error and the number of FP64 re-solves
+    are printed."""
+    from supra_b200 import workloads as W
+    g3, x3 = W.c3_raw_delayed()
+    out, stats = _mv(x3, subarray_size=W.C3_L, temporal_smoothing=W.C3_T, loading_scale=W.C3_LOADING,
+                     fp64_threshold=1e6)
+    sub = x3[::16].contiguous()
+    ref = oracle.mv(sub.cpu().numpy(), W.C3_L, W.C3_T, loading_scale=W.C3_LOADING, precision=64)
+    err = _peak_err(out[:, ::16], ref)
+    print(f"c3 MV vs FP64 (16 of 128 scanlines, 2048 depths): {err:.3g} of the peak; FP64 re-solves "
+          f"{stats.fp64_systems} of {stats.systems}; largest condition estimate {stats.max_condition_estimate:.4g}")
+    assert err <= 1e-3
