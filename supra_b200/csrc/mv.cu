@@ -18,8 +18,12 @@
 //    kept as an unevaluated pair (hi, lo) updated by TwoSum (Knuth), so a bright echo that leaves the
 //    window cancels to O(eps^2) instead of leaving O(eps) of its energy behind. For L in (32, 64]
 //    (real data) every sample's window is summed directly.
+//    The window's TwoSum updates of complex entries run on (re, im) pairs in packed adds
+//    (__fadd2_rn, and s - h as the exact __ffma2_rn(h, -1, s)).
 //  * The loaded matrix is transposed through shared memory into one row per lane and factored by an
-//    FP32 Crout Cholesky R = G G^H (broadcast reads of the finished rows). Only forward substitutions
+//    FP32 Crout Cholesky R = G G^H (broadcast reads of the finished rows). Complex matrices with one
+//    row per lane are kept in two planes (real and imaginary parts), so that the inner products over
+//    pairs of columns run as packed FMAs with natural operands (solveRegsCplx). Only forward substitutions
 //    are needed: with z = G^-1 1 and w = G^-1 xbar, sum_v a_v = z^H z and sum_v xbar_v a*_v = w^T z*.
 //  * Condition estimate (max G_ii / min G_ii)^2. Systems above the threshold (or whose FP32
 //    factorisation breaks down) are appended to a queue that a second kernel re-solves in FP64
@@ -37,7 +41,7 @@ namespace sb {
 namespace {
 
 constexpr uint32_t kMvBlock = 2000;  // RxBeamformerMV.cu:390 sampleBlockSize
-constexpr uint32_t kMvRun = 50;      // consecutive samples per warp; divides kMvBlock
+constexpr uint32_t kMvRun = 25;      // consecutive samples per warp; divides kMvBlock (25: the c3 warps fill 8.9 waves of 148 SMs x 8 warps)
 constexpr int kMvMaxWarps = 8;
 constexpr size_t kMvSmemBudget = 220 * 1024;
 constexpr uint32_t kFull = 0xffffffffu;
@@ -259,7 +263,20 @@ __device__ __forceinline__ void addCov(const Elem<C>* xv, SampleMeta m, V<T>* d0
                 cur = c == 0 ? E0[q] : nxt;
             }
             if (act) {
-                if constexpr (COMP) {
+                if constexpr (COMP && C && std::is_same<T, float>::value) {
+                    // TwoSum of the real and imaginary parts in packed adds (s - h etc. as fma(h, -1, s))
+                    const float2 m1 = make_float2(-1.0f, -1.0f);
+                    const float2 h = make_float2(hi[q][r].re, hi[q][r].im);
+                    const float2 b = make_float2(sign * cur.re, sign * cur.im);
+                    const float2 s2 = __fadd2_rn(h, b);
+                    const float2 bb = __ffma2_rn(h, m1, s2);
+                    const float2 e = __fadd2_rn(__ffma2_rn(__ffma2_rn(bb, m1, s2), m1, h), __ffma2_rn(bb, m1, b));
+                    const float2 l = __fadd2_rn(make_float2(lo[q][r].re, lo[q][r].im), e);
+                    hi[q][r].re = s2.x;
+                    hi[q][r].im = s2.y;
+                    lo[q][r].re = l.x;
+                    lo[q][r].im = l.y;
+                } else if constexpr (COMP) {
                     twoSumAdd(hi[q][r].re, lo[q][r].re, sign * cur.re);
                     if constexpr (C) twoSumAdd(hi[q][r].im, lo[q][r].im, sign * cur.im);
                 } else {
@@ -403,6 +420,111 @@ __device__ __forceinline__ MvOut<T> solveRegs(GE* Gs, int GP, int L, int sz, T l
     res.y.re = zw.re * scale;
     res.y.im = zw.im * scale;
     res.cond = gmin > T(0) ? (gmax / gmin) * (gmax / gmin) : T(INFINITY);
+    return res;
+}
+
+// The Cholesky and forward substitutions of solveRegs for complex data with one row per lane (L <= 32),
+// the loaded matrix kept in two planes of floats (real parts at re, imaginary parts at im, row pitch
+// GP). The inner products of column j run over pairs of columns (k, k + 1) in packed FMAs: each lane
+// keeps its row of G negated, in pairs, so that every product is a natural packed operand:
+//   re(A - sum g conj(b)) = A.re + sum (-g.re) b.re + sum (-g.im) b.im
+//   im(A - sum g conj(b)) = (A.im + sum (-g.im) b.re) - sum (-g.re) b.im
+// with b = G[j][k] read from the planes as pairs of floats.
+__device__ __forceinline__ MvOut<float> solveRegsCplx(float* Gre, float* Gim, int GP, int L, int sz, float loading,
+                                                      int lane, const V<float> (&xbar)[1], float power, int K) {
+    float2 nr[16], ni[16];  // -G[lane][2m], -G[lane][2m + 1]: real and imaginary parts
+    MvOut<float> res;
+    res.ok = true;
+    res.y = vz<true, float>();
+    float gmin = INFINITY, gmax = 0.0f;
+    V<float> az = vz<true, float>(), aw = xbar[0], zf = vz<true, float>(), wf = vz<true, float>();
+    az.re = 1.0f;
+    const int i = lane;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        if (j >= L) break;
+        float are = 0.0f, aim = 0.0f;
+        if (i < sz && j < sz) {
+            are = Gre[i * GP + j];
+            aim = Gim[i * GP + j];
+        }
+        if (i == j) are += loading;
+        float2 accR = make_float2(are, 0.0f), accIp = make_float2(aim, 0.0f), accIn = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int k = 0; k + 1 < j; k += 2) {
+            // entries (j, k) and (j, k + 1): rows have an even pitch, so each plane's pair is aligned
+            const float2 bR = *reinterpret_cast<const float2*>(&Gre[j * GP + k]);
+            const float2 bI = *reinterpret_cast<const float2*>(&Gim[j * GP + k]);
+            accR = __ffma2_rn(nr[k / 2], bR, accR);
+            accR = __ffma2_rn(ni[k / 2], bI, accR);
+            accIp = __ffma2_rn(ni[k / 2], bR, accIp);
+            accIn = __ffma2_rn(nr[k / 2], bI, accIn);
+        }
+        if (j & 1) {
+            const float bre = Gre[j * GP + j - 1], bim = Gim[j * GP + j - 1];
+            accR.x = fmaf(nr[(j - 1) / 2].x, bre, accR.x);
+            accR.x = fmaf(ni[(j - 1) / 2].x, bim, accR.x);
+            accIp.x = fmaf(ni[(j - 1) / 2].x, bre, accIp.x);
+            accIn.x = fmaf(nr[(j - 1) / 2].x, bim, accIn.x);
+        }
+        const float accRe = accR.x + accR.y;
+        const float accIm = (accIp.x + accIp.y) - (accIn.x + accIn.y);
+        const float djj = __shfl_sync(kFull, accRe, j & 31);
+        if (!(djj > 0.0f)) {  // warp-uniform: the factorisation broke down
+            res.ok = false;
+            return res;
+        }
+        const float inv = rsqrtf(djj);  // MUFU reciprocal square root (about 2 ulp)
+        const float gjj = djj * inv;
+        float vre = 0.0f, vim = 0.0f;
+        if (i > j) {
+            vre = accRe * inv;
+            vim = accIm * inv;
+        } else if (i == j) {
+            vre = gjj;
+        }
+        if (j & 1) {
+            nr[j / 2].y = -vre;
+            ni[j / 2].y = -vim;
+        } else {
+            nr[j / 2].x = -vre;
+            ni[j / 2].x = -vim;
+        }
+        if (i < L) {
+            Gre[i * GP + j] = vre;
+            Gim[i * GP + j] = vim;
+        }
+        __syncwarp();
+        if (j < sz) {
+            gmin = fminf(gmin, gjj);
+            gmax = fmaxf(gmax, gjj);
+            V<float> zk = shflV<true, float>(az, j & 31);
+            V<float> wk = shflV<true, float>(aw, j & 31);
+            zk.re *= inv;
+            zk.im *= inv;
+            wk.re *= inv;
+            wk.im *= inv;
+            if (i == j) {
+                zf = zk;
+                wf = wk;
+            }
+            if (i > j) {
+                const V<float> g{vre, vim};
+                msc<true, float>(az, g, zk);
+                msc<true, float>(aw, g, wk);
+            }
+        }
+    }
+    float zz = zf.re * zf.re + zf.im * zf.im;
+    V<float> zw = vz<true, float>();
+    macConj<true, float>(zw, wf, zf);
+    zz = warpSum(zz);
+    zw.re = warpSum(zw.re);
+    zw.im = warpSum(zw.im);
+    const float scale = 1.0f / (zz * pow(static_cast<float>(K), power));
+    res.y.re = zw.re * scale;
+    res.y.im = zw.im * scale;
+    res.cond = gmin > 0.0f ? (gmax / gmin) * (gmax / gmin) : INFINITY;
     return res;
 }
 
@@ -831,9 +953,13 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
                     if (r >= L) break;
                     int c = r + d;
                     if (c >= L) c -= L;
-                    Elem<C>& e = Gs[r * L_::GP + c];
-                    e.re = hi[q][r].re + lo[q][r].re;
-                    if constexpr (C) e.im = hi[q][r].im + lo[q][r].im;
+                    if constexpr (C) {  // complex: real and imaginary planes
+                        float* pl = reinterpret_cast<float*>(Gs);
+                        pl[r * L_::GP + c] = hi[q][r].re + lo[q][r].re;
+                        pl[L_::GR * L_::GP + r * L_::GP + c] = hi[q][r].im + lo[q][r].im;
+                    } else {
+                        Gs[r * L_::GP + c].re = hi[q][r].re + lo[q][r].re;
+                    }
                 }
             }
         }
@@ -845,7 +971,7 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
 #pragma unroll
         for (int q = 0; q < NR; q++) {
             const int i = lane + 32 * q;
-            if (i < ms.sz) tr += Gs[i * L_::GP + i].re;
+            if (i < ms.sz) tr += C ? reinterpret_cast<const float*>(Gs)[i * L_::GP + i] : Gs[i * L_::GP + i].re;
         }
         tr = warpSum(tr);
         const float loading = (1.0f / static_cast<float>(ms.sz)) * tr * a.loadScale;
@@ -882,8 +1008,13 @@ __global__ void __launch_bounds__(32 * kMvMaxWarps, 1) mvKernel(MvArgs a) {
                                                   a.pcgThr).y;
             }
         } else if (tr > 0.0f && isfinite(tr)) {
-            const MvOut<float> r =
-                solveRegs<C, NR, float, Elem<C>>(Gs, L_::GP, L, ms.sz, loading, lane, xbar, a.power, ms.K);
+            MvOut<float> r;
+            if constexpr (C && NR == 1) {
+                float* pl = reinterpret_cast<float*>(Gs);
+                r = solveRegsCplx(pl, pl + L_::GR * L_::GP, L_::GP, L, ms.sz, loading, lane, xbar, a.power, ms.K);
+            } else {
+                r = solveRegs<C, NR, float, Elem<C>>(Gs, L_::GP, L, ms.sz, loading, lane, xbar, a.power, ms.K);
+            }
             const float cond = r.ok ? r.cond : INFINITY;
             condMax = fmaxf(condMax, fminf(cond, FLT_MAX));
             if (a.thr > 0.0f && (!r.ok || cond > a.thr)) {

@@ -157,6 +157,15 @@ class SmoothModelTorch:
         self.xe_mm = torch.tensor(geom.element_x.astype(np.float64), device=device)
         self.d_mm = torch.tensor(geom.depths.astype(np.float64), device=device)
 
+    def weight_ratio(self):
+        """Sum of the aperture's window weights over the number of aperture elements, per pixel:
+        [num_depths][num_rx] (0 for an empty aperture). The normalisation n / D amplifies every term
+        of a pixel whose ratio is small."""
+        import torch
+        den = self.w.sum(dim=2)
+        r = torch.where(self.count > 0, den / torch.clamp(self.count, min=1.0), torch.zeros_like(den))
+        return r.T.contiguous()
+
     def tau_range(self, c_mm_s):
         """(smallest, largest) delay in samples over each pixel's aperture elements at c:
         [num_depths][num_rx] each (+inf / -inf for an empty aperture)."""
@@ -169,10 +178,12 @@ class SmoothModelTorch:
         hi = torch.where(self.member, tau, -inf).amax(dim=2)
         return lo.T.contiguous(), hi.T.contiguous()
 
-    def forward(self, rf, c_mm_s, apod=None):
+    def forward(self, rf, c_mm_s, apod=None, cells_of=None):
         """rf [num_tx][num_channels][num_samples] (torch, any float type, on the model's device) ->
         FP64 image [num_depths][num_rx] (0 where no element is in the aperture, NaN where the weights
-        of the aperture's elements sum to 0)."""
+        of the aperture's elements sum to 0). cells_of: a speed of sound whose sample cells (the
+        interpolation's index i = floor(tau)) are kept for every term, so that each term is linear in
+        tau and the image is smooth in c; its derivative at c = cells_of is the forward's."""
         import torch
         g = self.geom
         nS = g.num_samples
@@ -181,7 +192,10 @@ class SmoothModelTorch:
         lat = self.xe_mm[self.e][:, None, :] - (self.px[:, None, None] + self.dirx[:, None, None] * self.d_mm[None, :, None])
         path = torch.hypot(lat, (self.diry[:, None] * self.d_mm[None, :])[:, :, None]) + self.d_mm[None, :, None]
         tau = self.t0[:, None, None] + path / (c_mm_s * self.dt)
-        i = torch.floor(tau)
+        if cells_of is None:
+            i = torch.floor(tau)
+        else:
+            i = torch.floor(self.t0[:, None, None] + path / (cells_of * self.dt))
         fr = tau - i
         i = i.long()
         ok = (i >= 0) & (i < nS - 1)
