@@ -369,6 +369,22 @@ def reference_gpu_rows(res):
     g0, rf0 = synth.c0_frame(0, device="cpu")
     x0 = np.ascontiguousarray(rf0.numpy())
     gc = geo(g0)
+    # the library's MV timings first: the reference's container pool frees buffers from a background
+    # thread (cudaFree synchronises the device), which would stall launches timed after its calls
+    from supra_b200.api import RxBeamformer, mv_beamform_pcg
+    raw = RxBeamformer(g0).raw_delay(rf0.cuda(), 1.0, window_type=1)
+    raw[~(raw.abs() < 1e30)] = 0.0
+    raw = raw[:, :, :2000].contiguous()
+    rh = np.ascontiguousarray(raw.cpu().numpy())
+    ours_mv = _event_ms(lambda: mv_beamform(raw, 32, 5, 1.5, False, 1.0, 1e6, with_stats=False), 5, warm=2)
+    ours_pcg = _event_ms(lambda: mv_beamform_pcg(raw, 32, 5, convergence_threshold=1e-4), 5, warm=2)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    big = torch.randn((16384, 2048), generator=gen, device="cuda") * 1000.0  # 128 MB, above L2
+    hil = HilbertFirEnvelope(65)
+    ours_hil = _graph_ms(lambda: hil.demodulate(big), 10)
+    hb = np.ascontiguousarray(big.cpu().numpy())
+    del big
     ms = lib.refg_time_das(C.byref(gc), C.c_void_p(x0.ctypes.data), C.c_double(1.0),
                            C.c_double(g0.speed_of_sound_mm_s), 1, 0, C.c_double(g0.depth_mm), 20)
     row("das_c0", ms, res.get("das_c0", {}).get("ms"), "2D DAS, c0 frame (128 lines x 2048 depths, int16 in)")
@@ -387,14 +403,8 @@ def reference_gpu_rows(res):
     row("das3d_c2", ms, res.get("das3d_c2", {}).get("ms"), "3D DAS, c2 volume (32 x 32 lines x 1024 depths)")
     del x2
     # envelope chain on a 16384 x 2048 float image (128 MB, above L2)
-    gen = torch.Generator(device="cuda")
-    gen.manual_seed(7)
-    big = torch.randn((16384, 2048), generator=gen, device="cuda") * 1000.0
-    hb = np.ascontiguousarray(big.cpu().numpy())
     ms = lib.refg_time_hilbert(C.c_void_p(hb.ctypes.data), C.c_uint32(2048), C.c_uint32(16384), C.c_uint32(65), 10)
-    hil = HilbertFirEnvelope(65)
-    row("hilbert_env_large_65taps", ms, _graph_ms(lambda: hil.demodulate(big), 10),
-        "Hilbert FIR envelope, 65 taps, 16384 x 2048 float image")
+    row("hilbert_env_large_65taps", ms, ours_hil, "Hilbert FIR envelope, 65 taps, 16384 x 2048 float image")
     f = np.array([7e6]), np.array([1e6]), np.array([1.0])
     fa = [np.ascontiguousarray(v, np.float64) for v in f]
     ms = lib.refg_time_iq(C.c_void_p(hb.ctypes.data), C.c_uint32(2048), C.c_uint32(16384), C.c_double(40e6),
@@ -406,7 +416,7 @@ def reference_gpu_rows(res):
                                    C.c_double(1.0), C.c_double(4000.0), 10)
     row("logcompress_large", ms, res.get("logcompress_large", {}).get("ms"),
         "log compression to uint8, 16384 x 2048 float image")
-    del big, hb
+    del hb
     # scan conversion of the c0 envelope at 0.1 mm
     img0 = np.abs(np.random.Generator(np.random.PCG64(3)).standard_normal((g0.num_depths, g0.num_rx))).astype(np.float32)
     rs = O.RefScan(g0.scanlines, g0.rx_layout, g0.num_depths, g0.depth_mm, 0.1, lib=lib)
@@ -422,20 +432,12 @@ def reference_gpu_rows(res):
     del t
     # minimum variance on the c0 frame's raw-delayed data (real), 2000 depths (the reference's MV
     # handles at most 2000 samples), L 32, +-5; the library with the reference's loading trace/L
-    from supra_b200.api import RxBeamformer
-    raw = RxBeamformer(g0).raw_delay(rf0.cuda(), 1.0, window_type=1)
-    raw[~(raw.abs() < 1e30)] = 0.0
-    raw = raw[:, :, :2000].contiguous()
-    rh = np.ascontiguousarray(raw.cpu().numpy())
     ms = lib.refg_time_mv(C.c_void_p(rh.ctypes.data), C.c_uint32(128), C.c_uint32(64), C.c_uint32(2000), C.c_uint32(32),
                           C.c_uint32(5), C.c_double(1.5), 1)
-    ours = _event_ms(lambda: mv_beamform(raw, 32, 5, 1.5, False, 1.0, 1e6, with_stats=False), 5, warm=2)
-    row("mv_c0_2000", ms, ours, "MV (real, loading trace/L), c0 raw-delayed 128 lines x 64 channels x 2000 depths, L 32, +-5")
+    row("mv_c0_2000", ms, ours_mv, "MV (real, loading trace/L), c0 raw-delayed 128 lines x 64 channels x 2000 depths, L 32, +-5")
     ms = lib.refg_time_mvpcg(C.c_void_p(rh.ctypes.data), C.c_uint32(128), C.c_uint32(64), C.c_uint32(2000),
                              C.c_uint32(32), C.c_uint32(5), C.c_double(1e-4), C.c_double(1.5), 2)
-    from supra_b200.api import mv_beamform_pcg
-    ours = _event_ms(lambda: mv_beamform_pcg(raw, 32, 5, convergence_threshold=1e-4), 5, warm=2)
-    row("mv_pcg_c0_2000", ms, ours, "MV-PCG (convergence threshold 1e-4, the node's default), same input")
+    row("mv_pcg_c0_2000", ms, ours_pcg, "MV-PCG (convergence threshold 1e-4, the node's default), same input")
     return out
 
 
