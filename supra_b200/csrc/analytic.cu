@@ -15,6 +15,11 @@
 // range of each output tile is split over the 8 CTAs of a thread-block cluster (CTA r sums chunks
 // r, r + 8, ...); rank 0 adds the 8 partial tiles from distributed shared memory in rank order (a
 // deterministic reduction, no scratch memory) and writes the envelope.
+// Power-of-two lengths (64 .. 16384) take an FFT path instead: a CTA packs two real scanlines x, y as
+// z = x + i y, transforms z in shared memory (radix-2, decimation in time from a bit-reversed load),
+// multiplies by -i sgn(k) (DC and Nyquist bins zeroed) and transforms back (decimation in frequency,
+// bit-reversed result): since the Hilbert transform is linear and real for real input, the result
+// over N is h_x + i h_y. O(N log N) instead of the circulant product's 2 N^2 flops per scanline.
 #include <cooperative_groups.h>
 
 #include <cmath>
@@ -25,7 +30,8 @@
 
 struct sb_analytic_plan {
     uint32_t n = 0;
-    float* dK = nullptr;  // k[0..N)
+    float* dK = nullptr;    // k[0..N)
+    float2* dTw = nullptr;  // exp(-2 pi i j / N), j < N / 2 (power-of-two N only)
 };
 
 namespace sb {
@@ -35,6 +41,10 @@ constexpr int kAT = 32;   // samples and scanlines per CTA tile, and samples per
 constexpr int kAThreads = 64;
 
 constexpr int kASplit = 8;  // CTAs per cluster sharing one output tile
+
+// Lengths of the FFT path: powers of two from 64 to 16384 (the transform and its twiddles, 12 N bytes,
+// fit a CTA's shared memory).
+inline bool fftLength(uint32_t N) { return N >= 64 && N <= 16384 && (N & (N - 1)) == 0; }
 
 __device__ __forceinline__ float4 load4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ float4 load4(const int16_t* p) {
@@ -196,6 +206,77 @@ __global__ void __launch_bounds__(kAThreads) analyticEnvKernel(const IN* __restr
     analyticStore<IN, OUT>(in, out, N, nL, n0, l0, tot);
 }
 
+constexpr int kFftThreads = 256;
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+template <typename T> __device__ __forceinline__ float ldf(const T* p) { return static_cast<float>(__ldg(p)); }
+
+// Envelopes of scanlines (2 b, 2 b + 1) of a [N][nL] image by FFT (N = 2^logN): see the file comment.
+template <typename IN, typename OUT>
+__global__ void __launch_bounds__(kFftThreads) analyticFftKernel(const IN* __restrict__ in, OUT* __restrict__ out,
+                                                                 const float2* __restrict__ tw, int N, int logN, int nL) {
+    extern __shared__ float2 fsm[];
+    float2* z = fsm;       // N values
+    float2* w = fsm + N;   // N / 2 twiddles
+    const int tid = threadIdx.x;
+    const int l = 2 * static_cast<int>(blockIdx.x);
+    const bool two = l + 1 < nL;
+    const int half = N >> 1;
+    for (int j = tid; j < half; j += kFftThreads) w[j] = __ldg(tw + j);
+    for (int n = tid; n < N; n += kFftThreads) {
+        const size_t base = static_cast<size_t>(n) * nL + l;
+        const float x = ldf(in + base), y = two ? ldf(in + base + 1) : 0.0f;
+        z[__brev(static_cast<uint32_t>(n)) >> (32 - logN)] = make_float2(x, y);
+    }
+    __syncthreads();
+    // forward transform, decimation in time: stage s joins blocks of 2^(s-1) with exp(-2 pi i j / 2^s)
+    for (int s = 1; s <= logN; s++) {
+        const int h = 1 << (s - 1), stride = N >> s;
+        for (int b = tid; b < half; b += kFftThreads) {
+            const int j = b & (h - 1);
+            const int i0 = ((b >> (s - 1)) << s) + j, i1 = i0 + h;
+            const float2 t = cmulf(w[j * stride], z[i1]);
+            const float2 a = z[i0];
+            z[i0] = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
+            z[i1] = make_float2(__fsub_rn(a.x, t.x), __fsub_rn(a.y, t.y));
+        }
+        __syncthreads();
+    }
+    // times -i sgn(k): positive frequencies (1 .. N/2 - 1) (re, im) -> (im, -re), negative ones
+    // (N/2 + 1 .. N - 1) -> (-im, re), DC and Nyquist -> 0
+    for (int k = tid; k < N; k += kFftThreads) {
+        const float2 v = z[k];
+        z[k] = (k == 0 || k == half) ? make_float2(0.0f, 0.0f) : (k < half ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x));
+    }
+    __syncthreads();
+    // inverse transform, decimation in frequency: stage s splits blocks of 2^s with exp(+2 pi i j / 2^s)
+    for (int s = logN; s >= 1; s--) {
+        const int h = 1 << (s - 1), stride = N >> s;
+        for (int b = tid; b < half; b += kFftThreads) {
+            const int j = b & (h - 1);
+            const int i0 = ((b >> (s - 1)) << s) + j, i1 = i0 + h;
+            const float2 a = z[i0], c = z[i1];
+            const float2 wj = w[j * stride];
+            z[i0] = make_float2(__fadd_rn(a.x, c.x), __fadd_rn(a.y, c.y));
+            z[i1] = cmulf(make_float2(__fsub_rn(a.x, c.x), __fsub_rn(a.y, c.y)), make_float2(wj.x, -wj.y));
+        }
+        __syncthreads();
+    }
+    const float invN = __fdiv_rn(1.0f, static_cast<float>(N));
+    for (int n = tid; n < N; n += kFftThreads) {
+        const float2 hv = z[__brev(static_cast<uint32_t>(n)) >> (32 - logN)];
+        const size_t base = static_cast<size_t>(n) * nL + l;
+        const float x = ldf(in + base), hx = __fmul_rn(hv.x, invN);
+        out[base] = clampCast<OUT>(__fsqrt_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(hx, hx))));
+        if (two) {
+            const float y = ldf(in + base + 1), hy = __fmul_rn(hv.y, invN);
+            out[base + 1] = clampCast<OUT>(__fsqrt_rn(__fadd_rn(__fmul_rn(y, y), __fmul_rn(hy, hy))));
+        }
+    }
+}
+
 }  // namespace
 }  // namespace sb
 
@@ -222,8 +303,18 @@ int sb_analytic_plan_create(uint32_t num_samples, sb_analytic_plan** out) {
     p->n = N;
     cudaError_t e = cudaMalloc(&p->dK, N * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpy(p->dK, k.data(), N * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && fftLength(N)) {
+        std::vector<float2> tw(N / 2);
+        for (uint32_t j = 0; j < N / 2; j++) {
+            const double a = 2.0 * pi * static_cast<double>(j) / N;
+            tw[j] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(-std::sin(a)));
+        }
+        e = cudaMalloc(&p->dTw, (N / 2) * sizeof(float2));
+        if (e == cudaSuccess) e = cudaMemcpy(p->dTw, tw.data(), (N / 2) * sizeof(float2), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) {
         cudaFree(p->dK);
+        cudaFree(p->dTw);
         delete p;
         return cudaFail(e, "sb_analytic_plan_create");
     }
@@ -234,6 +325,7 @@ int sb_analytic_plan_create(uint32_t num_samples, sb_analytic_plan** out) {
 int sb_analytic_plan_destroy(sb_analytic_plan* p) {
     if (p) {
         cudaFree(p->dK);
+        cudaFree(p->dTw);
         delete p;
     }
     return SB_OK;
@@ -247,6 +339,27 @@ int sb_analytic_env_run(const sb_analytic_plan* p, const void* in, int in_dtype,
                out_dtype);
     if (num_scanlines == 0) return SB_OK;
     const int N = static_cast<int>(p->n), nL = static_cast<int>(num_scanlines);
+    if (p->dTw) {  // power-of-two length: the FFT path
+        int logN = 0;
+        while ((1 << logN) < N) logN++;
+        const size_t shm = static_cast<size_t>(N) * sizeof(float2) + static_cast<size_t>(N / 2) * sizeof(float2);
+        const unsigned grid = static_cast<unsigned>((nL + 1) / 2);
+        cudaStream_t stf = S(stream);
+#define SB_AF(IT, OT)                                                                                                  \
+    do {                                                                                                               \
+        SB_CUDA(cudaFuncSetAttribute(analyticFftKernel<IT, OT>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                                     static_cast<int>(shm)));                                                          \
+        analyticFftKernel<IT, OT><<<grid, kFftThreads, shm, stf>>>(static_cast<const IT*>(in), static_cast<OT*>(out),  \
+                                                                   p->dTw, N, logN, nL);                              \
+    } while (0)
+        if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_AF(int16_t, float);
+        else if (in_dtype == SB_INT16) SB_AF(int16_t, int16_t);
+        else if (out_dtype == SB_FLOAT32) SB_AF(float, float);
+        else SB_AF(float, int16_t);
+#undef SB_AF
+        SB_CHECK_LAUNCH("analyticFftKernel");
+        return SB_OK;
+    }
     dim3 grid((nL + kAT - 1) / kAT, (N + kAT - 1) / kAT);
     SB_REQUIRE(grid.y <= 65535u, "sb_analytic_env_run: %d samples exceed the grid", N);
     cudaStream_t st = S(stream);
