@@ -241,10 +241,12 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
         G g = geom(j0, true);
         for (int j = j0; j < j1; j++) {
             int16_t a[K], b[K];
+            const uint32_t o2 = g.off << 1;  // byte offset in the transmit's rows (< 4 GB)
 #pragma unroll
             for (int f = 0; f < K; f++) {
-                a[f] = __ldg(tb[f] + g.off);
-                b[f] = __ldg(tb[f] + g.off + 1);
+                const char* pb = reinterpret_cast<const char*>(tb[f]) + o2;
+                a[f] = __ldg(reinterpret_cast<const int16_t*>(pb));
+                b[f] = __ldg(reinterpret_cast<const int16_t*>(pb + 2));
             }
             if (j + kPrefetchAhead < j1) {
                 // row offset of element j + kPrefetchAhead plus element j's sample index (< nS - 1):
@@ -252,7 +254,8 @@ __device__ __forceinline__ void packDepthPipelined(const ElemRec* el, int j0, in
                 const uint32_t offp = static_cast<uint32_t>(el[j + kPrefetchAhead].ch) +
                                       (g.off - static_cast<uint32_t>(el[j].ch));
 #pragma unroll
-                for (int f = 0; f < K; f++) asm volatile("prefetch.global.L2 [%0];" ::"l"(tb[f] + offp));
+                for (int f = 0; f < K; f++)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char*>(tb[f]) + (offp << 1)));
             }
             const G gn = geom(min(j + 1, j1 - 1), j + 1 < j1);
             const float2 wA2 = make_float2(g.wA, g.wA), wB2 = make_float2(g.wB, g.wB);
@@ -488,8 +491,15 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         const bool dx2 = dx2Line != 0;
         const int16_t* tb[FP];
 #pragma unroll
-        for (int f = 0; f < FP; f++)
-            tb[f] = P.rf[f < nf ? f : 0] + static_cast<size_t>(s.txIdx) * P.nCh * P.nS;
+        for (int f = 0; f < FP; f++) {
+            // The same for every thread of the CTA; passing it through a warp reduction makes that
+            // visible to the compiler, which then keeps the frame bases in uniform registers (one
+            // fewer 64-bit register pair per frame in the gather loops: -1.7% on a 64-frame batch).
+            const uint64_t u = reinterpret_cast<uint64_t>(P.rf[f < nf ? f : 0] + static_cast<size_t>(s.txIdx) * P.nCh * P.nS);
+            const uint32_t lo = __reduce_max_sync(0xffffffffu, static_cast<uint32_t>(u));
+            const uint32_t hi = __reduce_max_sync(0xffffffffu, static_cast<uint32_t>(u >> 32));
+            tb[f] = reinterpret_cast<const int16_t*>((static_cast<uint64_t>(hi) << 32) | lo);
+        }
         const int nD = static_cast<int>(P.nD);
         const int rStart = MODE == 1 ? static_cast<int>(pi.seg0) : max(0, static_cast<int>(pi.seg0) - a.half);
         const int rEnd = MODE == 1 ? min(nD, static_cast<int>(pi.seg1)) : min(nD, static_cast<int>(pi.seg1) + a.half + 1);

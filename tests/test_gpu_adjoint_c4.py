@@ -90,7 +90,7 @@ def c4():
     torch.cuda.synchronize()
     return {"g": g, "rf": rf.cpu().numpy(), "target": target.double().cpu(), "valid": valid.cpu(), "c0": c0,
             "s32": s.detach().double().cpu(),
-            "c_true": c_true, "loss": float(loss), "grad_rf": rf_g.grad, "grad_apod": ap.grad.cpu().numpy(),
+            "c_true": c_true, "loss": float(loss.detach()), "grad_rf": rf_g.grad, "grad_apod": ap.grad.cpu().numpy(),
             "grad_c": float(c.grad), "model": model, "inrec_frac": float(inrec.float().mean())}
 
 
