@@ -358,6 +358,101 @@ __global__ void __launch_bounds__(256) iqMagnitudeKernel(const IN* __restrict__ 
     }
 }
 
+// One reference frequency (the common case): the filter-bank stage of sample s is
+// scale w0 sqrt((x cI)^2 + (x cQ)^2) with mixer values cI, cQ that depend on s only, i.e. |x| G(s) with
+// G(s) = scale w0 sqrt(cI^2 + cQ^2) (equal up to the rounding of the products, ~1e-7 relative).
+// A CTA of 32 scanlines x 64 decimated outputs forms cI, cQ and G once per input row and |x| G per
+// sample (no halo recomputation of the mixer), then each thread sums 8 outputs of one scanline, one
+// shared tap value per step for all 8 (fused multiply-adds, as nvcc contracts the reference's
+// `accumulator += sample * filterElement` in its default build). A sample with |x| >= 2^63 or not finite, whose squares may overflow, takes the
+// reference's expression (so clamped +-FLT_MAX pixels give the same infinities). Samples outside the
+// record are staged as 0: their terms leave the sums unchanged, as the reference skips them.
+constexpr int IQ1_OT = 64;
+constexpr int IQ1_R = 8;  // outputs per thread (256 threads = 32 scanlines x 8 groups of 8 outputs)
+
+template <typename IN, typename OUT>
+__global__ void __launch_bounds__(256) iqMagnitude1Kernel(const IN* __restrict__ in, OUT* __restrict__ out, IqArgs a) {
+    extern __shared__ float sm[];
+    __shared__ float lps[kIqMaxTaps + 1];
+    const int rows = (IQ1_OT - 1) * a.stride + a.lpN + 1;
+    float* band = sm;                     // [rows][IQ_LINES]
+    float* gain = sm + rows * IQ_LINES;   // [rows]
+    float2* mix = reinterpret_cast<float2*>(gain + rows + (rows & 1));  // [rows] (cI, cQ), 8-byte aligned
+    const int l0 = blockIdx.x * IQ_LINES;
+    const int so0 = blockIdx.y * IQ1_OT;
+    const int sIn0 = so0 * a.stride - a.lpN / 2;
+    const int tid = threadIdx.x;
+    for (int r = tid; r < rows; r += blockDim.x) {
+        const int s = sIn0 + r;
+        float gv = 0.0f, cI = 0.0f, cQ = 0.0f;
+        if (s >= 0 && s < a.nS) {
+            const float ph = __fmul_rn(static_cast<float>(s), a.fOverFs[0]);
+            float phI = __fadd_rn(ph, 0.0f);
+            float phQ = __fadd_rn(ph, 0.75f);
+            phI = __fsub_rn(phI, truncf(phI));
+            phQ = __fsub_rn(phQ, truncf(phQ));
+            cI = mixCos(phI);
+            cQ = mixCos(phQ);
+            gv = __fmul_rn(a.scale, __fmul_rn(a.weights[0], __fsqrt_rn(__fadd_rn(__fmul_rn(cI, cI), __fmul_rn(cQ, cQ)))));
+        }
+        gain[r] = gv;
+        mix[r] = make_float2(cI, cQ);
+    }
+    for (int j = tid; j <= a.lpN; j += blockDim.x) lps[j] = a.lp[j];
+    __syncthreads();
+    // the tile's samples, eight loads in flight per thread before any is used
+    const int total = rows * IQ_LINES;
+    constexpr int kU = 8;
+    for (int base = tid; base < total; base += 256 * kU) {
+        float xs[kU];
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int idx = base + u * 256;
+            const int s = sIn0 + idx / IQ_LINES, l = l0 + idx % IQ_LINES;
+            const bool ok = idx < total && l < a.nL && s >= 0 && s < a.nS;
+            xs[u] = ok ? toFloat(in[l + static_cast<size_t>(ok ? s : 0) * a.nL]) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int idx = base + u * 256;
+            if (idx < total) {
+                const int row = idx / IQ_LINES;
+                const float x = xs[u];  // 0 outside the record and the image
+                float v;
+                if (fabsf(x) < 9.22337204e18f) {  // 2^63: x^2 stays finite
+                    v = __fmul_rn(fabsf(x), gain[row]);
+                } else {
+                    const float2 c = mix[row];
+                    const float dI = __fmul_rn(x, c.x), dQ = __fmul_rn(x, c.y);
+                    v = __fmul_rn(a.scale, __fmul_rn(a.weights[0], __fsqrt_rn(__fadd_rn(__fmul_rn(dI, dI), __fmul_rn(dQ, dQ)))));
+                }
+                band[idx] = v;
+            }
+        }
+    }
+    __syncthreads();
+    const int li = tid % IQ_LINES, o0 = (tid / IQ_LINES) * IQ1_R;
+    const float* b = band + o0 * a.stride * IQ_LINES + li;
+    const int step = a.stride * IQ_LINES;
+    const int nTaps = 2 * (a.lpN / 2) + 1;  // the reference's window [si - lpN/2, si + lpN/2]
+    float acc[IQ1_R];
+#pragma unroll
+    for (int k = 0; k < IQ1_R; k++) acc[k] = 0.0f;
+#pragma unroll 2
+    for (int j = 0; j < nTaps; j++) {
+        const float t = lps[j];
+        const float* bj = b + j * IQ_LINES;
+#pragma unroll
+        for (int k = 0; k < IQ1_R; k++) acc[k] = fmaf(bj[k * step], t, acc[k]);
+    }
+    const int l = l0 + li;
+#pragma unroll
+    for (int k = 0; k < IQ1_R; k++) {
+        const int so = so0 + o0 + k;
+        if (so < a.nOut && l < a.nL) out[l + static_cast<size_t>(so) * a.nL] = clampCast<OUT>(acc[k]);
+    }
+}
+
 // ----------------------------------------------------------------------------- complex IQ
 template <typename IN>
 __global__ void __launch_bounds__(256) iqComplexKernel(const IN* __restrict__ in, float2* __restrict__ out,
@@ -631,10 +726,30 @@ int sb_iq_magnitude_run(const sb_iq_plan* p, const void* in, int in_dtype, void*
     a.stride = static_cast<int>(std::max(decimation, 1u));
     a.nOut = decimation > 1 ? a.nS / static_cast<int>(decimation) : a.nS;
     if (a.nOut == 0) return SB_OK;
+    cudaStream_t st = S(stream);
+    const int rows1 = (IQ1_OT - 1) * a.stride + a.lpN + 1;
+    const size_t shm1 = (static_cast<size_t>(rows1) * (IQ_LINES + 1) + (rows1 & 1) + 2 * static_cast<size_t>(rows1)) * sizeof(float);
+    if (a.numFilters == 1 && shm1 <= 100 * 1024) {
+        dim3 grid1((a.nL + IQ_LINES - 1) / IQ_LINES, (a.nOut + IQ1_OT - 1) / IQ1_OT);
+        SB_REQUIRE(grid1.y <= 65535u, "sb_iq_magnitude_run: %d outputs exceed the grid", a.nOut);
+#define SB_IQ1(INT, OUTT)                                                                                         \
+    do {                                                                                                          \
+        SB_CUDA(cudaFuncSetAttribute(iqMagnitude1Kernel<INT, OUTT>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                     static_cast<int>(shm1)));                                                    \
+        iqMagnitude1Kernel<INT, OUTT><<<grid1, 256, shm1, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), a); \
+        SB_CHECK_LAUNCH("iqMagnitude1Kernel");                                                                    \
+        return SB_OK;                                                                                             \
+    } while (0)
+        if (in_dtype == SB_FLOAT32 && out_dtype == SB_FLOAT32) SB_IQ1(float, float);
+        if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_IQ1(int16_t, float);
+        if (in_dtype == SB_FLOAT32 && out_dtype == SB_INT16) SB_IQ1(float, int16_t);
+        if (in_dtype == SB_INT16 && out_dtype == SB_INT16) SB_IQ1(int16_t, int16_t);
+#undef SB_IQ1
+        return fail(SB_ERR_UNSUPPORTED, "sb_iq_magnitude_run: %d -> %d unsupported", in_dtype, out_dtype);
+    }
     const int rows = (IQ_OT - 1) * a.stride + a.lpN + 1;
     size_t shm = static_cast<size_t>(rows) * IQ_LINES * sizeof(float);
     SB_REQUIRE(shm <= 200 * 1024, "sb_iq_magnitude_run: decimation %u too large", decimation);
-    cudaStream_t st = S(stream);
     dim3 grid((a.nL + IQ_LINES - 1) / IQ_LINES, (a.nOut + IQ_OT - 1) / IQ_OT);
 #define SB_IQM(INT, OUTT)                                                                                      \
     do {                                                                                                       \
