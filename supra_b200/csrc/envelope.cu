@@ -453,6 +453,113 @@ __global__ void __launch_bounds__(256) iqMagnitude1Kernel(const IN* __restrict__
     }
 }
 
+// Several reference frequencies (frequency compounding): a CTA of 32 scanlines x 32 decimated outputs
+// stages its raw samples (band-pass and low-pass halos included, eight loads in flight per thread)
+// and the filter bank in shared memory, forms each filter's mixer values once per input row, then
+// evaluates the filter-bank magnitude per sample from shared memory in the reference's operation
+// order (IQDemodulator.cu:68-137: band-pass sums by separately rounded products and additions, the
+// weighted magnitudes summed over the filters in order), and the decimating low-pass as in
+// iqMagnitude1Kernel (four outputs per thread).
+constexpr int IQB_OT = 32;
+constexpr int IQB_R = 4;
+
+template <typename IN, typename OUT, int NF>
+__global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restrict__ in, OUT* __restrict__ out, IqArgs a) {
+    extern __shared__ float sm[];
+    __shared__ float lps[kIqMaxTaps + 1];
+    __shared__ float bank[8 * (kIqMaxTaps + 1)];
+    const int rows = (IQB_OT - 1) * a.stride + a.lpN + 1;  // band rows
+    const int hb = a.bpN / 2;
+    const int rowsX = rows + 2 * hb;                        // raw rows
+    constexpr int nf = NF;
+    float* raw = sm;                                        // [rowsX][IQ_LINES]
+    float* band = raw + rowsX * IQ_LINES;                   // [rows][IQ_LINES]
+    float2* mix = reinterpret_cast<float2*>(band + rows * IQ_LINES);  // [rows][nf] (cI, cQ); offsets even
+    const int l0 = blockIdx.x * IQ_LINES;
+    const int so0 = blockIdx.y * IQB_OT;
+    const int sIn0 = so0 * a.stride - a.lpN / 2;
+    const int sX0 = sIn0 - hb;
+    const int tid = threadIdx.x;
+    for (int j = tid; j < nf * (a.bpN + 1); j += blockDim.x) bank[j] = a.bank[j];
+    for (int j = tid; j <= a.lpN; j += blockDim.x) lps[j] = a.lp[j];
+    for (int k = tid; k < rows * nf; k += blockDim.x) {
+        const int r = k / nf, f = k % nf;
+        const int s = sIn0 + r;
+        const float ph = __fmul_rn(static_cast<float>(s), a.fOverFs[f]);
+        float phI = __fadd_rn(ph, 0.0f);
+        float phQ = __fadd_rn(ph, 0.75f);
+        phI = __fsub_rn(phI, truncf(phI));
+        phQ = __fsub_rn(phQ, truncf(phQ));
+        mix[k] = make_float2(mixCos(phI), mixCos(phQ));
+    }
+    const int totalX = rowsX * IQ_LINES;
+    constexpr int kU = 8;
+    for (int base = tid; base < totalX; base += 256 * kU) {
+        float xs[kU];
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            const int idx = base + u * 256;
+            const int s = sX0 + idx / IQ_LINES, l = l0 + idx % IQ_LINES;
+            const bool ok = idx < totalX && l < a.nL && s >= 0 && s < a.nS;
+            xs[u] = ok ? toFloat(in[l + static_cast<size_t>(ok ? s : 0) * a.nL]) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; u++)
+            if (base + u * 256 < totalX) raw[base + u * 256] = xs[u];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < rows * IQ_LINES; idx += blockDim.x) {
+        const int row = idx / IQ_LINES, li = idx % IQ_LINES;
+        const int s = sIn0 + row, l = l0 + li;
+        float v = 0.0f;
+        if (l < a.nL && s >= 0 && s < a.nS) {
+            float acc[NF];
+            const float* xr = raw + row * IQ_LINES + li;  // band-pass window of sample s: rows row .. row + 2 hb
+            acc[0] = xr[hb * IQ_LINES];
+#pragma unroll
+            for (int f = 1; f < NF; f++) acc[f] = 0.0f;
+            // out-of-record samples are staged as 0: their terms (+-0) leave the sums unchanged, as the
+            // reference skips them
+            const float* bk = bank + (a.bpN + 1);
+            for (int fe = 0; fe <= 2 * hb; fe++) {
+                const float x = xr[fe * IQ_LINES];
+#pragma unroll
+                for (int f = 1; f < NF; f++) acc[f] = __fadd_rn(acc[f], __fmul_rn(x, bk[(f - 1) * (a.bpN + 1) + fe]));
+            }
+            float m = 0.0f;
+#pragma unroll
+            for (int f = 0; f < NF; f++) {
+                const float2 c = mix[row * nf + f];
+                const float dI = __fmul_rn(acc[f], c.x), dQ = __fmul_rn(acc[f], c.y);
+                m = __fadd_rn(m, __fmul_rn(a.weights[f], __fsqrt_rn(__fadd_rn(__fmul_rn(dI, dI), __fmul_rn(dQ, dQ)))));
+            }
+            v = __fmul_rn(a.scale, m);
+        }
+        band[idx] = v;
+    }
+    __syncthreads();
+    const int li = tid % IQ_LINES, o0 = (tid / IQ_LINES) * IQB_R;
+    const float* b = band + o0 * a.stride * IQ_LINES + li;
+    const int step = a.stride * IQ_LINES;
+    const int nTaps = 2 * (a.lpN / 2) + 1;
+    float acc[IQB_R];
+#pragma unroll
+    for (int k = 0; k < IQB_R; k++) acc[k] = 0.0f;
+#pragma unroll 2
+    for (int j = 0; j < nTaps; j++) {
+        const float t = lps[j];
+        const float* bj = b + j * IQ_LINES;
+#pragma unroll
+        for (int k = 0; k < IQB_R; k++) acc[k] = fmaf(bj[k * step], t, acc[k]);
+    }
+    const int l = l0 + li;
+#pragma unroll
+    for (int k = 0; k < IQB_R; k++) {
+        const int so = so0 + o0 + k;
+        if (so < a.nOut && l < a.nL) out[l + static_cast<size_t>(so) * a.nL] = clampCast<OUT>(acc[k]);
+    }
+}
+
 // ----------------------------------------------------------------------------- complex IQ
 template <typename IN>
 __global__ void __launch_bounds__(256) iqComplexKernel(const IN* __restrict__ in, float2* __restrict__ out,
@@ -745,6 +852,39 @@ int sb_iq_magnitude_run(const sb_iq_plan* p, const void* in, int in_dtype, void*
         if (in_dtype == SB_FLOAT32 && out_dtype == SB_INT16) SB_IQ1(float, int16_t);
         if (in_dtype == SB_INT16 && out_dtype == SB_INT16) SB_IQ1(int16_t, int16_t);
 #undef SB_IQ1
+        return fail(SB_ERR_UNSUPPORTED, "sb_iq_magnitude_run: %d -> %d unsupported", in_dtype, out_dtype);
+    }
+    const int rowsB = (IQB_OT - 1) * a.stride + a.lpN + 1, rowsBX = rowsB + 2 * (a.bpN / 2);
+    const size_t shmB = (static_cast<size_t>(rowsBX + rowsB) * IQ_LINES + 2 * static_cast<size_t>(rowsB) * a.numFilters) * sizeof(float);
+    if (a.numFilters > 1 && shmB <= 150 * 1024) {
+        dim3 gridB((a.nL + IQ_LINES - 1) / IQ_LINES, (a.nOut + IQB_OT - 1) / IQB_OT);
+        SB_REQUIRE(gridB.y <= 65535u, "sb_iq_magnitude_run: %d outputs exceed the grid", a.nOut);
+#define SB_IQBN(INT, OUTT, NF)                                                                                       \
+    do {                                                                                                             \
+        SB_CUDA(cudaFuncSetAttribute(iqMagnitudeBankKernel<INT, OUTT, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     static_cast<int>(shmB)));                                                       \
+        iqMagnitudeBankKernel<INT, OUTT, NF><<<gridB, 256, shmB, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), a); \
+    } while (0)
+#define SB_IQB(INT, OUTT)                                                                                            \
+    do {                                                                                                             \
+        switch (a.numFilters) {                                                                                      \
+            case 2: SB_IQBN(INT, OUTT, 2); break;                                                                    \
+            case 3: SB_IQBN(INT, OUTT, 3); break;                                                                    \
+            case 4: SB_IQBN(INT, OUTT, 4); break;                                                                    \
+            case 5: SB_IQBN(INT, OUTT, 5); break;                                                                    \
+            case 6: SB_IQBN(INT, OUTT, 6); break;                                                                    \
+            case 7: SB_IQBN(INT, OUTT, 7); break;                                                                    \
+            default: SB_IQBN(INT, OUTT, 8); break;                                                                   \
+        }                                                                                                            \
+        SB_CHECK_LAUNCH("iqMagnitudeBankKernel");                                                                    \
+        return SB_OK;                                                                                                \
+    } while (0)
+        if (in_dtype == SB_FLOAT32 && out_dtype == SB_FLOAT32) SB_IQB(float, float);
+        if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_IQB(int16_t, float);
+        if (in_dtype == SB_FLOAT32 && out_dtype == SB_INT16) SB_IQB(float, int16_t);
+        if (in_dtype == SB_INT16 && out_dtype == SB_INT16) SB_IQB(int16_t, int16_t);
+#undef SB_IQB
+#undef SB_IQBN
         return fail(SB_ERR_UNSUPPORTED, "sb_iq_magnitude_run: %d -> %d unsupported", in_dtype, out_dtype);
     }
     const int rows = (IQ_OT - 1) * a.stride + a.lpN + 1;
