@@ -228,6 +228,9 @@ def chain_rows(g0, o0, hbm_row):
     iq = IQDemodulator(40e6, 2.5e6, 51, 51, (7e6,), (1e6,), (1.0,))
     ms = _graph_ms(lambda: iq.demodulate_magnitude(big, 4), 10)
     res["iq_magnitude_large"] = {"ms": ms, "px_per_s": n / ms * 1e3, **hbm_row(4 * n + 4 * (n // 4), ms)}
+    iq3 = IQDemodulator(40e6, 2.5e6, 51, 51, (7e6, 5e6, 9e6), (1e6, 2e6, 2e6), (1.0, 0.5, 0.5))
+    ms = _graph_ms(lambda: iq3.demodulate_magnitude(big, 4), 5)
+    res["iq_magnitude_3f_large"] = {"ms": ms, "px_per_s": n / ms * 1e3, "filters": 3, **hbm_row(4 * n + 4 * (n // 4), ms)}
     ms = _graph_ms(lambda: logc.compress(big, 50.0, 1.0, 4000.0, out_dtype=torch.uint8), 10)
     res["logcompress_large"] = {"ms": ms, "px_per_s": n / ms * 1e3, **hbm_row(5 * n, ms)}
     del big
@@ -418,6 +421,12 @@ def reference_gpu_rows(res):
                           C.c_uint32(1), *(C.c_void_p(v.ctypes.data) for v in fa), 10)
     row("iq_magnitude_large", ms, res.get("iq_magnitude_large", {}).get("ms"),
         "IQ magnitude, 51-tap filters, decimation 4, 16384 x 2048 float image")
+    f3 = [np.ascontiguousarray(v, np.float64) for v in ((7e6, 5e6, 9e6), (1e6, 2e6, 2e6), (1.0, 0.5, 0.5))]
+    ms = lib.refg_time_iq(C.c_void_p(hb.ctypes.data), C.c_uint32(2048), C.c_uint32(16384), C.c_double(40e6),
+                          C.c_double(7e6), C.c_double(2.5e6), C.c_uint32(51), C.c_uint32(51), C.c_uint32(4),
+                          C.c_uint32(3), *(C.c_void_p(v.ctypes.data) for v in f3), 3)
+    row("iq_magnitude_3f_large", ms, res.get("iq_magnitude_3f_large", {}).get("ms"),
+        "IQ magnitude with frequency compounding (3 filters), decimation 4, 16384 x 2048 float image")
     ms = lib.refg_time_logcompress(C.c_void_p(hb.ctypes.data), C.c_uint32(2048), C.c_uint32(16384), C.c_double(50.0),
                                    C.c_double(1.0), C.c_double(4000.0), 10)
     row("logcompress_large", ms, res.get("logcompress_large", {}).get("ms"),
