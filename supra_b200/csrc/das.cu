@@ -540,7 +540,10 @@ template <> __device__ __forceinline__ float ldSample<int16_t>(const int16_t* p)
 template <> __device__ __forceinline__ float ldSample<float>(const float* p) { return __ldg(p); }
 
 // elA[j] = (x, z, deep weight, channel row offset as int bits), elB[j] = (dx, dz, dx^2 + dz^2, 0).
-template <typename RF, bool DEEP>
+// STRAIGHT (a scanline with dirX = dirZ = 0): the element's offsets from the scanline do not depend on
+// depth, so elA[j].x holds dx^2 + dz^2, the same float operations the general form performs per
+// depth. OFS: a nonzero sample offset is added (x + 0 is x, so a zero offset is skipped).
+template <typename RF, bool DEEP, bool STRAIGHT, bool OFS>
 __device__ __forceinline__ void das3dAccum(const float4* elA, const float4* elB, const float* lut, int nPad,
                                            const RF* tx, uint32_t nS, float px, float pz, float ay2, float iD,
                                            float d, float offset, float aDT2, float invX, float invY,
@@ -564,9 +567,15 @@ __device__ __forceinline__ void das3dAccum(const float4* elA, const float4* elB,
                     numAdds++;
                 }
             }
-            const float qx = __fsub_rn(A.x, px), qz = __fsub_rn(A.y, pz);
-            const float q = __fadd_rn(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qz, qz)), ay2);
-            const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(__fsqrt_rn(q), d)), offset);
+            float q;
+            if constexpr (STRAIGHT) {
+                q = __fadd_rn(A.x, ay2);
+            } else {
+                const float qx = __fsub_rn(A.x, px), qz = __fsub_rn(A.y, pz);
+                q = __fadd_rn(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qz, qz)), ay2);
+            }
+            const float dl = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(q), d));
+            const float delayf = OFS ? __fadd_rn(dl, offset) : dl;
             // floor as unsigned, saturating at 0 for negative (and NaN) positions like the reference's
             // conversion; positions >= 2^23 give an index >= 2^23, beyond every record
             const float t = __fadd_rd(fmaxf(delayf, 0.0f), 8388608.0f);
@@ -611,6 +620,7 @@ __global__ void __launch_bounds__(256, 5) das3dTableKernel(DasArgs a, int cap) {
     const int n0 = min(nx * ny, cap);  // nx * ny <= maxApertureX * maxApertureY <= cap for every line
     const float invXd = __fdiv_rn(1.0f, s.maxDistX), invYd = __fdiv_rn(1.0f, s.maxDistY);
     const bool mapped = a.e2c != nullptr;
+    const bool straight = s.dirX == 0.0f && s.dirZ == 0.0f;
     for (int j = tid; j < n0; j += 256) {
         const uint32_t ex = s.firstX[k] + j / ny, ey = s.firstY[k] + j % ny;
         const uint32_t e = ex + ey * a.layoutX;
@@ -621,7 +631,7 @@ __global__ void __launch_bounds__(256, 5) das3dTableKernel(DasArgs a, int cap) {
         const float wDeep = __fsqrt_rn(__fmul_rn(lutGet(lut, __fmul_rn(dx, invXd)), lutGet(lut, __fmul_rn(dz, invYd))));
         // unmapped elements (ch < 0) are removed below; the row offset keeps them recognisable
         const int chOff = ch < 0 ? -1 : ch * static_cast<int>(a.nS);
-        elA[j] = make_float4(xel, zel, wDeep, __int_as_float(chOff));
+        elA[j] = make_float4(straight ? r2 : xel, zel, wDeep, __int_as_float(chOff));
         elB[j] = make_float4(dx, dz, r2, 0.0f);
         if (!mapped && r2 == r2) atomicMax(&maxR2Bits, __float_as_int(r2));
     }
@@ -678,12 +688,19 @@ __global__ void __launch_bounds__(256, 5) das3dTableKernel(DasArgs a, int cap) {
         const float pz = __fadd_rn(s.z, __fmul_rn(s.dirZ, d));
         const float ay = __fmul_rn(s.dirY, d);
         const float ay2 = __fmul_rn(ay, ay);
-        if (deep)
-            das3dAccum<RF, true>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset, aDT2,
-                                 invX, invY, sample, weightAcum, numAdds);
-        else
-            das3dAccum<RF, false>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset, aDT2,
-                                  invX, invY, sample, weightAcum, numAdds);
+#define SB_3D(DP, ST, OF)                                                                                      \
+    das3dAccum<RF, DP, ST, OF>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset, aDT2, \
+                               invX, invY, sample, weightAcum, numAdds)
+        const bool ofs = a.offset != 0.0f;
+        if (straight && !ofs) {
+            if (deep) SB_3D(true, true, false);
+            else SB_3D(false, true, false);
+        } else if (deep) {
+            SB_3D(true, false, true);
+        } else {
+            SB_3D(false, false, true);
+        }
+#undef SB_3D
     }
     __syncthreads();  // sumDeep
     if (!inRange) return;
