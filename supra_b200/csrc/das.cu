@@ -404,14 +404,19 @@ __global__ void __launch_bounds__(256) dasVariantKernel(DasArgs a) {
 // entries. Each pass takes elements four at a time: aperture test, weight and running weight sum in
 // element order, delays, then the eight gathers together, then the reducer's updates in element order,
 // so the arithmetic and its order are those of variant2D (bit-identical).
+// Elements outside the aperture change nothing in the reference's loop, so a pass may start at any
+// multiple of four at or below the first element inside it and stop after the last (j0, j1: a range
+// covering the aperture). DX2 (unsteered scanline): the table's w field holds dx * dx, the product the
+// general form computes per depth. OFS: a nonzero sample offset is added. INTERIOR (checked by the
+// caller for the warp): every element of [j0, j1) has its delay in [0, nS - 1).
 constexpr int kVarUnroll = 4;
 
-template <typename RF, int BF, int PASS>
-__device__ __forceinline__ void variantPass(const float4* el, int nPad, const float* lut, const RF* tx, uint32_t nS,
+template <typename RF, int BF, int PASS, bool DX2, bool OFS, bool INTERIOR>
+__device__ __forceinline__ void variantPass(const float4* el, int j0, int j1, const float* lut, const RF* tx, uint32_t nS,
                                             float aDT, float invMax, float xz, float dy2, float depth, float iD,
                                             float offset, float mean, float& sample, float& weightAcum, int& numAdds,
                                             float& value, float& cs, float& energy) {
-    for (int j = 0; j < nPad; j += kVarUnroll) {
+    for (int j = j0; j < j1; j += kVarUnroll) {
         float w[kVarUnroll], frac[kVarUnroll], v0[kVarUnroll], v1[kVarUnroll];
         int32_t idx[kVarUnroll];
         bool inAp[kVarUnroll], one[kVarUnroll], two[kVarUnroll];
@@ -426,13 +431,25 @@ __device__ __forceinline__ void variantPass(const float4* el, int nPad, const fl
                 weightAcum = __fadd_rn(weightAcum, w[u]);
                 numAdds++;
             }
-            const float ex = __fsub_rn(e.x, xz);
-            const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), dy2));
-            const float delayf = __fadd_rn(__fadd_rn(iD, __fadd_rn(dist, depth)), offset);
+            float ex2;
+            if constexpr (DX2) {
+                ex2 = e.w;
+            } else {
+                const float ex = __fsub_rn(e.x, xz);
+                ex2 = __fmul_rn(ex, ex);
+            }
+            const float dist = __fsqrt_rn(__fadd_rn(ex2, dy2));
+            const float dl = __fadd_rn(iD, __fadd_rn(dist, depth));
+            const float delayf = OFS ? __fadd_rn(dl, offset) : dl;
             const int32_t delay = static_cast<int32_t>(floorf(delayf));
             frac[u] = __fsub_rn(delayf, static_cast<float>(delay));
-            two[u] = inAp[u] && static_cast<uint32_t>(delay) < nS - 1;
-            one[u] = two[u] || (inAp[u] && static_cast<uint32_t>(delay) < nS && frac[u] == 0.0f);
+            if constexpr (INTERIOR) {
+                two[u] = inAp[u];
+                one[u] = inAp[u];
+            } else {
+                two[u] = inAp[u] && static_cast<uint32_t>(delay) < nS - 1;
+                one[u] = two[u] || (inAp[u] && static_cast<uint32_t>(delay) < nS && frac[u] == 0.0f);
+            }
             idx[u] = static_cast<int32_t>(static_cast<uint32_t>(chOff) + static_cast<uint32_t>(delay));  // used when one[u]
         }
 #pragma unroll
@@ -473,17 +490,24 @@ __global__ void __launch_bounds__(256) dasVariantTableKernel(DasArgs a) {
     const bool active = (s.activeMask >> k) & 1;
     const int n = active ? max(static_cast<int>(s.lastX[k]) - static_cast<int>(s.firstX[k]), 0) : 0;  // <= 256 (host)
     const int nPad = (n + kVarUnroll - 1) / kVarUnroll * kVarUnroll;
+    const bool dx2 = s.dirX == 0.0f;
     for (int j = tid; j < nPad; j += 256) {
         float4 r = make_float4(0.0f, 0.0f, __int_as_float(-1), 0.0f);
         if (j < n) {
             const int e = s.firstX[k] + j;
             const int ch = a.e2c ? __ldg(a.e2c + e) : static_cast<int>(static_cast<uint32_t>(e) % a.nCh);
             const float xel = __ldg(a.xe + e);
-            r = make_float4(xel, __fsub_rn(xel, s.x), __int_as_float(ch < 0 ? -1 : ch * static_cast<int>(a.nS)), 0.0f);
+            const float dx = __fsub_rn(xel, s.x);
+            r = make_float4(xel, dx, __int_as_float(ch < 0 ? -1 : ch * static_cast<int>(a.nS)), __fmul_rn(dx, dx));
         }
         el[j] = r;
     }
     __syncthreads();
+    // ordered by dx (the usual linear probe): the aperture is a contiguous range
+    int unsortedMine = 0;
+    for (int j = tid + 1; j < n; j += 256)
+        if (!(el[j].y >= el[j - 1].y)) unsortedMine = 1;
+    const bool sortedX = !__syncthreads_or(unsortedMine);
     const uint32_t r = blockIdx.x * blockDim.x + tid;
     if (r >= a.nD) return;
     float acc = 0.0f;
@@ -498,17 +522,56 @@ __global__ void __launch_bounds__(256) dasVariantTableKernel(DasArgs a) {
         const float iD = s.initialDelay[k];
         float sample = 0.0f, weightAcum = 0.0f, value = 0.0f, cs = 0.0f, energy = 0.0f;
         int numAdds = 0;
-        variantPass<RF, BF, 0>(el, nPad, lut, tx, a.nS, aDT, invMax, xz, dy2, d, iD, a.offset, 0.0f, sample,
-                               weightAcum, numAdds, value, cs, energy);
+        // the aperture's range: binary searches on dx, the first element rounded down to a group of four
+        int j0 = 0, j1 = nPad;
+        if (sortedX) {
+            int lo = 0, hi = n;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (el[mid].y < -aDT) lo = mid + 1;
+                else hi = mid;
+            }
+            j0 = lo & ~(kVarUnroll - 1);
+            hi = n;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (el[mid].y <= aDT) lo = mid + 1;
+                else hi = mid;
+            }
+            j1 = lo;
+        }
+        // every delay of the range inside [0, nS - 1)? delays grow with dx^2 (largest at an end of the
+        // range) and are at least iD + depth; for unsteered lines without an offset, voted over the warp
+        bool interior = false;
+        const bool ofs = a.offset != 0.0f;
+        if (sortedX && dx2 && !ofs && j1 > j0) {
+            const int jl = max(j0, 0), jr = min(j1, n) - 1;
+            const float e2 = fmaxf(el[jl].w, el[jr].w);
+            const float lo = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(dy2), d));
+            const float hi = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(__fadd_rn(e2, dy2)), d));
+            interior = lo >= 0.0f && hi < static_cast<float>(a.nS - 1);
+        }
+        interior = __all_sync(__activemask(), interior);
+#define SB_VPASS(PS, DXX, OF, IN, MEAN)                                                                          \
+    variantPass<RF, BF, PS, DXX, OF, IN>(el, j0, j1, lut, tx, a.nS, aDT, invMax, xz, dy2, d, iD, a.offset, MEAN,  \
+                                         sample, weightAcum, numAdds, value, cs, energy)
+#define SB_VPASS_ALL(PS, MEAN)                                                                                   \
+    do {                                                                                                         \
+        if (interior) SB_VPASS(PS, true, false, true, MEAN);                                                     \
+        else if (dx2 && !ofs) SB_VPASS(PS, true, false, false, MEAN);                                            \
+        else SB_VPASS(PS, false, true, false, MEAN);                                                             \
+    } while (0)
+        SB_VPASS_ALL(0, 0.0f);
         float v = 0.0f;
         if (BF == SB_BF_DELAY_AND_STDDEV) {
             const float mean = numAdds > 0 ? __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds)) : 0.0f;
             weightAcum = 0.0f;
             numAdds = 0;
             value = 0.0f;
-            variantPass<RF, BF, 1>(el, nPad, lut, tx, a.nS, aDT, invMax, xz, dy2, d, iD, a.offset, mean, sample,
-                                   weightAcum, numAdds, value, cs, energy);
+            SB_VPASS_ALL(1, mean);
             if (numAdds > 0) v = __fmul_rn(__fdiv_rn(__fsqrt_rn(cs), weightAcum), static_cast<float>(numAdds));
+#undef SB_VPASS_ALL
+#undef SB_VPASS
         } else if (numAdds > 0) {
             const float das = __fmul_rn(__fdiv_rn(sample, weightAcum), static_cast<float>(numAdds));
             v = __fmul_rn(__fdiv_rn(__fdiv_rn(__fmul_rn(cs, cs), energy), static_cast<float>(numAdds)), das);
@@ -543,7 +606,10 @@ template <> __device__ __forceinline__ float ldSample<float>(const float* p) { r
 // STRAIGHT (a scanline with dirX = dirZ = 0): the element's offsets from the scanline do not depend on
 // depth, so elA[j].x holds dx^2 + dz^2, the same float operations the general form performs per
 // depth. OFS: a nonzero sample offset is added (x + 0 is x, so a zero offset is skipped).
-template <typename RF, bool DEEP, bool STRAIGHT, bool OFS>
+// INTERIOR (STRAIGHT only, checked by the caller for the whole warp): every element's delay lies in
+// [0, nS - 1), so the record-edge cases drop out. Padding elements then have r2 = 0, deep weight 0 and
+// row 0 (an in-range gather whose term is +-0, which leaves the sum unchanged) and no aperture.
+template <typename RF, bool DEEP, bool STRAIGHT, bool OFS, bool INTERIOR>
 __device__ __forceinline__ void das3dAccum(const float4* elA, const float4* elB, const float* lut, int nPad,
                                            const RF* tx, uint32_t nS, float px, float pz, float ay2, float iD,
                                            float d, float offset, float aDT2, float invX, float invY,
@@ -581,8 +647,13 @@ __device__ __forceinline__ void das3dAccum(const float4* elA, const float4* elB,
             const float t = __fadd_rd(fmaxf(delayf, 0.0f), 8388608.0f);
             const uint32_t delay = __float_as_uint(t) - 0x4B000000u;
             frac[u] = __fsub_rn(delayf, __fsub_rn(t, 8388608.0f));
-            two[u] = inR && delay < nS - 1;
-            one[u] = two[u] || (inR && delay < nS && frac[u] == 0.0f);
+            if constexpr (INTERIOR) {
+                two[u] = inR;
+                one[u] = inR;
+            } else {
+                two[u] = inR && delay < nS - 1;
+                one[u] = two[u] || (inR && delay < nS && frac[u] == 0.0f);
+            }
             idx[u] = static_cast<int>(static_cast<uint32_t>(__float_as_int(A.w)) + delay);  // used when one[u]
         }
 #pragma unroll
@@ -659,7 +730,9 @@ __global__ void __launch_bounds__(256, 5) das3dTableKernel(DasArgs a, int cap) {
     const int n = mapped ? nEl : n0;
     const int nPad = (n + k3DUnroll - 1) / k3DUnroll * k3DUnroll;  // <= cap (cap is a multiple of 4)
     for (int j = n + tid; j < nPad; j += 256) {
-        elA[j] = make_float4(INFINITY, 0.0f, 0.0f, __int_as_float(0));
+        // general form: an element at infinity (delay beyond every record); unsteered: r2 = 0, deep
+        // weight 0, row 0 (see das3dAccum)
+        elA[j] = make_float4(straight ? 0.0f : INFINITY, 0.0f, 0.0f, __int_as_float(0));
         elB[j] = make_float4(0.0f, 0.0f, INFINITY, 0.0f);
     }
     __syncthreads();
@@ -688,17 +761,28 @@ __global__ void __launch_bounds__(256, 5) das3dTableKernel(DasArgs a, int cap) {
         const float pz = __fadd_rn(s.z, __fmul_rn(s.dirZ, d));
         const float ay = __fmul_rn(s.dirY, d);
         const float ay2 = __fmul_rn(ay, ay);
-#define SB_3D(DP, ST, OF)                                                                                      \
-    das3dAccum<RF, DP, ST, OF>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset, aDT2, \
-                               invX, invY, sample, weightAcum, numAdds)
+#define SB_3D(DP, ST, OF, IN)                                                                                  \
+    das3dAccum<RF, DP, ST, OF, IN>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset,    \
+                                   aDT2, invX, invY, sample, weightAcum, numAdds)
         const bool ofs = a.offset != 0.0f;
         if (straight && !ofs) {
-            if (deep) SB_3D(true, true, false);
-            else SB_3D(false, true, false);
+            // delays grow with q = r2 + ay2 (monotone float operations), so the element with the largest
+            // r2 and q = ay2 bound every delay of this depth (the padding's r2 = 0 included)
+            const float iD = s.initialDelay[k];
+            const float lo = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(ay2), d));
+            const float hi = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(__fadd_rn(maxR2, ay2)), d));
+            const bool interior = __all_sync(__activemask(), lo >= 0.0f && hi < static_cast<float>(a.nS - 1));
+            if (interior) {
+                if (deep) SB_3D(true, true, false, true);
+                else SB_3D(false, true, false, true);
+            } else {
+                if (deep) SB_3D(true, true, false, false);
+                else SB_3D(false, true, false, false);
+            }
         } else if (deep) {
-            SB_3D(true, false, true);
+            SB_3D(true, false, true, false);
         } else {
-            SB_3D(false, false, true);
+            SB_3D(false, false, true, false);
         }
 #undef SB_3D
     }
