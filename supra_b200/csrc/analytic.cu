@@ -22,6 +22,7 @@
 // over N is h_x + i h_y. O(N log N) instead of the circulant product's 2 N^2 flops per scanline.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -31,7 +32,7 @@
 struct sb_analytic_plan {
     uint32_t n = 0;
     float* dK = nullptr;    // k[0..N)
-    float2* dTw = nullptr;  // exp(-2 pi i j / N), j < N / 2 (power-of-two N only)
+    float2* dTw = nullptr;  // per FFT stage s (h = 2^(s-1) entries at offset h - 1): exp(-2 pi i j / 2^s), j < h
 };
 
 namespace sb {
@@ -42,8 +43,8 @@ constexpr int kAThreads = 64;
 
 constexpr int kASplit = 8;  // CTAs per cluster sharing one output tile
 
-// Lengths of the FFT path: powers of two from 64 to 16384 (the transform and its twiddles, 12 N bytes,
-// fit a CTA's shared memory).
+// Lengths of the FFT path: powers of two from 64 to 16384 (the transform, 8 N bytes, fits a CTA's
+// shared memory).
 inline bool fftLength(uint32_t N) { return N >= 64 && N <= 16384 && (N & (N - 1)) == 0; }
 
 __device__ __forceinline__ float4 load4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(kAThreads) analyticEnvKernel(const IN* __restr
     analyticStore<IN, OUT>(in, out, N, nL, n0, l0, tot);
 }
 
-constexpr int kFftThreads = 256;
+constexpr int kFftThreads = 1024;  // upper bound; a launch uses min(1024, N / 2) threads (one butterfly each per stage)
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
     return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
@@ -218,26 +219,27 @@ template <typename IN, typename OUT>
 __global__ void __launch_bounds__(kFftThreads) analyticFftKernel(const IN* __restrict__ in, OUT* __restrict__ out,
                                                                  const float2* __restrict__ tw, int N, int logN, int nL) {
     extern __shared__ float2 fsm[];
-    float2* z = fsm;       // N values
-    float2* w = fsm + N;   // N / 2 twiddles
-    const int tid = threadIdx.x;
+    float2* z = fsm;  // N values
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int l = 2 * static_cast<int>(blockIdx.x);
     const bool two = l + 1 < nL;
     const int half = N >> 1;
-    for (int j = tid; j < half; j += kFftThreads) w[j] = __ldg(tw + j);
-    for (int n = tid; n < N; n += kFftThreads) {
+    for (int n = tid; n < N; n += nt) {
         const size_t base = static_cast<size_t>(n) * nL + l;
         const float x = ldf(in + base), y = two ? ldf(in + base + 1) : 0.0f;
         z[__brev(static_cast<uint32_t>(n)) >> (32 - logN)] = make_float2(x, y);
     }
     __syncthreads();
     // forward transform, decimation in time: stage s joins blocks of 2^(s-1) with exp(-2 pi i j / 2^s)
+    // (the stage's twiddles are contiguous in global memory: L1-resident, no shared-memory bank
+    // conflicts for any stage)
     for (int s = 1; s <= logN; s++) {
-        const int h = 1 << (s - 1), stride = N >> s;
-        for (int b = tid; b < half; b += kFftThreads) {
+        const int h = 1 << (s - 1);
+        const float2* ws = tw + (h - 1);
+        for (int b = tid; b < half; b += nt) {
             const int j = b & (h - 1);
             const int i0 = ((b >> (s - 1)) << s) + j, i1 = i0 + h;
-            const float2 t = cmulf(w[j * stride], z[i1]);
+            const float2 t = cmulf(__ldg(ws + j), z[i1]);
             const float2 a = z[i0];
             z[i0] = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
             z[i1] = make_float2(__fsub_rn(a.x, t.x), __fsub_rn(a.y, t.y));
@@ -246,26 +248,27 @@ __global__ void __launch_bounds__(kFftThreads) analyticFftKernel(const IN* __res
     }
     // times -i sgn(k): positive frequencies (1 .. N/2 - 1) (re, im) -> (im, -re), negative ones
     // (N/2 + 1 .. N - 1) -> (-im, re), DC and Nyquist -> 0
-    for (int k = tid; k < N; k += kFftThreads) {
+    for (int k = tid; k < N; k += nt) {
         const float2 v = z[k];
         z[k] = (k == 0 || k == half) ? make_float2(0.0f, 0.0f) : (k < half ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x));
     }
     __syncthreads();
     // inverse transform, decimation in frequency: stage s splits blocks of 2^s with exp(+2 pi i j / 2^s)
     for (int s = logN; s >= 1; s--) {
-        const int h = 1 << (s - 1), stride = N >> s;
-        for (int b = tid; b < half; b += kFftThreads) {
+        const int h = 1 << (s - 1);
+        const float2* ws = tw + (h - 1);
+        for (int b = tid; b < half; b += nt) {
             const int j = b & (h - 1);
             const int i0 = ((b >> (s - 1)) << s) + j, i1 = i0 + h;
             const float2 a = z[i0], c = z[i1];
-            const float2 wj = w[j * stride];
+            const float2 wj = __ldg(ws + j);
             z[i0] = make_float2(__fadd_rn(a.x, c.x), __fadd_rn(a.y, c.y));
             z[i1] = cmulf(make_float2(__fsub_rn(a.x, c.x), __fsub_rn(a.y, c.y)), make_float2(wj.x, -wj.y));
         }
         __syncthreads();
     }
     const float invN = __fdiv_rn(1.0f, static_cast<float>(N));
-    for (int n = tid; n < N; n += kFftThreads) {
+    for (int n = tid; n < N; n += nt) {
         const float2 hv = z[__brev(static_cast<uint32_t>(n)) >> (32 - logN)];
         const size_t base = static_cast<size_t>(n) * nL + l;
         const float x = ldf(in + base), hx = __fmul_rn(hv.x, invN);
@@ -304,13 +307,14 @@ int sb_analytic_plan_create(uint32_t num_samples, sb_analytic_plan** out) {
     cudaError_t e = cudaMalloc(&p->dK, N * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpy(p->dK, k.data(), N * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && fftLength(N)) {
-        std::vector<float2> tw(N / 2);
-        for (uint32_t j = 0; j < N / 2; j++) {
-            const double a = 2.0 * pi * static_cast<double>(j) / N;
-            tw[j] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(-std::sin(a)));
-        }
-        e = cudaMalloc(&p->dTw, (N / 2) * sizeof(float2));
-        if (e == cudaSuccess) e = cudaMemcpy(p->dTw, tw.data(), (N / 2) * sizeof(float2), cudaMemcpyHostToDevice);
+        std::vector<float2> tw(N - 1);
+        for (uint32_t h = 1; h < N; h <<= 1)  // stage with blocks of 2h: exp(-2 pi i j / (2 h)), j < h
+            for (uint32_t j = 0; j < h; j++) {
+                const double a = pi * static_cast<double>(j) / h;
+                tw[h - 1 + j] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(-std::sin(a)));
+            }
+        e = cudaMalloc(&p->dTw, (N - 1) * sizeof(float2));
+        if (e == cudaSuccess) e = cudaMemcpy(p->dTw, tw.data(), (N - 1) * sizeof(float2), cudaMemcpyHostToDevice);
     }
     if (e != cudaSuccess) {
         cudaFree(p->dK);
@@ -342,14 +346,15 @@ int sb_analytic_env_run(const sb_analytic_plan* p, const void* in, int in_dtype,
     if (p->dTw) {  // power-of-two length: the FFT path
         int logN = 0;
         while ((1 << logN) < N) logN++;
-        const size_t shm = static_cast<size_t>(N) * sizeof(float2) + static_cast<size_t>(N / 2) * sizeof(float2);
+        const size_t shm = static_cast<size_t>(N) * sizeof(float2);
         const unsigned grid = static_cast<unsigned>((nL + 1) / 2);
+        const int fftThreads = std::min(kFftThreads, N / 2);
         cudaStream_t stf = S(stream);
 #define SB_AF(IT, OT)                                                                                                  \
     do {                                                                                                               \
         SB_CUDA(cudaFuncSetAttribute(analyticFftKernel<IT, OT>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
                                      static_cast<int>(shm)));                                                          \
-        analyticFftKernel<IT, OT><<<grid, kFftThreads, shm, stf>>>(static_cast<const IT*>(in), static_cast<OT*>(out),  \
+        analyticFftKernel<IT, OT><<<grid, fftThreads, shm, stf>>>(static_cast<const IT*>(in), static_cast<OT*>(out),  \
                                                                    p->dTw, N, logN, nL);                              \
     } while (0)
         if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_AF(int16_t, float);

@@ -362,13 +362,13 @@ __global__ void __launch_bounds__(256) iqMagnitudeKernel(const IN* __restrict__ 
 // scale w0 sqrt((x cI)^2 + (x cQ)^2) with mixer values cI, cQ that depend on s only, i.e. |x| G(s) with
 // G(s) = scale w0 sqrt(cI^2 + cQ^2) (equal up to the rounding of the products, ~1e-7 relative).
 // A CTA of 32 scanlines x 64 decimated outputs forms cI, cQ and G once per input row and |x| G per
-// sample (no halo recomputation of the mixer), then each thread sums 8 outputs of one scanline, one
-// shared tap value per step for all 8 (fused multiply-adds, as nvcc contracts the reference's
+// sample (no halo recomputation of the mixer), then each thread sums 4 outputs of two neighbouring
+// scanlines, one shared tap value per step for all 8 (fused multiply-adds, as nvcc contracts the reference's
 // `accumulator += sample * filterElement` in its default build). A sample with |x| >= 2^63 or not finite, whose squares may overflow, takes the
 // reference's expression (so clamped +-FLT_MAX pixels give the same infinities). Samples outside the
 // record are staged as 0: their terms leave the sums unchanged, as the reference skips them.
 constexpr int IQ1_OT = 64;
-constexpr int IQ1_R = 8;  // outputs per thread (256 threads = 32 scanlines x 8 groups of 8 outputs)
+constexpr int IQ1_R = 8;  // outputs per thread (256 threads = 16 scanline pairs x 16 groups of 4 outputs)
 
 template <typename IN, typename OUT>
 __global__ void __launch_bounds__(256) iqMagnitude1Kernel(const IN* __restrict__ in, OUT* __restrict__ out, IqArgs a) {
@@ -431,25 +431,32 @@ __global__ void __launch_bounds__(256) iqMagnitude1Kernel(const IN* __restrict__
         }
     }
     __syncthreads();
-    const int li = tid % IQ_LINES, o0 = (tid / IQ_LINES) * IQ1_R;
-    const float* b = band + o0 * a.stride * IQ_LINES + li;
-    const int step = a.stride * IQ_LINES;
+    // a thread: two neighbouring scanlines (one 8-byte shared-memory read per row) x IQ1_R / 2 outputs;
+    // the pair's two sums in one packed FMA (two IEEE fused multiply-adds)
+    constexpr int kR = IQ1_R / 2;
+    const int lp = tid % (IQ_LINES / 2), o0 = (tid / (IQ_LINES / 2)) * kR;
+    const float2* b = reinterpret_cast<const float2*>(band) + o0 * a.stride * (IQ_LINES / 2) + lp;
+    const int step = a.stride * (IQ_LINES / 2);
     const int nTaps = 2 * (a.lpN / 2) + 1;  // the reference's window [si - lpN/2, si + lpN/2]
-    float acc[IQ1_R];
+    float2 acc[kR];
 #pragma unroll
-    for (int k = 0; k < IQ1_R; k++) acc[k] = 0.0f;
+    for (int k = 0; k < kR; k++) acc[k] = make_float2(0.0f, 0.0f);
 #pragma unroll 2
     for (int j = 0; j < nTaps; j++) {
         const float t = lps[j];
-        const float* bj = b + j * IQ_LINES;
+        const float2 t2 = make_float2(t, t);
+        const float2* bj = b + j * (IQ_LINES / 2);
 #pragma unroll
-        for (int k = 0; k < IQ1_R; k++) acc[k] = fmaf(bj[k * step], t, acc[k]);
+        for (int k = 0; k < kR; k++) acc[k] = __ffma2_rn(bj[k * step], t2, acc[k]);
     }
-    const int l = l0 + li;
+    const int l = l0 + 2 * lp;
 #pragma unroll
-    for (int k = 0; k < IQ1_R; k++) {
+    for (int k = 0; k < kR; k++) {
         const int so = so0 + o0 + k;
-        if (so < a.nOut && l < a.nL) out[l + static_cast<size_t>(so) * a.nL] = clampCast<OUT>(acc[k]);
+        if (so < a.nOut) {
+            if (l < a.nL) out[l + static_cast<size_t>(so) * a.nL] = clampCast<OUT>(acc[k].x);
+            if (l + 1 < a.nL) out[l + 1 + static_cast<size_t>(so) * a.nL] = clampCast<OUT>(acc[k].y);
+        }
     }
 }
 
