@@ -214,8 +214,12 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
 }
 template <typename T> __device__ __forceinline__ float ldf(const T* p) { return static_cast<float>(__ldg(p)); }
 
+constexpr int kFftOneLog = 11;  // ONE: N <= 2^11, one butterfly per thread and stage
+
 // Envelopes of scanlines (2 b, 2 b + 1) of a [N][nL] image by FFT (N = 2^logN): see the file comment.
-template <typename IN, typename OUT>
+// ONE (N / 2 threads, N <= 2^kFftOneLog): each thread's twiddle of every stage is loaded into registers
+// before the transforms, so no stage waits on a twiddle load.
+template <typename IN, typename OUT, bool ONE>
 __global__ void __launch_bounds__(kFftThreads) analyticFftKernel(const IN* __restrict__ in, OUT* __restrict__ out,
                                                                  const float2* __restrict__ tw, int N, int logN, int nL) {
     extern __shared__ float2 fsm[];
@@ -224,6 +228,12 @@ __global__ void __launch_bounds__(kFftThreads) analyticFftKernel(const IN* __res
     const int l = 2 * static_cast<int>(blockIdx.x);
     const bool two = l + 1 < nL;
     const int half = N >> 1;
+    float2 wr[ONE ? kFftOneLog : 1];
+    if constexpr (ONE) {
+#pragma unroll
+        for (int s = 1; s <= kFftOneLog; s++)
+            if (s <= logN) wr[s - 1] = __ldg(tw + ((1 << (s - 1)) - 1) + (tid & ((1 << (s - 1)) - 1)));
+    }
     for (int n = tid; n < N; n += nt) {
         const size_t base = static_cast<size_t>(n) * nL + l;
         const float x = ldf(in + base), y = two ? ldf(in + base + 1) : 0.0f;
@@ -233,18 +243,33 @@ __global__ void __launch_bounds__(kFftThreads) analyticFftKernel(const IN* __res
     // forward transform, decimation in time: stage s joins blocks of 2^(s-1) with exp(-2 pi i j / 2^s)
     // (the stage's twiddles are contiguous in global memory: L1-resident, no shared-memory bank
     // conflicts for any stage)
-    for (int s = 1; s <= logN; s++) {
-        const int h = 1 << (s - 1);
-        const float2* ws = tw + (h - 1);
-        for (int b = tid; b < half; b += nt) {
+    if constexpr (ONE) {
+#pragma unroll
+        for (int s = 1; s <= kFftOneLog; s++) {
+            if (s > logN) break;
+            const int h = 1 << (s - 1), b = tid;
             const int j = b & (h - 1);
             const int i0 = ((b >> (s - 1)) << s) + j, i1 = i0 + h;
-            const float2 t = cmulf(__ldg(ws + j), z[i1]);
+            const float2 t = cmulf(wr[s - 1], z[i1]);
             const float2 a = z[i0];
             z[i0] = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
             z[i1] = make_float2(__fsub_rn(a.x, t.x), __fsub_rn(a.y, t.y));
+            __syncthreads();
         }
-        __syncthreads();
+    } else {
+        for (int s = 1; s <= logN; s++) {
+            const int h = 1 << (s - 1);
+            const float2* ws = tw + (h - 1);
+            for (int b = tid; b < half; b += nt) {
+                const int j = b & (h - 1);
+                const int i0 = ((b >> (s - 1)) << s) + j, i1 = i0 + h;
+                const float2 t = cmulf(__ldg(ws + j), z[i1]);
+                const float2 a = z[i0];
+                z[i0] = make_float2(__fadd_rn(a.x, t.x), __fadd_rn(a.y, t.y));
+                z[i1] = make_float2(__fsub_rn(a.x, t.x), __fsub_rn(a.y, t.y));
+            }
+            __syncthreads();
+        }
     }
     // times -i sgn(k): positive frequencies (1 .. N/2 - 1) (re, im) -> (im, -re), negative ones
     // (N/2 + 1 .. N - 1) -> (-im, re), DC and Nyquist -> 0
@@ -254,18 +279,33 @@ __global__ void __launch_bounds__(kFftThreads) analyticFftKernel(const IN* __res
     }
     __syncthreads();
     // inverse transform, decimation in frequency: stage s splits blocks of 2^s with exp(+2 pi i j / 2^s)
-    for (int s = logN; s >= 1; s--) {
-        const int h = 1 << (s - 1);
-        const float2* ws = tw + (h - 1);
-        for (int b = tid; b < half; b += nt) {
+    if constexpr (ONE) {
+#pragma unroll
+        for (int s = kFftOneLog; s >= 1; s--) {
+            if (s > logN) continue;
+            const int h = 1 << (s - 1), b = tid;
             const int j = b & (h - 1);
             const int i0 = ((b >> (s - 1)) << s) + j, i1 = i0 + h;
             const float2 a = z[i0], c = z[i1];
-            const float2 wj = __ldg(ws + j);
+            const float2 wj = wr[s - 1];
             z[i0] = make_float2(__fadd_rn(a.x, c.x), __fadd_rn(a.y, c.y));
             z[i1] = cmulf(make_float2(__fsub_rn(a.x, c.x), __fsub_rn(a.y, c.y)), make_float2(wj.x, -wj.y));
+            __syncthreads();
         }
-        __syncthreads();
+    } else {
+        for (int s = logN; s >= 1; s--) {
+            const int h = 1 << (s - 1);
+            const float2* ws = tw + (h - 1);
+            for (int b = tid; b < half; b += nt) {
+                const int j = b & (h - 1);
+                const int i0 = ((b >> (s - 1)) << s) + j, i1 = i0 + h;
+                const float2 a = z[i0], c = z[i1];
+                const float2 wj = __ldg(ws + j);
+                z[i0] = make_float2(__fadd_rn(a.x, c.x), __fadd_rn(a.y, c.y));
+                z[i1] = cmulf(make_float2(__fsub_rn(a.x, c.x), __fsub_rn(a.y, c.y)), make_float2(wj.x, -wj.y));
+            }
+            __syncthreads();
+        }
     }
     const float invN = __fdiv_rn(1.0f, static_cast<float>(N));
     for (int n = tid; n < N; n += nt) {
@@ -349,13 +389,21 @@ int sb_analytic_env_run(const sb_analytic_plan* p, const void* in, int in_dtype,
         const size_t shm = static_cast<size_t>(N) * sizeof(float2);
         const unsigned grid = static_cast<unsigned>((nL + 1) / 2);
         const int fftThreads = std::min(kFftThreads, N / 2);
+        const bool one = fftThreads == N / 2 && logN <= kFftOneLog;
         cudaStream_t stf = S(stream);
 #define SB_AF(IT, OT)                                                                                                  \
     do {                                                                                                               \
-        SB_CUDA(cudaFuncSetAttribute(analyticFftKernel<IT, OT>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
-                                     static_cast<int>(shm)));                                                          \
-        analyticFftKernel<IT, OT><<<grid, fftThreads, shm, stf>>>(static_cast<const IT*>(in), static_cast<OT*>(out),  \
-                                                                   p->dTw, N, logN, nL);                              \
+        if (one) {                                                                                                     \
+            SB_CUDA(cudaFuncSetAttribute(analyticFftKernel<IT, OT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         static_cast<int>(shm)));                                                      \
+            analyticFftKernel<IT, OT, true><<<grid, fftThreads, shm, stf>>>(static_cast<const IT*>(in),                \
+                                                                             static_cast<OT*>(out), p->dTw, N, logN, nL); \
+        } else {                                                                                                       \
+            SB_CUDA(cudaFuncSetAttribute(analyticFftKernel<IT, OT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         static_cast<int>(shm)));                                                      \
+            analyticFftKernel<IT, OT, false><<<grid, fftThreads, shm, stf>>>(static_cast<const IT*>(in),               \
+                                                                              static_cast<OT*>(out), p->dTw, N, logN, nL); \
+        }                                                                                                              \
     } while (0)
         if (in_dtype == SB_INT16 && out_dtype == SB_FLOAT32) SB_AF(int16_t, float);
         else if (in_dtype == SB_INT16) SB_AF(int16_t, int16_t);
