@@ -256,20 +256,37 @@ template <> struct Vec4<uint8_t> {
     static __device__ __forceinline__ uchar4 make(uint8_t a, uint8_t b, uint8_t c, uint8_t d) { return make_uchar4(a, b, c, d); }
 };
 
+// Grid-stride over groups of four: each thread loads kLogU groups before converting any, so that
+// their loads are in flight together (one group per short-lived thread left the kernel waiting on
+// load latency at about half its issue rate).
+constexpr int kLogU = 4;
+
 template <typename IN, typename OUT>
 __global__ void __launch_bounds__(256) logKernel4(const IN* __restrict__ in, OUT* __restrict__ out, size_t n, float inScale,
                                                   float k) {
-    const size_t g = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    using VI = typename Vec4<IN>::type;
+    using VO = typename Vec4<OUT>::type;
     const size_t n4 = n / 4;
-    if (g < n4) {
-        const auto v = __ldcs(reinterpret_cast<const typename Vec4<IN>::type*>(in) + g);
-        const auto o = Vec4<OUT>::make(clampCast<OUT>(logCompress(toFloat(v.x), inScale, k)),
-                                       clampCast<OUT>(logCompress(toFloat(v.y), inScale, k)),
-                                       clampCast<OUT>(logCompress(toFloat(v.z), inScale, k)),
-                                       clampCast<OUT>(logCompress(toFloat(v.w), inScale, k)));
-        __stcs(reinterpret_cast<typename Vec4<OUT>::type*>(out) + g, o);
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t g0 = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; g0 < n4; g0 += stride * kLogU) {
+        VI v[kLogU];
+#pragma unroll
+        for (int u = 0; u < kLogU; u++) {
+            const size_t g = g0 + u * stride;
+            if (g < n4) v[u] = __ldcs(reinterpret_cast<const VI*>(in) + g);
+        }
+#pragma unroll
+        for (int u = 0; u < kLogU; u++) {
+            const size_t g = g0 + u * stride;
+            if (g < n4)
+                __stcs(reinterpret_cast<VO*>(out) + g,
+                       Vec4<OUT>::make(clampCast<OUT>(logCompress(toFloat(v[u].x), inScale, k)),
+                                       clampCast<OUT>(logCompress(toFloat(v[u].y), inScale, k)),
+                                       clampCast<OUT>(logCompress(toFloat(v[u].z), inScale, k)),
+                                       clampCast<OUT>(logCompress(toFloat(v[u].w), inScale, k))));
+        }
     }
-    if (g == 0)
+    if (blockIdx.x == 0 && threadIdx.x == 0)
         for (size_t i = 4 * n4; i < n; i++) out[i] = clampCast<OUT>(logCompress(toFloat(in[i]), inScale, k));
 }
 
@@ -618,7 +635,9 @@ int launchLog(const void* in, int inDt, void* out, int outDt, size_t n, float in
                      (n / 4 + 255) / 256 <= 0x7fffffffu;
     int blocks = static_cast<int>(std::min<size_t>((n + 255) / 256, static_cast<size_t>(smCount()) * 16));
     if (blocks < 1) blocks = 1;
-    const unsigned blocks4 = static_cast<unsigned>(std::max<size_t>((n / 4 + 255) / 256, 1));
+    // four resident CTAs per SM (55-57 registers), each thread kLogU groups of four per step
+    const unsigned blocks4 = static_cast<unsigned>(std::max<size_t>(
+        std::min<size_t>((n / 4 + 256 * kLogU - 1) / (256 * kLogU), static_cast<size_t>(smCount()) * 4), 1));
 #define SB_LOG(INT, OUTT)                                                                                                  \
     do {                                                                                                                   \
         if (vec) logKernel4<INT, OUTT><<<blocks4, 256, 0, st>>>(static_cast<const INT*>(in), static_cast<OUTT*>(out), n, inScale, k); \
