@@ -589,10 +589,10 @@ __global__ void __launch_bounds__(256) dasVariantTableKernel(DasArgs a) {
 // depend on depth: they and their running sum are computed once per scanline in the same order, so
 // results stay bit-identical to sample3D. The loop takes elements four at a time: delays and
 // weights of all four, then their gathers, then the four additions in element order (an element the
-// reference skips adds nothing). The table is padded to a multiple of four with elements at infinity,
-// whose delays fall beyond every record. Five CTAs per SM (48 registers): the gathers' latency is
-// hidden by occupancy and the four-element groups; eight-element groups need 80 registers and run
-// slower.
+// reference skips adds nothing). The table is padded to a multiple of four (see das3dAccum for the
+// padding entries). Six CTAs per SM (40 registers, 56 bytes of spill stores): the
+// gathers' latency is hidden by occupancy and the four-element groups (2% faster than five CTAs at 48
+// registers on c2); eight-element groups run slower at 64 registers and four CTAs.
 constexpr int kMax3DElems = 1024;
 constexpr int k3DUnroll = 4;
 
@@ -671,7 +671,7 @@ __device__ __forceinline__ void das3dAccum(const float4* elA, const float4* elB,
 }
 
 template <typename RF, typename OUT>
-__global__ void __launch_bounds__(256, 5) das3dTableKernel(DasArgs a, int cap) {
+__global__ void __launch_bounds__(256, 6) das3dTableKernel(DasArgs a, int cap) {
     __shared__ float lut[64];
     __shared__ int nEl, maxR2Bits;
     __shared__ float sumDeep;
