@@ -132,6 +132,49 @@ def cpu_sample(threads):
     return geoms, rfs
 
 
+def cpu_rows(res):
+    """The reference's CPU path beside the library's GPU time for the other configurations, on the box's
+    host cores: c0 2D DAS and c2 3D DAS through the reference's own sampleBeamform2D/3D (oracle/_ref; the
+    oracle's restatement when it is absent), c3 MV through the oracle's FP32 restatement of
+    RxBeamformerMV on 16 of the 128 scanlines, scaled to the full c3 (the reference has no CPU MV)."""
+    import torch
+    from oracle import oracle as O
+    from supra_b200 import synth
+    from supra_b200 import workloads as W
+    use_ref = O.ref_lib() is not None
+    threads = os.cpu_count() or 1
+    out = {"cores": threads, "kind": "reference" if use_ref else "port"}
+
+    def timed(fn, reps):
+        best = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            best = min(best, time.perf_counter() - t0)
+        return best * 1e3
+
+    def row(name, cpu_ms, what):
+        gpu_ms = (res or {}).get(name, {}).get("ms")
+        out[name] = {"cpu_ms": cpu_ms, "gpu_ms": gpu_ms, "speedup": (cpu_ms / gpu_ms) if gpu_ms else None, "what": what}
+
+    g0, rf0 = synth.c0_frame(0, device="cpu")
+    rf0 = rf0.numpy()
+    ms = timed(lambda: O.das(g0, rf0, 1.0, window=1, ref=use_ref, threads=threads), 3)
+    row("das_c0", ms, "2D DAS of the c0 frame (128 lines x 2048 depths)")
+    g2 = W.c2_geometry()
+    rf2 = W.c2_volume(g2, device="cpu").numpy()
+    ms = timed(lambda: O.das(g2, rf2, 1.0, window=1, ref=use_ref, threads=threads), 1)
+    row("das3d_c2", ms, "3D DAS of the c2 volume (32 x 32 lines x 1024 depths)")
+    del rf2
+    _, x3 = W.c3_raw_delayed()
+    x16 = x3[:16].cpu().numpy()
+    del x3
+    torch.cuda.empty_cache()
+    ms = timed(lambda: O.mv(x16, W.C3_L, W.C3_T, 1.5, W.C3_LOADING, threads=threads), 1) * (128 / 16)
+    row("mv_c3", ms, "complex MV of c3, timed on 16 of 128 scanlines and scaled by 8 (oracle FP32 restatement)")
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -650,6 +693,8 @@ def main():
         cpu = {"value": n / (time.perf_counter() - t0), "unit": UNIT, "cores": threads, "kind": kind,
                "sample": ("the reference's sampleBeamform2D" if kind == "reference" else "oracle DAS (reference FP32 "
                           "semantics)") + " + complex IQ (oracle), one frame per probe per step, ~10 s"}
+        if extra is not None:
+            extra["cpu"] = cpu_rows(extra)
 
     if rank == 0:
         out = {
