@@ -228,8 +228,8 @@ def _graph_ms(fn, n, warm=2):
 
 def _event_ms(fn, n, warm=2, reps=3):
     """Mean time of n back-to-back calls (CUDA events on the current stream), the smallest of `reps`
-    repetitions, as the reference rows are timed: run-to-run spread on a shared node (other tenants'
-    GPUs share its power and cooling) reaches tens of percent for multi-millisecond kernels."""
+    repetitions, as the reference rows are timed: back-to-back runs of a multi-millisecond kernel were
+    seen to spread by tens of percent on one box."""
     import torch
     for _ in range(warm):
         fn()
