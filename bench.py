@@ -399,7 +399,7 @@ def extras(wl, plans):
 
 
 def reference_gpu_rows(res):
-    """The reference's own kernels on this GPU (BASELINE row B2): the reference's sources built with its
+    """The reference's own kernels on this GPU: the reference's sources built with its
     production flags (--use_fast_math, release), oracle/_ref/libsupra_ref_gpu_fast.so, each called as its
     node calls it per frame (kernels + pooled output allocation), CUDA-event time per call on the call's
     stream. Beside each: the library's time for the same input from `res` and the speed-up. Even FIR
