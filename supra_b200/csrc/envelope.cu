@@ -480,10 +480,10 @@ __global__ void __launch_bounds__(256) iqMagnitude1Kernel(const IN* __restrict__
 // Several reference frequencies (frequency compounding): a CTA of 32 scanlines x 32 decimated outputs
 // stages its raw samples (band-pass and low-pass halos included, eight loads in flight per thread)
 // and the filter bank in shared memory, forms each filter's mixer values once per input row, then
-// evaluates the filter-bank magnitude per sample from shared memory in the reference's operation
-// order (IQDemodulator.cu:68-137: band-pass sums by separately rounded products and additions, the
-// weighted magnitudes summed over the filters in order), and the decimating low-pass as in
-// iqMagnitude1Kernel (four outputs per thread).
+// evaluates the filter-bank magnitude of two neighbouring samples per thread from shared memory in
+// the reference's order (IQDemodulator.cu:68-137: band-pass sums over the taps in order, contracted
+// into fused multiply-adds as nvcc contracts them; the weighted magnitudes summed over the filters in
+// order), and the decimating low-pass as in iqMagnitude1Kernel (four outputs per thread).
 constexpr int IQB_OT = 32;
 constexpr int IQB_R = 4;
 
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
     __shared__ float bank[8 * (kIqMaxTaps + 1)];
     const int rows = (IQB_OT - 1) * a.stride + a.lpN + 1;  // band rows
     const int hb = a.bpN / 2;
-    const int rowsX = rows + 2 * hb;                        // raw rows
+    const int rowsX = rows + 2 * hb + 1;                    // raw rows (one past the last window: pair reads)
     constexpr int nf = NF;
     float* raw = sm;                                        // [rowsX][IQ_LINES]
     float* band = raw + rowsX * IQ_LINES;                   // [rows][IQ_LINES]
@@ -532,34 +532,65 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
             if (base + u * 256 < totalX) raw[base + u * 256] = xs[u];
     }
     __syncthreads();
-    for (int idx = tid; idx < rows * IQ_LINES; idx += blockDim.x) {
-        const int row = idx / IQ_LINES, li = idx % IQ_LINES;
-        const int s = sIn0 + row, l = l0 + li;
-        float v = 0.0f;
-        if (l < a.nL && s >= 0 && s < a.nS) {
-            float acc[NF];
-            const float* xr = raw + row * IQ_LINES + li;  // band-pass window of sample s: rows row .. row + 2 hb
-            acc[0] = xr[hb * IQ_LINES];
+    // two neighbouring rows per thread: their band-pass windows overlap in all but one row, so each
+    // raw value is read once for both, each tap once for both (fused multiply-adds, as nvcc contracts
+    // the reference's `accumulators[filter] += sample * filterElement`). Out-of-record samples are
+    // staged as 0 and add nothing, as the reference skips them.
+    const float* bk = bank + (a.bpN + 1);
+    const int nPairs = (rows + 1) / 2;
+    for (int idx = tid; idx < nPairs * IQ_LINES; idx += blockDim.x) {
+        const int row = 2 * (idx / IQ_LINES), li = idx % IQ_LINES;
+        const float* xr = raw + row * IQ_LINES + li;  // windows: rows row .. row + 2 hb and row + 1 .. row + 1 + 2 hb
+        float accA[NF], accB[NF], tp[NF];
+        accA[0] = xr[hb * IQ_LINES];
+        accB[0] = xr[(hb + 1) * IQ_LINES];
 #pragma unroll
-            for (int f = 1; f < NF; f++) acc[f] = 0.0f;
-            // out-of-record samples are staged as 0: their terms (+-0) leave the sums unchanged, as the
-            // reference skips them
-            const float* bk = bank + (a.bpN + 1);
-            for (int fe = 0; fe <= 2 * hb; fe++) {
-                const float x = xr[fe * IQ_LINES];
-#pragma unroll
-                for (int f = 1; f < NF; f++) acc[f] = __fadd_rn(acc[f], __fmul_rn(x, bk[(f - 1) * (a.bpN + 1) + fe]));
-            }
-            float m = 0.0f;
-#pragma unroll
-            for (int f = 0; f < NF; f++) {
-                const float2 c = mix[row * nf + f];
-                const float dI = __fmul_rn(acc[f], c.x), dQ = __fmul_rn(acc[f], c.y);
-                m = __fadd_rn(m, __fmul_rn(a.weights[f], __fsqrt_rn(__fadd_rn(__fmul_rn(dI, dI), __fmul_rn(dQ, dQ)))));
-            }
-            v = __fmul_rn(a.scale, m);
+        for (int f = 1; f < NF; f++) {
+            accA[f] = 0.0f;
+            accB[f] = 0.0f;
         }
-        band[idx] = v;
+        {
+            const float x = xr[0];
+#pragma unroll
+            for (int f = 1; f < NF; f++) {
+                tp[f] = bk[(f - 1) * (a.bpN + 1)];
+                accA[f] = fmaf(x, tp[f], accA[f]);
+            }
+        }
+        for (int fe = 1; fe <= 2 * hb; fe++) {
+            const float x = xr[fe * IQ_LINES];
+#pragma unroll
+            for (int f = 1; f < NF; f++) {
+                const float t = bk[(f - 1) * (a.bpN + 1) + fe];
+                accA[f] = fmaf(x, t, accA[f]);
+                accB[f] = fmaf(x, tp[f], accB[f]);
+                tp[f] = t;
+            }
+        }
+        {
+            const float x = xr[(2 * hb + 1) * IQ_LINES];
+#pragma unroll
+            for (int f = 1; f < NF; f++) accB[f] = fmaf(x, tp[f], accB[f]);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int rr = row + h;
+            const int s = sIn0 + rr, l = l0 + li;
+            if (rr >= rows) break;
+            float v = 0.0f;
+            if (l < a.nL && s >= 0 && s < a.nS) {
+                float m = 0.0f;
+#pragma unroll
+                for (int f = 0; f < NF; f++) {
+                    const float av = h == 0 ? accA[f] : accB[f];
+                    const float2 c = mix[rr * nf + f];
+                    const float dI = __fmul_rn(av, c.x), dQ = __fmul_rn(av, c.y);
+                    m = __fadd_rn(m, __fmul_rn(a.weights[f], __fsqrt_rn(__fadd_rn(__fmul_rn(dI, dI), __fmul_rn(dQ, dQ)))));
+                }
+                v = __fmul_rn(a.scale, m);
+            }
+            band[rr * IQ_LINES + li] = v;
+        }
     }
     __syncthreads();
     const int li = tid % IQ_LINES, o0 = (tid / IQ_LINES) * IQB_R;
@@ -880,7 +911,7 @@ int sb_iq_magnitude_run(const sb_iq_plan* p, const void* in, int in_dtype, void*
 #undef SB_IQ1
         return fail(SB_ERR_UNSUPPORTED, "sb_iq_magnitude_run: %d -> %d unsupported", in_dtype, out_dtype);
     }
-    const int rowsB = (IQB_OT - 1) * a.stride + a.lpN + 1, rowsBX = rowsB + 2 * (a.bpN / 2);
+    const int rowsB = (IQB_OT - 1) * a.stride + a.lpN + 1, rowsBX = rowsB + 2 * (a.bpN / 2) + 1;
     const size_t shmB = (static_cast<size_t>(rowsBX + rowsB) * IQ_LINES + 2 * static_cast<size_t>(rowsB) * a.numFilters) * sizeof(float);
     if (a.numFilters > 1 && shmB <= 150 * 1024) {
         dim3 gridB((a.nL + IQ_LINES - 1) / IQ_LINES, (a.nOut + IQB_OT - 1) / IQB_OT);
