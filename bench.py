@@ -31,8 +31,8 @@ WORKLOAD = ("c1 batched DAS+IQ: 64 frames/launch (22x P64/1024 smp, 21x P128/204
             "fs 40 MHz, 64-ch aperture, F#1 Hann, int16 in; IQ 5 MHz mix, 32-tap LPF, /4, complex64 out")
 # DRAM bytes per beamformed pixel of batchPackKernel (8 frames per pack, the autotuner's shape) measured
 # by ncu on a 24-frame case of this workload ((dram__bytes_read.sum + dram__bytes_write.sum) / pixels
-# = 993.4 MB / 7,249,920 px), scaled by pixels; profiles/batchPackKernel_c1_24frames_full.md has the capture.
-TRAFFIC_BYTES_PER_PX = 137.0
+# = 916.7 MB / 7,249,920 px), scaled by pixels; profiles/batchPackKernel_c1_24frames_full.md has the capture.
+TRAFFIC_BYTES_PER_PX = 126.4
 
 
 def peaks():

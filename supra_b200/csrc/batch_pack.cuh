@@ -402,15 +402,22 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
     __shared__ float lut[64];
     constexpr int kHalf = FP >= 4 ? FP / 2 : 1;
     // the item's beamformed depths (segment + low-pass halo), for the IQ epilogue of MODE 0
-    __shared__ float seg[MODE == 0 ? FP : 1][MODE == 0 ? kPackRows : 1];
+    // stored by decimation phase (row q of the item at (q mod dec) * segQ + q / dec), so that the
+    // epilogue's lanes, dec rows apart, read consecutive words
+    constexpr int kSegStride = kPackRows + 32;
+    __shared__ float seg[MODE == 0 ? FP : 1][MODE == 0 ? kSegStride : 1];
     __shared__ uint32_t itemIdx;
+    __shared__ int rowChunk;  // MODE 0: the item's next 32-row chunk
     __shared__ int nEl, cntDeep, deepOk, sortedX, dx2Line;
     __shared__ float sumDeep;
     const int tid = threadIdx.x;
     if (tid < 64) lut[tid] = a.lut.v[tid];
     __syncthreads();
     for (;;) {
-        if (tid == 0) itemIdx = atomicAdd(a.counter, 1u);
+        if (tid == 0) {
+            itemIdx = atomicAdd(a.counter, 1u);
+            rowChunk = 0;  // the previous item's warps left its row loop before its epilogue barrier
+        }
         __syncthreads();
         const uint32_t it = itemIdx;
         if (it >= a.nItems) return;
@@ -506,37 +513,59 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
         const int so0 = static_cast<int>(pi.seg0) / a.dec;
         const int so1 = min(static_cast<int>(pi.seg1) / a.dec, nD / a.dec);
         const int nBlocks = (rEnd - rStart + NT - 1) / NT;
+        const int pd = a.dec <= 32 ? a.dec : 1;
+        const int segQ = (kPackRows + 32) / pd;
+        auto segAt = [pd, segQ](int q) { return (q % pd) * segQ + q / pd; };
         // frames of a partial pack take the narrower loops (a pack of 4 frames holding 1 or 2; a pack of
         // 8 holding 5 or 6 takes the 6-frame loop)
         constexpr int kSix = FP == 8 ? 6 : FP;
         const int kw = nf > kSix ? FP : nf > kHalf ? kSix : (nf > 1 ? kHalf : 1);
-        for (int k = 0; k < nBlocks; k++) {
-            // deeper rows hold wider apertures (more elements): odd blocks give the warps their rows in
-            // mirrored order, so that over an item each warp sums a mix of shallow and deep rows and
-            // the warps reach the item's barrier together
-            const int wb = tid & ~31;
-            const int r = rStart + k * NT + (((k & 1) && MODE == 0) ? (NT - 32 - wb) + (tid & 31) : tid);
-            PackAcc<FP> acc;
+        if constexpr (MODE == 0) {
+            // the warps take the item's rows 32 at a time from a CTA counter, deepest chunk first
+            // (deeper rows hold wider apertures): a warp that finishes early takes more rows, so the
+            // warps reach the item's barrier together
+            const int lane = tid & 31;
+            const int nChunks = (rEnd - rStart + 31) >> 5;
+            for (;;) {
+                int c = 0;
+                if (lane == 0) c = atomicAdd(&rowChunk, 1);
+                c = __shfl_sync(0xffffffffu, c, 0);
+                if (c >= nChunks) break;
+                const int r = rStart + ((nChunks - 1 - c) << 5) + lane;
+                PackAcc<FP> acc;
 #pragma unroll
-            for (int f = 0; f < FP; f++) acc.v[f] = 0.0f;
-            if (r < rEnd && valid) {
-                const float d = __ldg(P.depth + r);
-                if (kw == FP) packRow<FP, FP, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
-                else if (FP == 8 && kw == kSix) packRow<FP, kSix, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
-                else if (kw == kHalf) packRow<FP, kHalf, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
-                else packRow<FP, 1, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
-            }
-            if (MODE == 1) {
-                if (r < rEnd) P.rfOut[0][pi.line + static_cast<size_t>(r) * P.nRx] = acc.v[0];
-                continue;
-            }
-            if (r < rEnd) {
-#pragma unroll
-                for (int f = 0; f < FP; f++) {
-                    seg[f][r - rStart] = acc.v[f];
-                    if (f < nf && r >= static_cast<int>(pi.seg0) && r < static_cast<int>(pi.seg1) && P.rfOut[f])
-                        P.rfOut[f][pi.line + static_cast<size_t>(r) * P.nRx] = acc.v[f];
+                for (int f = 0; f < FP; f++) acc.v[f] = 0.0f;
+                if (r < rEnd && valid) {
+                    const float d = __ldg(P.depth + r);
+                    if (kw == FP) packRow<FP, FP, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                    else if (FP == 8 && kw == kSix) packRow<FP, kSix, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                    else if (kw == kHalf) packRow<FP, kHalf, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                    else packRow<FP, 1, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
                 }
+                if (r < rEnd) {
+#pragma unroll
+                    for (int f = 0; f < FP; f++) {
+                        seg[f][segAt(r - rStart)] = acc.v[f];
+                        if (f < nf && r >= static_cast<int>(pi.seg0) && r < static_cast<int>(pi.seg1) && P.rfOut[f])
+                            P.rfOut[f][pi.line + static_cast<size_t>(r) * P.nRx] = acc.v[f];
+                    }
+                }
+            }
+        } else {
+            // MODE 1: one frame, rows in block order, RF straight to the image
+            for (int k = 0; k < nBlocks; k++) {
+                const int r = rStart + k * NT + tid;
+                PackAcc<FP> acc;
+#pragma unroll
+                for (int f = 0; f < FP; f++) acc.v[f] = 0.0f;
+                if (r < rEnd && valid) {
+                    const float d = __ldg(P.depth + r);
+                    if (kw == FP) packRow<FP, FP, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                    else if (FP == 8 && kw == kSix) packRow<FP, kSix, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                    else if (kw == kHalf) packRow<FP, kHalf, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                    else packRow<FP, 1, EXACT>(el, n, lut, P, s, tb, nf, d, deepOk, sortedX, sumDeep, cntDeep, dx2, acc);
+                }
+                if (r < rEnd) P.rfOut[0][pi.line + static_cast<size_t>(r) * P.nRx] = acc.v[0];
             }
         }
         if (MODE == 1) continue;  // the next item's first barrier orders the table's reuse
@@ -553,17 +582,30 @@ __global__ void __launch_bounds__(NT, MINB) batchPackKernel(PackArgs a) {
             float2 z[FP];
 #pragma unroll
             for (int f = 0; f < FP; f++) z[f] = make_float2(0.0f, 0.0f);
-            for (int j = 0; j < a.taps; j++) {
+            // taps inside the record, in order; the first one's row is at or after rStart
+            const int jLo = interior ? 0 : max(0, -base);
+            const int jHi = interior ? a.taps : min(a.taps, nD - base);
+            int ph = 0, qi = 0;
+            if (jLo < jHi) {
+                const int q = base + jLo - rStart;
+                ph = q % pd;
+                qi = q / pd;
+            }
+            for (int j = jLo; j < jHi; j++) {
                 const int nn = base + j;
-                if (!interior && (nn < 0 || nn >= nD)) continue;
                 const float lpj = a.lp[j];
                 const float2 w = __ldg(a.rot + nn);
+                const int sq = ph * segQ + qi;
 #pragma unroll
                 for (int f = 0; f < FP; f++) {
                     if (f < nf) {
-                        const float x = __fmul_rn(seg[f][nn - rStart], lpj);
+                        const float x = __fmul_rn(seg[f][sq], lpj);
                         z[f] = __ffma2_rn(make_float2(x, x), w, z[f]);
                     }
+                }
+                if (++ph == pd) {
+                    ph = 0;
+                    qi++;
                 }
             }
 #pragma unroll
