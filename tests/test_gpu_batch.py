@@ -57,6 +57,27 @@ def test_batch_iq_vs_fp64(small_batch, oracle):
         assert err <= 2e-6 * np.max(np.abs(ref)), (k, err, np.max(np.abs(ref)))
 
 
+@pytest.mark.parametrize("decimation,lowpass", [(1, 16), (2, 31), (3, 32), (5, 20), (8, 64), (40, 8)])
+@pytest.mark.parametrize("frames_per_pack", [4, 8])
+def test_batch_iq_decimations(small_batch, oracle, decimation, lowpass, frames_per_pack):
+    """The pack kernel keeps an item's rows in shared memory ordered by decimation phase; every
+    decimation (up to 32 phases, row order above) and low-pass length gives the FP64 IQ of its RF."""
+    from supra_b200.api import BatchedDasIq
+    geoms, plans, probe, rfs = small_batch
+    b = BatchedDasIq([(plans[p], rf) for p, rf in zip(probe, rfs)], 1.0, 1540e3, 1, 0.0, 5e6, 2.5e6, lowpass,
+                     decimation, ctas_per_sm=4, depth_tile=256, frames_per_pack=frames_per_pack)
+    b.enable_rf_outputs()
+    b.run(use_graph=True)
+    torch.cuda.synchronize()
+    for k, p in enumerate(probe):
+        rf = b.rf_outputs[k].cpu().numpy()
+        ref = oracle.iq_complex(rf, 40e6, 5e6, 2.5e6, lowpass, decimation)
+        got = b.outputs[k].cpu().numpy()
+        assert got.shape == ref.shape
+        err = np.max(np.abs(got - ref))
+        assert err <= 2e-6 * np.max(np.abs(ref)), (k, err, np.max(np.abs(ref)))
+
+
 def test_batch_autotune_and_cache(small_batch, tmp_path):
     from supra_b200.api import BatchedDasIq
     geoms, plans, probe, rfs = small_batch
