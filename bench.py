@@ -532,6 +532,7 @@ def profile_case(case: str):
         big = torch.randn((16384, 2048), generator=gen, device="cuda") * 1000.0
         HilbertFirEnvelope(64).demodulate(big)
         IQDemodulator(40e6, 2.5e6, 51, 51, (7e6,), (1e6,), (1.0,)).demodulate_magnitude(big, 4)
+        IQDemodulator(40e6, 2.5e6, 51, 51, (7e6, 5e6, 9e6), (1e6, 2e6, 2e6), (1.0, 0.5, 0.5)).demodulate_magnitude(big, 4)
         LogCompressor().compress(big, 50.0, 1.0, 4000.0, out_dtype=torch.uint8)
     elif case == "misc":
         # one launch each: c0 DAS (single-frame pack kernel), DelayAndStdDev on c0, the FFT envelope of

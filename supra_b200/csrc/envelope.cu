@@ -486,6 +486,9 @@ __global__ void __launch_bounds__(256) iqMagnitude1Kernel(const IN* __restrict__
 // order), and the decimating low-pass as in iqMagnitude1Kernel (four outputs per thread).
 constexpr int IQB_OT = 32;
 constexpr int IQB_R = 4;
+// band rows per thread in the band-pass stage: their windows share all raw reads and tap reads (eight
+// rows for two filters, four for three or four, two above: the measured best at 16384 x 2048)
+__host__ __device__ constexpr int iqbRowsPerThread(int nf) { return nf <= 2 ? 8 : nf <= 4 ? 4 : 2; }
 
 template <typename IN, typename OUT, int NF>
 __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restrict__ in, OUT* __restrict__ out, IqArgs a) {
@@ -494,7 +497,8 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
     __shared__ float bank[8 * (kIqMaxTaps + 1)];
     const int rows = (IQB_OT - 1) * a.stride + a.lpN + 1;  // band rows
     const int hb = a.bpN / 2;
-    const int rowsX = rows + 2 * hb + 1;                    // raw rows (one past the last window: pair reads)
+    constexpr int RB = iqbRowsPerThread(NF);
+    const int rowsX = rows + 2 * hb + RB - 1;               // raw rows (the last group's windows included)
     constexpr int nf = NF;
     float* raw = sm;                                        // [rowsX][IQ_LINES]
     float* band = raw + rowsX * IQ_LINES;                   // [rows][IQ_LINES]
@@ -532,48 +536,82 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
             if (base + u * 256 < totalX) raw[base + u * 256] = xs[u];
     }
     __syncthreads();
-    // two neighbouring rows per thread: their band-pass windows overlap in all but one row, so each
-    // raw value is read once for both, each tap once for both (fused multiply-adds, as nvcc contracts
-    // the reference's `accumulators[filter] += sample * filterElement`). Out-of-record samples are
-    // staged as 0 and add nothing, as the reference skips them.
+    // RB neighbouring rows per thread: their band-pass windows overlap, so each raw value and each tap
+    // is read once for all of them (fused multiply-adds, as nvcc contracts the reference's
+    // `accumulators[filter] += sample * filterElement`; every row sums its taps in order). Raw value e
+    // of the group meets tap e - h of row h; tp[f][h] holds filter f's tap e - h. Out-of-record samples
+    // are staged as 0 and add nothing, as the reference skips them.
     const float* bk = bank + (a.bpN + 1);
-    const int nPairs = (rows + 1) / 2;
-    for (int idx = tid; idx < nPairs * IQ_LINES; idx += blockDim.x) {
-        const int row = 2 * (idx / IQ_LINES), li = idx % IQ_LINES;
-        const float* xr = raw + row * IQ_LINES + li;  // windows: rows row .. row + 2 hb and row + 1 .. row + 1 + 2 hb
-        float accA[NF], accB[NF], tp[NF];
-        accA[0] = xr[hb * IQ_LINES];
-        accB[0] = xr[(hb + 1) * IQ_LINES];
+    const int W = 2 * hb;  // last tap
+    const int nGroups = (rows + RB - 1) / RB;
+    for (int idx = tid; idx < nGroups * IQ_LINES; idx += blockDim.x) {
+        const int row = RB * (idx / IQ_LINES), li = idx % IQ_LINES;
+        const float* xr = raw + row * IQ_LINES + li;
+        float acc[RB][NF], tp[NF][RB];
 #pragma unroll
-        for (int f = 1; f < NF; f++) {
-            accA[f] = 0.0f;
-            accB[f] = 0.0f;
-        }
-        {
-            const float x = xr[0];
+        for (int h = 0; h < RB; h++) {
+            acc[h][0] = xr[(hb + h) * IQ_LINES];
 #pragma unroll
             for (int f = 1; f < NF; f++) {
-                tp[f] = bk[(f - 1) * (a.bpN + 1)];
-                accA[f] = fmaf(x, tp[f], accA[f]);
+                acc[h][f] = 0.0f;
+                tp[f][h] = 0.0f;
             }
         }
-        for (int fe = 1; fe <= 2 * hb; fe++) {
-            const float x = xr[fe * IQ_LINES];
+        if (W >= RB - 1) {
+            // e < RB - 1: rows h <= e have begun
 #pragma unroll
-            for (int f = 1; f < NF; f++) {
-                const float t = bk[(f - 1) * (a.bpN + 1) + fe];
-                accA[f] = fmaf(x, t, accA[f]);
-                accB[f] = fmaf(x, tp[f], accB[f]);
-                tp[f] = t;
+            for (int e = 0; e < RB - 1; e++) {
+                const float x = xr[e * IQ_LINES];
+#pragma unroll
+                for (int f = 1; f < NF; f++) {
+#pragma unroll
+                    for (int k = RB - 1; k > 0; k--) tp[f][k] = tp[f][k - 1];
+                    tp[f][0] = bk[(f - 1) * (a.bpN + 1) + e];
+#pragma unroll
+                    for (int h = 0; h <= e; h++) acc[h][f] = fmaf(x, tp[f][h], acc[h][f]);
+                }
+            }
+            // every row of the group takes a tap
+#pragma unroll 4
+            for (int e = RB - 1; e <= W; e++) {
+                const float x = xr[e * IQ_LINES];
+#pragma unroll
+                for (int f = 1; f < NF; f++) {
+#pragma unroll
+                    for (int k = RB - 1; k > 0; k--) tp[f][k] = tp[f][k - 1];
+                    tp[f][0] = bk[(f - 1) * (a.bpN + 1) + e];
+#pragma unroll
+                    for (int h = 0; h < RB; h++) acc[h][f] = fmaf(x, tp[f][h], acc[h][f]);
+                }
+            }
+            // e = W + i: rows h > i - 1 still take tap e - h
+#pragma unroll
+            for (int i = 1; i < RB; i++) {
+                const float x = xr[(W + i) * IQ_LINES];
+#pragma unroll
+                for (int f = 1; f < NF; f++) {
+#pragma unroll
+                    for (int k = RB - 1; k > 0; k--) tp[f][k] = tp[f][k - 1];
+#pragma unroll
+                    for (int h = i; h < RB; h++) acc[h][f] = fmaf(x, tp[f][h], acc[h][f]);
+                }
+            }
+        } else {
+            // filters shorter than the group: the same sums with the tap range tested per row
+            for (int e = 0; e <= W + RB - 1; e++) {
+                const float x = xr[e * IQ_LINES];
+#pragma unroll
+                for (int f = 1; f < NF; f++) {
+#pragma unroll
+                    for (int h = 0; h < RB; h++) {
+                        const int fe = e - h;
+                        if (fe >= 0 && fe <= W) acc[h][f] = fmaf(x, bk[(f - 1) * (a.bpN + 1) + fe], acc[h][f]);
+                    }
+                }
             }
         }
-        {
-            const float x = xr[(2 * hb + 1) * IQ_LINES];
 #pragma unroll
-            for (int f = 1; f < NF; f++) accB[f] = fmaf(x, tp[f], accB[f]);
-        }
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
+        for (int h = 0; h < RB; h++) {
             const int rr = row + h;
             const int s = sIn0 + rr, l = l0 + li;
             if (rr >= rows) break;
@@ -582,7 +620,7 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
                 float m = 0.0f;
 #pragma unroll
                 for (int f = 0; f < NF; f++) {
-                    const float av = h == 0 ? accA[f] : accB[f];
+                    const float av = acc[h][f];
                     const float2 c = mix[rr * nf + f];
                     const float dI = __fmul_rn(av, c.x), dQ = __fmul_rn(av, c.y);
                     m = __fadd_rn(m, __fmul_rn(a.weights[f], __fsqrt_rn(__fadd_rn(__fmul_rn(dI, dI), __fmul_rn(dQ, dQ)))));
@@ -911,7 +949,8 @@ int sb_iq_magnitude_run(const sb_iq_plan* p, const void* in, int in_dtype, void*
 #undef SB_IQ1
         return fail(SB_ERR_UNSUPPORTED, "sb_iq_magnitude_run: %d -> %d unsupported", in_dtype, out_dtype);
     }
-    const int rowsB = (IQB_OT - 1) * a.stride + a.lpN + 1, rowsBX = rowsB + 2 * (a.bpN / 2) + 1;
+    const int rowsB = (IQB_OT - 1) * a.stride + a.lpN + 1;
+    const int rowsBX = rowsB + 2 * (a.bpN / 2) + iqbRowsPerThread(static_cast<int>(a.numFilters)) - 1;
     const size_t shmB = (static_cast<size_t>(rowsBX + rowsB) * IQ_LINES + 2 * static_cast<size_t>(rowsB) * a.numFilters) * sizeof(float);
     if (a.numFilters > 1 && shmB <= 150 * 1024) {
         dim3 gridB((a.nL + IQ_LINES - 1) / IQ_LINES, (a.nOut + IQB_OT - 1) / IQB_OT);
