@@ -41,18 +41,21 @@ def test_logcompress(oracle, out_dtype):
         assert np.max(np.abs(got - ref)) <= 1e-5 * 255
 
 
-@pytest.mark.parametrize("dec,filters", [(8, 1), (4, 3), (1, 1), (2, 5), (1, 8)])
-def test_iq_magnitude(oracle, dec, filters):
-    """One reference frequency (iqMagnitude1Kernel) and 3, 5 and 8 frequencies (the filter-bank kernel
-    specialised on the filter count) against the oracle's restatement of IQDemodulator.cu:68-175."""
+@pytest.mark.parametrize("dec,filters,bp", [(8, 1, 51), (4, 3, 51), (1, 1, 51), (2, 5, 51), (1, 8, 51), (4, 2, 51),
+                                            (3, 3, 3), (2, 2, 5), (4, 4, 7)])
+def test_iq_magnitude(oracle, dec, filters, bp):
+    """One reference frequency (iqMagnitude1Kernel) and 2-8 frequencies (the filter-bank kernel
+    specialised on the filter count, band-pass rows in groups of 8, 4 or 2 per thread; band-pass
+    filters shorter than a group take the per-row tap test) against the oracle's restatement of
+    IQDemodulator.cu:68-175."""
     from supra_b200.api import IQDemodulator
     g, img = rf_image()
     img = torch.nan_to_num(img, nan=0.0, posinf=0.0, neginf=0.0)
     refs = [7e6, 5e6, 9e6, 6e6, 8e6, 4e6, 10e6, 7.5e6][:filters]
     bws = [1e6, 2e6, 2e6, 1.5e6, 1.5e6, 1e6, 2e6, 1e6][:filters]
     ws = [1.0, 0.5, 0.5, 0.25, 0.25, 0.75, 0.5, 1.0][:filters]
-    ref = oracle.iq_magnitude(img.cpu().numpy(), dec, 40e6, 2.5e6, 51, 51, refs, bws, ws)
-    got = IQDemodulator(40e6, 2.5e6, 51, 51, refs, bws, ws).demodulate_magnitude(img, dec).cpu().numpy()
+    ref = oracle.iq_magnitude(img.cpu().numpy(), dec, 40e6, 2.5e6, 51, bp, refs, bws, ws)
+    got = IQDemodulator(40e6, 2.5e6, 51, bp, refs, bws, ws).demodulate_magnitude(img, dec).cpu().numpy()
     assert got.shape == ref.shape
     assert np.max(np.abs(got - ref)) <= 1e-5 * np.max(np.abs(ref))
 

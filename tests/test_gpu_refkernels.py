@@ -99,7 +99,7 @@ def test_logcompress_identical_to_reference_kernel(ref, rf_image, uint8):
         assert np.array_equal(bits(got), bits(want))
 
 
-@pytest.mark.parametrize("dec,filters", [(4, 1), (8, 3)])
+@pytest.mark.parametrize("dec,filters", [(4, 1), (8, 3), (4, 2)])
 def test_iq_magnitude_matches_reference_kernel(ref, rf_image, dec, filters):
     from supra_b200.api import IQDemodulator
     refs = [7e6, 5e6, 9e6][:filters]
