@@ -382,6 +382,13 @@ int sb_check_device_errors(int reset);
  * arrive = 1 the wait completes. *completed (may be NULL) receives 1 if the wait completed. No fault:
  * the context stays usable. Synchronises `stream`. */
 int sb_selftest_bounded_wait(uint32_t polls, int arrive, int* completed, sb_stream stream);
+/* Self-test of the Newton square root the 3D delay kernel takes for arguments in [2^-102, FLT_MAX] (bit
+ * patterns [0x0C800000, 0x7F800000); no reference counterpart): compares it with the IEEE square root
+ * (__fsqrt_rn) on every float whose bit pattern lies in [first_bits, end_bits)
+ * (end_bits <= 2^32; equal bits, or NaN for both); *mismatches receives the number of differing results, *first_mismatch (may be
+ * NULL) the lowest differing bit pattern (0xFFFFFFFF when none). Synchronises `stream`. */
+int sb_selftest_sqrt(uint32_t first_bits, uint64_t end_bits, uint64_t* mismatches, uint32_t* first_mismatch,
+                     sb_stream stream);
 
 /* ---------------------------------------------------------------- adjoint DAS */
 

@@ -152,6 +152,7 @@ _SIGNATURES = {
     "sb_das_run_beamformer": (_int, [_vp, _int, _vp, _int, _vp, _int, _f64, _f64, _int, _f32, _int, _i32, _vp]),
     "sb_temporal_filter_run": (_int, [_vp, _u32, _vp, _int, _vp, _int, C.c_uint64, _vp]),
     "sb_selftest_bounded_wait": (_int, [_u32, _int, C.POINTER(_int), _vp]),
+    "sb_selftest_sqrt": (_int, [_u32, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(_u32), _vp]),
     "sb_analytic_plan_create": (_int, [_u32, C.POINTER(_vp)]),
     "sb_analytic_plan_destroy": (_int, [_vp]),
     "sb_analytic_env_run": (_int, [_vp, _vp, _int, _vp, _int, _u32, _vp]),

@@ -62,6 +62,19 @@ template <> __device__ __forceinline__ uint16_t clampCast<uint16_t>(float x) {
 
 template <typename T> __device__ __forceinline__ float toFloat(T v) { return static_cast<float>(v); }
 
+// Square root by one Newton step from the hardware reciprocal square root (Markstein's refinement:
+// s = x y, the residual r = x - s^2 exactly by a fused multiply-add, then s + r y / 2). On this GPU it
+// equals __fsqrt_rn bit for bit for every x in [2^-102, FLT_MAX] (sb_selftest_sqrt compares all of
+// them); callers use it only where their arguments provably lie in that range.
+#ifdef __CUDACC__
+__device__ __forceinline__ float sqrtNewton(float x) {
+    const float y = rsqrtf(x);
+    const float s = __fmul_rn(x, y);
+    const float r = __fmaf_rn(-s, s, x);
+    return __fmaf_rn(r, __fmul_rn(0.5f, y), s);
+}
+#endif
+
 // Number of SMs of the current device (cached per device).
 int smCount();
 

@@ -609,7 +609,7 @@ template <> __device__ __forceinline__ float ldSample<float>(const float* p) { r
 // INTERIOR (STRAIGHT only, checked by the caller for the whole warp): every element's delay lies in
 // [0, nS - 1), so the record-edge cases drop out. Padding elements then have r2 = 0, deep weight 0 and
 // row 0 (an in-range gather whose term is +-0, which leaves the sum unchanged) and no aperture.
-template <typename RF, bool DEEP, bool STRAIGHT, bool OFS, bool INTERIOR>
+template <typename RF, bool DEEP, bool STRAIGHT, bool OFS, bool INTERIOR, bool NEWTON>
 __device__ __forceinline__ void das3dAccum(const float4* elA, const float4* elB, const float* lut, int nPad,
                                            const RF* tx, uint32_t nS, float px, float pz, float ay2, float iD,
                                            float d, float offset, float aDT2, float invX, float invY,
@@ -640,7 +640,7 @@ __device__ __forceinline__ void das3dAccum(const float4* elA, const float4* elB,
                 const float qx = __fsub_rn(A.x, px), qz = __fsub_rn(A.y, pz);
                 q = __fadd_rn(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qz, qz)), ay2);
             }
-            const float dl = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(q), d));
+            const float dl = __fadd_rn(iD, __fadd_rn(NEWTON ? sqrtNewton(q) : __fsqrt_rn(q), d));
             const float delayf = OFS ? __fadd_rn(dl, offset) : dl;
             // floor as unsigned, saturating at 0 for negative (and NaN) positions like the reference's
             // conversion; positions >= 2^23 give an index >= 2^23, beyond every record
@@ -761,9 +761,9 @@ __global__ void __launch_bounds__(256, 6) das3dTableKernel(DasArgs a, int cap) {
         const float pz = __fadd_rn(s.z, __fmul_rn(s.dirZ, d));
         const float ay = __fmul_rn(s.dirY, d);
         const float ay2 = __fmul_rn(ay, ay);
-#define SB_3D(DP, ST, OF, IN)                                                                                  \
-    das3dAccum<RF, DP, ST, OF, IN>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset,    \
-                                   aDT2, invX, invY, sample, weightAcum, numAdds)
+#define SB_3D(DP, ST, OF, IN, NW)                                                                              \
+    das3dAccum<RF, DP, ST, OF, IN, NW>(elA, elB, lut, nPad, tx, a.nS, px, pz, ay2, s.initialDelay[k], d, a.offset, \
+                                       aDT2, invX, invY, sample, weightAcum, numAdds)
         const bool ofs = a.offset != 0.0f;
         if (straight && !ofs) {
             // delays grow with q = r2 + ay2 (monotone float operations), so the element with the largest
@@ -771,18 +771,24 @@ __global__ void __launch_bounds__(256, 6) das3dTableKernel(DasArgs a, int cap) {
             const float iD = s.initialDelay[k];
             const float lo = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(ay2), d));
             const float hi = __fadd_rn(iD, __fadd_rn(__fsqrt_rn(__fadd_rn(maxR2, ay2)), d));
-            const bool interior = __all_sync(__activemask(), lo >= 0.0f && hi < static_cast<float>(a.nS - 1));
+            // every q = r2 + ay2 of this depth (r2 >= 0 from the table, sums of non-negative floats are
+            // monotone) lies in [ay2, maxR2 + ay2]: inside [2^-102, FLT_MAX], where the Newton square root
+            // is the IEEE one, unless ay2 is 0 or tiny (the first depths) or the sum overflows. The
+            // interior loop takes the Newton root; a warp with any other depth takes the general loop.
+            const bool newton = ay2 >= 0x1p-102f && __fadd_rn(maxR2, ay2) <= FLT_MAX;
+            const bool interior =
+                __all_sync(__activemask(), lo >= 0.0f && hi < static_cast<float>(a.nS - 1) && newton);
             if (interior) {
-                if (deep) SB_3D(true, true, false, true);
-                else SB_3D(false, true, false, true);
+                if (deep) SB_3D(true, true, false, true, true);
+                else SB_3D(false, true, false, true, true);
             } else {
-                if (deep) SB_3D(true, true, false, false);
-                else SB_3D(false, true, false, false);
+                if (deep) SB_3D(true, true, false, false, false);
+                else SB_3D(false, true, false, false, false);
             }
         } else if (deep) {
-            SB_3D(true, false, true, false);
+            SB_3D(true, false, true, false, false);
         } else {
-            SB_3D(false, false, true, false);
+            SB_3D(false, false, true, false, false);
         }
 #undef SB_3D
     }
