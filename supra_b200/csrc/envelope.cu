@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(256) iqMagnitude1Kernel(const IN* __restrict__
 // Several reference frequencies (frequency compounding): a CTA of 32 scanlines x 32 decimated outputs
 // stages its raw samples (band-pass and low-pass halos included, eight loads in flight per thread)
 // and the filter bank in shared memory, forms each filter's mixer values once per input row, then
-// evaluates the filter-bank magnitude of two neighbouring samples per thread from shared memory in
+// evaluates the filter-bank magnitude of a group of neighbouring samples per thread from shared memory in
 // the reference's order (IQDemodulator.cu:68-137: band-pass sums over the taps in order, contracted
 // into fused multiply-adds as nvcc contracts them; the weighted magnitudes summed over the filters in
 // order), and the decimating low-pass as in iqMagnitude1Kernel (four outputs per thread).
@@ -494,7 +494,7 @@ template <typename IN, typename OUT, int NF>
 __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restrict__ in, OUT* __restrict__ out, IqArgs a) {
     extern __shared__ float sm[];
     __shared__ float lps[kIqMaxTaps + 1];
-    __shared__ float bank[8 * (kIqMaxTaps + 1)];
+    __shared__ __align__(16) float bank[8 * (kIqMaxTaps + 4)];  // filter rows at a 16-byte pitch
     const int rows = (IQB_OT - 1) * a.stride + a.lpN + 1;  // band rows
     const int hb = a.bpN / 2;
     constexpr int RB = iqbRowsPerThread(NF);
@@ -508,7 +508,11 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
     const int sIn0 = so0 * a.stride - a.lpN / 2;
     const int sX0 = sIn0 - hb;
     const int tid = threadIdx.x;
-    for (int j = tid; j < nf * (a.bpN + 1); j += blockDim.x) bank[j] = a.bank[j];
+    const int bs = (a.bpN + 1 + 3) & ~3;  // bank row pitch (floats)
+    for (int j = tid; j < nf * bs; j += blockDim.x) {
+        const int f = j / bs, k = j % bs;
+        bank[j] = k <= a.bpN ? a.bank[f * (a.bpN + 1) + k] : 0.0f;
+    }
     for (int j = tid; j <= a.lpN; j += blockDim.x) lps[j] = a.lp[j];
     for (int k = tid; k < rows * nf; k += blockDim.x) {
         const int r = k / nf, f = k % nf;
@@ -541,7 +545,7 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
     // `accumulators[filter] += sample * filterElement`; every row sums its taps in order). Raw value e
     // of the group meets tap e - h of row h; tp[f][h] holds filter f's tap e - h. Out-of-record samples
     // are staged as 0 and add nothing, as the reference skips them.
-    const float* bk = bank + (a.bpN + 1);
+    const float* bk = bank + bs;
     const int W = 2 * hb;  // last tap
     const int nGroups = (rows + RB - 1) / RB;
     for (int idx = tid; idx < nGroups * IQ_LINES; idx += blockDim.x) {
@@ -566,23 +570,54 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
                 for (int f = 1; f < NF; f++) {
 #pragma unroll
                     for (int k = RB - 1; k > 0; k--) tp[f][k] = tp[f][k - 1];
-                    tp[f][0] = bk[(f - 1) * (a.bpN + 1) + e];
+                    tp[f][0] = bk[(f - 1) * bs + e];
 #pragma unroll
                     for (int h = 0; h <= e; h++) acc[h][f] = fmaf(x, tp[f][h], acc[h][f]);
                 }
             }
-            // every row of the group takes a tap
-#pragma unroll 4
-            for (int e = RB - 1; e <= W; e++) {
+            // every row of the group takes a tap: single steps up to a multiple of four, then four steps
+            // per iteration with each filter's four taps in one 16-byte read, then single steps
+            auto step = [&](int e, const float (&tv)[NF]) {
                 const float x = xr[e * IQ_LINES];
 #pragma unroll
                 for (int f = 1; f < NF; f++) {
 #pragma unroll
                     for (int k = RB - 1; k > 0; k--) tp[f][k] = tp[f][k - 1];
-                    tp[f][0] = bk[(f - 1) * (a.bpN + 1) + e];
+                    tp[f][0] = tv[f];
 #pragma unroll
                     for (int h = 0; h < RB; h++) acc[h][f] = fmaf(x, tp[f][h], acc[h][f]);
                 }
+            };
+            int e = RB - 1;
+            for (; e <= W && (e & 3); e++) {
+                float tv[NF];
+#pragma unroll
+                for (int f = 1; f < NF; f++) tv[f] = bk[(f - 1) * bs + e];
+                step(e, tv);
+            }
+            for (; e + 3 <= W; e += 4) {
+                float4 t4[NF];
+#pragma unroll
+                for (int f = 1; f < NF; f++) t4[f] = *reinterpret_cast<const float4*>(bk + (f - 1) * bs + e);
+                float tv[NF];
+#pragma unroll
+                for (int f = 1; f < NF; f++) tv[f] = t4[f].x;
+                step(e, tv);
+#pragma unroll
+                for (int f = 1; f < NF; f++) tv[f] = t4[f].y;
+                step(e + 1, tv);
+#pragma unroll
+                for (int f = 1; f < NF; f++) tv[f] = t4[f].z;
+                step(e + 2, tv);
+#pragma unroll
+                for (int f = 1; f < NF; f++) tv[f] = t4[f].w;
+                step(e + 3, tv);
+            }
+            for (; e <= W; e++) {
+                float tv[NF];
+#pragma unroll
+                for (int f = 1; f < NF; f++) tv[f] = bk[(f - 1) * bs + e];
+                step(e, tv);
             }
             // e = W + i: rows h > i - 1 still take tap e - h
 #pragma unroll
@@ -605,7 +640,7 @@ __global__ void __launch_bounds__(256) iqMagnitudeBankKernel(const IN* __restric
 #pragma unroll
                     for (int h = 0; h < RB; h++) {
                         const int fe = e - h;
-                        if (fe >= 0 && fe <= W) acc[h][f] = fmaf(x, bk[(f - 1) * (a.bpN + 1) + fe], acc[h][f]);
+                        if (fe >= 0 && fe <= W) acc[h][f] = fmaf(x, bk[(f - 1) * bs + fe], acc[h][f]);
                     }
                 }
             }
